@@ -1,0 +1,355 @@
+"""Benchmark of the droplet_b200 hot path: path-vertices/s of the plain renderer.
+
+Workload (one step = one frame): the single large cumulus, a 512^3 field made of
+the config-0 puff plus three offset copies, sigma_t = 60, albedo 0.999, Mie
+phase table, sun at 30 degrees plus Hosek sky (T = 3, ground albedo 0.3),
+1920x1080, 64 spp, at most 64 scattering events, binary32.  Inputs are seeded
+synthetic data (workloads.cumulus_recipe); no dataset is involved.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank renders its own frame with its own sample streams
+(independent units, no collective): scaling is weak, value = all ranks'
+vertices / the slowest rank's time.
+
+The --impl reference arm times the reference renderer's own CPU code
+(oracle/_ref: src/kernel.cpp etc. compiled unmodified) on the host cores over a
+bounded crop of the same frame; its vertex count comes from the CPU
+restatement (same estimator, counted), as the reference code is not
+instrumented.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "droplet-render_b200"))
+sys.path.insert(0, ROOT)
+
+from droplet_b200 import camera as cam  # noqa: E402
+from droplet_b200 import workloads as W  # noqa: E402
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+W_IMG, H_IMG, SPP = 1920, 1080, 64
+METRIC = "path-vertices/s (plain renderer, single large cumulus 512^3, 1920x1080, 64 spp)"
+CPU_CROP = 48  # reference / cpu_baseline sample: 48x48 centre crop at full spp
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_inputs():
+    z = np.load(os.path.join(GOLDEN, "mie_reference_table.npz"))
+    pdf, cdf = np.ascontiguousarray(z["pdf"], np.float32), np.ascontiguousarray(z["cdf"], np.float32)
+    with open(os.path.join(GOLDEN, "sky_states.json")) as f:
+        st = next(s for s in json.load(f) if s["note"] == "c0/c1 sun")
+    return pdf, cdf, np.asarray(st["configs"]), np.asarray(st["radiances"])
+
+
+def frame_cfg(pdf, cdf, cfgs, rads) -> dict:
+    sd = cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"])
+    eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], W.CAMERA["azimuth"], W.CAMERA["elevation"])
+    viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], W_IMG, H_IMG)
+    ss, sa, ev = W.medium("c1")
+    return dict(sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=sd, sun_color=np.asarray(W.SUN["color"], np.float32),
+                sun_angle=W.SUN["angle"], turbidity=W.SKY["turbidity"], ground_albedo=W.SKY["albedo"],
+                sky_configs=cfgs, sky_radiances=rads, mie_pdf=pdf, mie_cdf=cdf, viewi=viewi, proji=proji, w=W_IMG,
+                h=H_IMG)
+
+
+def build_scene(builder: str):
+    rec = W.cumulus_recipe(512)
+    t = time.time()
+    org, vals = W.sparse_field_fast(rec)
+    log(f"field: {len(org)} blocks in {time.time() - t:.1f}s")
+    t = time.time()
+    if builder == "product":
+        from droplet_b200.scene import build_octree
+
+        oc = build_octree(org, vals, rec.voxel_size, 12)
+        nodes, bricks, mlevel = oc.nodes, oc.bricks, oc.mlevel
+    else:
+        from oracle import Port
+
+        nodes, bricks, mlevel = Port().build_octree(org, vals, rec.voxel_size, 12)
+    log(f"octree: {len(nodes)} nodes, {len(bricks)} leaves, depth {mlevel}, {time.time() - t:.1f}s")
+    return nodes, bricks, mlevel, float((vals != 0).sum()) / 512 ** 3
+
+
+def crop_box(n=CPU_CROP):
+    return (W_IMG - n) // 2, (H_IMG - n) // 2, n, n
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.stop = threading.Event()
+        self.th = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch from the committed ncu summary, scaled to this frame."""
+    p = os.path.join(ROOT, "profiles", "render_tile_kernel_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_reference_sample(nodes, bricks, cfg, threads: int, steps: int = 1, warmup: int = 0):
+    """Times the reference renderer on the crop (one step = the crop at full spp);
+    the vertex count of a step comes from the CPU restatement on the same crop."""
+    from oracle import Port, Reference
+
+    ref = Reference()
+    ref.set_threads(threads)
+    rs = ref.scene(nodes, bricks)
+    x0, y0, tw, th = crop_box()
+    for _ in range(warmup):
+        rs.render(cfg, x0, y0, tw // 4, th // 4, SPP)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        rs.render(cfg, x0, y0, tw, th, SPP)
+        times.append(time.perf_counter() - t)
+    port = Port()
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    _, _, cnt = port.render_tile(S, P, x0, y0, tw, th, SPP, seed=99, threads=threads)
+    return cnt["vertices"], times
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pdf, cdf, cfgs, rads = load_inputs()
+    cfg = frame_cfg(pdf, cdf, cfgs, rads)
+    nodes, bricks, mlevel, occ = build_scene("oracle")
+    threads = os.cpu_count() or 1
+    verts, times = cpu_reference_sample(nodes, bricks, cfg, threads, steps=max(1, args.steps),
+                                        warmup=min(args.warmup, 1))
+    dt = float(np.mean(times))
+    value = verts / dt
+    x0, y0, tw, th = crop_box()
+    sample = f"{tw}x{th} centre crop of the 1920x1080 frame at {SPP} spp per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm puffs)",
+        "config": {"workload": "c1 single large cumulus 512^3, 1920x1080, 64 spp, 64 events", "crop": sample},
+        "cpu_baseline": {"value": value, "unit": "vertices/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "vertices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from droplet_b200.renderer import PhaseTable, Renderer, RenderSettings
+    from droplet_b200.scene import Octree
+    from droplet_b200.sky import SkyState
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    pdf, cdf, cfgs, rads = load_inputs()
+    cfg = frame_cfg(pdf, cdf, cfgs, rads)
+    nodes, bricks, mlevel, occ = build_scene("product")
+    settings = RenderSettings(sigma_s=cfg["sigma_s"], sigma_a=cfg["sigma_a"], scattevs=cfg["scattevs"],
+                              sun_dir=cfg["sun_dir"], sun_color=cfg["sun_color"], sun_angle=cfg["sun_angle"],
+                              sky=SkyState(cfgs, rads), phase=PhaseTable(pdf, cdf), viewi=cfg["viewi"],
+                              proji=cfg["proji"], w=W_IMG, h=H_IMG)
+    r = Renderer(local)
+    r.upload(Octree(nodes, bricks, mlevel))
+    r.set_params(settings)
+    stream = torch.cuda.current_stream()
+    sun = torch.empty((H_IMG, W_IMG, 4), dtype=torch.float32, device="cuda")
+    sky = torch.empty_like(sun)
+    seed = 1000 + rank
+
+    def step(k):
+        r.render_tile_async(0, 0, W_IMG, H_IMG, SPP, seed, k * SPP, sun.data_ptr(), sky.data_ptr(),
+                            stream.cuda_stream)
+
+    # L2 (126 MB) is flushed between timed steps by writing a 256 MB buffer
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    r.reset_counters()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            step(args.warmup + k)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    kernel_ms = [a.elapsed_time(b) for a, b in ev]
+    t_local = sum(kernel_ms) / 1e3
+    cnt = r.counters()
+    verts_local = cnt["vertices"]
+    if world > 1:
+        t = torch.tensor([t_local], dtype=torch.float64, device="cuda")
+        v = torch.tensor([float(verts_local)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(v, op=dist.ReduceOp.SUM)
+        t_max, verts = float(t.item()), float(v.item())
+    else:
+        t_max, verts = t_local, float(verts_local)
+    value = verts / t_max
+
+    # end to end through the public blocking API with host buffers (params upload
+    # from host + render + copy of both tile buffers back), timed on the host
+    h_sun = np.zeros((H_IMG, W_IMG, 4), np.float32)
+    h2d = 0
+    settings_c = settings.to_c()
+    h2d = int(pdf.nbytes / 3 * 4 + cdf.nbytes / 3 + 16 * 4 * 2 + 64)
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        r.set_params(settings)
+        a, b = r.render_tile(0, 0, W_IMG, H_IMG, SPP, seed=seed + 7, sample_base=k * SPP)
+    t_e2e = (time.perf_counter() - t0)
+    if world > 1:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e_value = (verts / args.steps) * e2e_steps / t_e2e  # same work per frame
+    d2h = 2 * H_IMG * W_IMG * 16
+
+    peak, peak_kind = measured_peak()
+    bytes_per_step = (64.0 * cnt["node_visits"] + 32.0 * cnt["density_lookups"] + 24.0 * cnt["mie_evals"]) / args.steps
+    avg_s = t_local / args.steps
+    achieved = bytes_per_step / avg_s / 1e9
+    traffic = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind,
+                "traffic": (traffic["dram_bytes_per_vertex"] * cnt["vertices"] / args.steps) if traffic else None,
+                "algorithmic_bytes_per_vertex": bytes_per_step / (cnt["vertices"] / args.steps)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            threads = os.cpu_count() or 1
+            v_cpu, times = cpu_reference_sample(nodes, bricks, cfg, threads)
+            dt_cpu = times[0]
+            x0, y0, tw, th = crop_box()
+            cpu = {"value": v_cpu / dt_cpu, "unit": "vertices/s", "cores": threads, "kind": "reference",
+                   "sample": f"{tw}x{th} centre crop at {SPP} spp, one run ({dt_cpu:.1f}s); vertices counted by "
+                             f"the CPU restatement on the same crop"}
+        except Exception as e:  # the reference oracle needs oracle/_ref
+            cpu = {"value": None, "unit": "vertices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm puffs)",
+            "config": {"workload": "c1 single large cumulus 512^3 (plain renderer)", "image": [W_IMG, H_IMG],
+                       "spp": SPP, "scattevs": 64, "sigma_t": 60.0, "albedo": 0.999, "leaves": int(len(bricks)),
+                       "nodes": int(len(nodes)), "octree_depth": int(mlevel), "occupancy": occ,
+                       "l2": "flushed between steps (256 MB write)"},
+            "e2e": {"value": e2e_value, "unit": "vertices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "gpu_launches": args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "counters_per_step": {k: v / args.steps for k, v in cnt.items()},
+            "kernel_ms": kernel_ms,
+        }
+        print(json.dumps(line))
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

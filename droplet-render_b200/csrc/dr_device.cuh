@@ -1,0 +1,623 @@
+// Device code of the droplet_b200 hot path.  Compiled with -fmad=false: every
+// multiply and add below rounds separately, exactly as the reference's SSE4
+// build does (src/smmath.inl madd/msub are mul+add there); fused operations are
+// written explicitly as fmaf().  With IEEE division and square root (nvcc's
+// defaults) this reproduces the reference's binary32 arithmetic for the
+// octree traversal, leaf intervals and brick lookups bit for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "dr_internal.h"
+
+namespace dr {
+
+// ---- comparisons with the reference's semantics --------------------------
+__device__ __forceinline__ float sse_max(float a, float b) { return a > b ? a : b; }  // _mm_max_ps(a, b)
+__device__ __forceinline__ float sse_min(float a, float b) { return a < b ? a : b; }  // _mm_min_ps(a, b)
+__device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; } // std::max
+__device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; } // std::min
+__device__ __forceinline__ float lerp_ref(float a, float b, float t) { return t * (b - a) + a; }  // t.madd(b-a, a)
+
+// ---- bit-reproducible transcendentals --------------------------------------
+// Same operation sequences as the CPU restatement, built from IEEE binary32
+// operations and explicit fused multiply-adds:
+//   log : e ln2 + 2 atanh(s), s = (m-1)/(m+1), atanh by Maclaurin series to s^11
+//   exp : Cody-Waite reduction by ln2, Taylor series to r^11
+//   sincos: Cody-Waite reduction by pi/2 (three parts), Taylor series on |r| <= pi/4
+constexpr float kLn2Hi = 0.693115234375f;
+constexpr float kLn2Lo = 3.19461833e-05f;
+constexpr float kPio2_1 = 1.5703125f;
+constexpr float kPio2_2 = 4.83751297e-04f;
+constexpr float kPio2_3 = 7.54979013e-08f;
+constexpr float kPi = 3.14159265358979f;   // SM_PI, src/smmath.inl:16
+
+__device__ __forceinline__ float dlog(float x) {
+    if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : __int_as_float(0x7fc00000);
+    if (x == INFINITY) return x;
+    int e = 0;
+    uint32_t u = __float_as_uint(x);
+    if (u < 0x00800000u) { x = x * 16777216.0f; u = __float_as_uint(x); e = -24; }
+    e += (int)(u >> 23) - 127;
+    float m = __uint_as_float((u & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    float p = 0.0909090909f;
+    p = fmaf(p, s2, 0.111111111f);
+    p = fmaf(p, s2, 0.142857143f);
+    p = fmaf(p, s2, 0.2f);
+    p = fmaf(p, s2, 0.333333333f);
+    float t = s * s2;
+    float atanh2 = fmaf(t * p, 2.0f, s * 2.0f);
+    float fe = (float)e;
+    return fmaf(fe, kLn2Hi, fmaf(fe, kLn2Lo, atanh2));
+}
+
+__device__ __forceinline__ float dexp(float x) {
+    if (x != x) return x;
+    if (x > 88.7f) return INFINITY;
+    if (x < -103.0f) return 0.0f;
+    float k = floorf(fmaf(x, 1.44269504f, 0.5f));
+    float r = fmaf(-k, kLn2Hi, x);
+    r = fmaf(-k, kLn2Lo, r);
+    float p = 2.50521084e-08f;
+    p = fmaf(p, r, 2.75573192e-07f);
+    p = fmaf(p, r, 2.75573192e-06f);
+    p = fmaf(p, r, 2.48015873e-05f);
+    p = fmaf(p, r, 1.98412698e-04f);
+    p = fmaf(p, r, 1.38888889e-03f);
+    p = fmaf(p, r, 8.33333333e-03f);
+    p = fmaf(p, r, 4.16666667e-02f);
+    p = fmaf(p, r, 1.66666667e-01f);
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    int ki = (int)k;
+    int k1 = ki / 2, k2 = ki - k1;
+    float s1 = __uint_as_float((uint32_t)(k1 + 127) << 23);
+    float s2 = __uint_as_float((uint32_t)(k2 + 127) << 23);
+    return (p * s1) * s2;
+}
+
+__device__ __forceinline__ float dpow(float x, float y) {
+    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : INFINITY);
+    if (x < 0.0f || x != x) return __int_as_float(0x7fc00000);
+    return dexp(y * dlog(x));
+}
+
+__device__ __forceinline__ void dsincos(float x, float *ps, float *pc) {
+    float k = rintf(x * 0.636619772f);
+    float r = fmaf(-k, kPio2_1, x);
+    r = fmaf(-k, kPio2_2, r);
+    r = fmaf(-k, kPio2_3, r);
+    float r2 = r * r;
+    float sp = -7.64716373e-13f;
+    sp = fmaf(sp, r2, 1.60590438e-10f);
+    sp = fmaf(sp, r2, -2.50521084e-08f);
+    sp = fmaf(sp, r2, 2.75573192e-06f);
+    sp = fmaf(sp, r2, -1.98412698e-04f);
+    sp = fmaf(sp, r2, 8.33333333e-03f);
+    sp = fmaf(sp, r2, -1.66666667e-01f);
+    float sn = fmaf(sp * r2, r, r);
+    float cp = 4.77947733e-14f;
+    cp = fmaf(cp, r2, -1.14707456e-11f);
+    cp = fmaf(cp, r2, 2.08767570e-09f);
+    cp = fmaf(cp, r2, -2.75573192e-07f);
+    cp = fmaf(cp, r2, 2.48015873e-05f);
+    cp = fmaf(cp, r2, -1.38888889e-03f);
+    cp = fmaf(cp, r2, 4.16666667e-02f);
+    cp = fmaf(cp, r2, -0.5f);
+    float cs = fmaf(cp, r2, 1.0f);
+    int q = ((int)k) & 3;
+    float s, c;
+    if (q == 0) { s = sn; c = cs; }
+    else if (q == 1) { s = cs; c = -sn; }
+    else if (q == 2) { s = -sn; c = -cs; }
+    else { s = -cs; c = sn; }
+    *ps = s;
+    *pc = c;
+}
+
+// The reference's polynomial arccos, src/smmath.inl:414-420.
+__device__ __forceinline__ float acos_ref(float s) {
+    float z = 0.0f - s;
+    float x = z > s ? z : s;
+    float r = -0.0187293f * x + 0.0742610f;
+    r = r * x - 0.2121144f;
+    r = r * x + 1.5707288f;
+    r = r * sqrtf(1.0f - x);
+    bool n = s < 0.0f;
+    r = r - (n ? 2.0f * r : 0.0f);
+    return (n ? kPi : 0.0f) + r;
+}
+
+// ---- PCG32 (O'Neill 2014, XSH-RR) with SplitMix64-hashed streams ----------
+struct Rng {
+    uint64_t state, inc;
+    __device__ __forceinline__ uint32_t next() {
+        uint64_t old = state;
+        state = old * 6364136223846793005ull + inc;
+        uint32_t xs = (uint32_t)(((old >> 18) ^ old) >> 27);
+        uint32_t rot = (uint32_t)(old >> 59);
+        return __funnelshift_r(xs, xs, rot);
+    }
+    // (2k+1) 2^-24 on the open interval (0,1)
+    __device__ __forceinline__ float uniform() {
+        return (float)(((next() >> 9) << 1) | 1u) * 5.96046448e-08f;
+    }
+};
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ Rng rng_seed(uint64_t seed, uint64_t pixel, uint64_t sample) {
+    uint64_t a = mix64(seed ^ mix64(pixel * 0x9e3779b97f4a7c15ull + sample));
+    uint64_t b = mix64(a + 0x632be59bd9b4e019ull);
+    Rng g;
+    g.state = 0u;
+    g.inc = (b << 1) | 1u;
+    (void)g.next();
+    g.state += a;
+    (void)g.next();
+    return g;
+}
+
+// ---- per-thread counters ----------------------------------------------------
+struct Count {
+    uint32_t vertices, node_visits, density_lookups, mie_evals, gave_up;
+    __device__ __forceinline__ void zero() { vertices = node_visits = density_lookups = mie_evals = gave_up = 0; }
+};
+
+// ---- octree traversal ----------------------------------------------------
+// The reference's step traverser (src/KernelOctree.cpp:230-349) keeps t0, t1,
+// tm for all 16 levels.  Here only the current internal node's (t0, t1) stay
+// in registers; an ancestor's interval is rebuilt on pop from the root
+// interval by replaying the child slots (3 bits per level), which repeats the
+// reference's tm = 0.5f*(t0+t1) selections and gives identical floats.
+// Ancestor node ids live in a 16-entry per-thread array (local memory).
+__device__ __forceinline__ uint32_t first_node(const float t0[3], const float tm[3]) {
+    uint32_t a = 0;
+    if (t0[0] > t0[1]) {
+        if (t0[0] > t0[2]) {
+            if (tm[1] < t0[0]) a |= 2;
+            if (tm[2] < t0[0]) a |= 1;
+            return a;
+        }
+    } else {
+        if (t0[1] > t0[2]) {
+            if (tm[0] < t0[1]) a |= 4;
+            if (tm[2] < t0[1]) a |= 1;
+            return a;
+        }
+    }
+    if (tm[0] < t0[2]) a |= 4;
+    if (tm[1] < t0[2]) a |= 2;
+    return a;
+}
+
+__device__ __forceinline__ uint32_t next_node(const float t[3], uint32_t x, uint32_t y, uint32_t z) {
+    if (t[0] < t[1]) {
+        if (t[0] < t[2]) return x;
+    } else {
+        if (t[1] < t[2]) return y;
+    }
+    return z;
+}
+
+__device__ __forceinline__ uint32_t child_entry(const DevScene &S, uint32_t node, uint32_t slot) {
+    const uint32_t *c = reinterpret_cast<const uint32_t *>(S.child) + 8u * node + slot;
+    return __ldg(c);
+}
+
+struct Trav {
+    float t0r[3], t1r[3];
+    float t0[3], t1[3];
+    uint64_t slots, tns;
+    uint32_t a, node, tn;
+    int l;
+    bool active;
+};
+
+__device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const float ro[3], const float rd[3],
+                                          Count &cnt) {
+    float ros[3], rds[3];
+    for (int k = 0; k < 3; ++k) {
+        ros[k] = (ro[k] - S.root_ce[k]) + S.root_ce[3];
+        rds[k] = rd[k];
+    }
+    uint32_t a = 0;
+    if (rds[0] < 0.0f) { ros[0] = 2.0f * S.root_ce[3] - ros[0]; rds[0] = -rds[0]; a |= 4; }
+    if (rds[1] < 0.0f) { ros[1] = 2.0f * S.root_ce[3] - ros[1]; rds[1] = -rds[1]; a |= 2; }
+    if (rds[2] < 0.0f) { ros[2] = 2.0f * S.root_ce[3] - ros[2]; rds[2] = -rds[2]; a |= 1; }
+    const float mx = 2.0f * S.root_ce[3];
+    for (int k = 0; k < 3; ++k) {
+        T.t0r[k] = (0.0f - ros[k]) / rds[k];
+        T.t1r[k] = (mx - ros[k]) / rds[k];
+    }
+    T.a = a;
+    T.active = std_max(std_max(T.t0r[0], T.t0r[1]), T.t0r[2]) < std_min(std_min(T.t1r[0], T.t1r[1]), T.t1r[2]);
+    if (T.active && (T.t1r[0] < 0.0f || T.t1r[1] < 0.0f || T.t1r[2] < 0.0f)) T.active = false;
+    if (T.active) {
+        ++cnt.node_visits;  // the root is examined; it is never a leaf (depth >= 2)
+        T.l = 0;
+        T.node = 0;
+        T.slots = 0;
+        T.tns = 0;
+        float tm[3];
+        for (int k = 0; k < 3; ++k) {
+            T.t0[k] = T.t0r[k];
+            T.t1[k] = T.t1r[k];
+            tm[k] = 0.5f * (T.t0[k] + T.t1[k]);
+        }
+        T.tn = first_node(T.t0, tm);
+    }
+}
+
+__device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
+                                          float &tra, float &trb, Count &cnt) {
+    if (!T.active) return false;
+    for (;;) {
+        if (T.tn >= 8) {
+            if (T.l == 0) {
+                T.active = false;
+                return false;
+            }
+            const int l = T.l - 1;
+            T.l = l;
+            T.node = nstack[l];
+            T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
+            float t0[3] = {T.t0r[0], T.t0r[1], T.t0r[2]}, t1[3] = {T.t1r[0], T.t1r[1], T.t1r[2]};
+            for (int k = 0; k < l; ++k) {
+                const uint32_t s = (uint32_t)(T.slots >> (3 * k)) & 7u;
+                const float mx = 0.5f * (t0[0] + t1[0]), my = 0.5f * (t0[1] + t1[1]), mz = 0.5f * (t0[2] + t1[2]);
+                if (s & 4) t0[0] = mx; else t1[0] = mx;
+                if (s & 2) t0[1] = my; else t1[1] = my;
+                if (s & 1) t0[2] = mz; else t1[2] = mz;
+            }
+            for (int k = 0; k < 3; ++k) {
+                T.t0[k] = t0[k];
+                T.t1[k] = t1[k];
+            }
+            continue;
+        }
+        const uint32_t tn = T.tn;
+        float tm[3], c0[3], c1[3];
+        for (int k = 0; k < 3; ++k) tm[k] = 0.5f * (T.t0[k] + T.t1[k]);
+        const bool bx = tn & 4, by = tn & 2, bz = tn & 1;
+        c0[0] = bx ? tm[0] : T.t0[0]; c1[0] = bx ? T.t1[0] : tm[0];
+        c0[1] = by ? tm[1] : T.t0[1]; c1[1] = by ? T.t1[1] : tm[1];
+        c0[2] = bz ? tm[2] : T.t0[2]; c1[2] = bz ? T.t1[2] : tm[2];
+        T.tn = (tn == 7) ? 8u : next_node(c1, bx ? 8u : (tn | 4u), by ? 8u : (tn | 2u), bz ? 8u : (tn | 1u));
+        // nla = {0,4,2,6,1,5,3,7}: reverse the three child bits
+        const uint32_t m = tn ^ T.a;
+        const uint32_t slot = ((m & 1u) << 2) | (m & 2u) | ((m >> 2) & 1u);
+        const uint32_t child = child_entry(S, T.node, slot);
+        if (c1[0] < 0.0f || c1[1] < 0.0f || c1[2] < 0.0f || child == 0u) continue;
+        ++cnt.node_visits;
+        if (child & kLeafBit) {
+            leaf = child & ~kLeafBit;
+            tra = std_max(std_max(c0[0], c0[1]), c0[2]);
+            trb = std_min(std_min(c1[0], c1[1]), c1[2]);
+            return true;
+        }
+        const int l = T.l;
+        if (l + 1 >= kMaxDepth - 1) {  // an internal node at level 15 has no stack room (reference limit)
+            T.active = false;
+            ++cnt.gave_up;
+            return false;
+        }
+        nstack[l] = T.node;
+        T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
+        T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));
+        T.l = l + 1;
+        T.node = child;
+        for (int k = 0; k < 3; ++k) {
+            T.t0[k] = c0[k];
+            T.t1[k] = c1[k];
+            tm[k] = 0.5f * (c0[k] + c1[k]);
+        }
+        T.tn = first_node(T.t0, tm);
+    }
+}
+
+// ---- brick lookup: SampleVoxelSpace, src/kernel.cpp:96-126 ----------------
+__device__ __forceinline__ float sample_voxel_space(const float p[3], const float *__restrict__ v, const float4 ce) {
+    const float nm1 = (float)kLvox - 1.0f;
+    const float top = (float)(kLvox - 1);
+    const float cc[3] = {ce.x, ce.y, ce.z};
+    uint32_t ia[3], ib[3];
+    float nl[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float ni = ((-0.5f * ((cc[k] - ce.w) - p[k])) * nm1) / ce.w;
+        float nf = sse_max(floorf(ni), 0.0f);
+        float nc = sse_min(ceilf(ni), nm1);
+        nl[k] = ni - nf;
+        nc = sse_max(sse_min(nc, top), 0.0f);
+        nf = sse_max(sse_min(nf, top), 0.0f);
+        ia[k] = (uint32_t)nf;
+        ib[k] = (uint32_t)nc;
+    }
+    const uint32_t za = ia[2] * 64u, zb = ib[2] * 64u, ya = ia[1] * 8u, yb = ib[1] * 8u;
+    const float u0 = lerp_ref(__ldg(v + za + ya + ia[0]), __ldg(v + za + ya + ib[0]), nl[0]);
+    const float u1 = lerp_ref(__ldg(v + za + yb + ia[0]), __ldg(v + za + yb + ib[0]), nl[0]);
+    const float u2 = lerp_ref(__ldg(v + zb + ya + ia[0]), __ldg(v + zb + ya + ib[0]), nl[0]);
+    const float u3 = lerp_ref(__ldg(v + zb + yb + ia[0]), __ldg(v + zb + yb + ib[0]), nl[0]);
+    const float v0 = lerp_ref(u0, u1, nl[1]);
+    const float v1 = lerp_ref(u2, u3, nl[1]);
+    return lerp_ref(v0, v1, nl[2]);
+}
+
+// ---- phase function: MiePhase, src/KernelSampler.cpp:214-285 --------------
+// Tables staged in shared memory: pdf as float4 (r, g, b, -), red CDF.
+struct MieSmem {
+    float4 *pdf;
+    float *cdf;
+    uint32_t n;
+};
+
+__device__ __forceinline__ float3 mie_eval_rgb(const MieSmem &M, float ct) {
+    float ct1 = sse_max(sse_min(ct, 1.0f), -1.0f);
+    float a = acos_ref(0.0f - ct1) / kPi;
+    float b = (float)M.n * a;
+    float c = floorf(b);
+    c = sse_min(c, (float)(M.n - 2));
+    c = sse_max(c, 0.0f);
+    const float t = b - c;
+    const uint32_t X = (uint32_t)c;
+    const float4 pa = M.pdf[X], pb = M.pdf[X + 1];
+    return make_float3(lerp_ref(pa.x, pb.x, t), lerp_ref(pa.y, pb.y, t), lerp_ref(pa.z, pb.z, t));
+}
+
+__device__ __forceinline__ float mie_scan_cdf(const MieSmem &M, float ub, uint32_t i, float &t_out) {
+    float b = sse_max(ub, (float)i);
+    float c = sse_min(floorf(b), (float)(M.n - 1));
+    float t = b - c;
+    t_out = t;
+    return lerp_ref(M.cdf[i], M.cdf[i + 1], t);
+}
+
+// The reference scans i = 0..n-2 and keeps the last step whose interpolated
+// CDF is below u1; the predicate is non-decreasing in i, so bisection finds
+// the same step in log2(n) probes.
+__device__ __forceinline__ float mie_theta_ref(const MieSmem &M, float u1) {
+    const float ub = (float)M.n * u1;
+    uint32_t lo = 0, hi = M.n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        float t;
+        if (mie_scan_cdf(M, ub, mid, t) < u1) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0) return 0.0f;
+    float t;
+    (void)mie_scan_cdf(M, ub, lo - 1, t);
+    return (float)(lo - 1) / (float)M.n + t / (float)M.n;
+}
+
+// SamplingBasis, src/KernelSampler.cpp:145-154, and the direction composition
+__device__ __forceinline__ void compose_dir(const float iv[3], float st, float ct, float ph, float out[3]) {
+    const float len = sqrtf(iv[0] * iv[0] + 0.0f * 0.0f + iv[2] * iv[2]);
+    const float b1[3] = {(0.0f - iv[2]) / len, 0.0f / len, iv[0] / len};
+    const float b2[3] = {iv[1] * b1[2] - iv[2] * b1[1], iv[2] * b1[0] - iv[0] * b1[2], iv[0] * b1[1] - iv[1] * b1[0]};
+    float sph, cph;
+    dsincos(ph, &sph, &cph);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = ((b1[k] * st) * cph + (b2[k] * st) * sph) + iv[k] * ct;
+}
+
+__device__ __forceinline__ void mie_sample(const MieSmem &M, const float iv[3], float u1, float u2, float out[3]) {
+    const float th = mie_theta_ref(M, u1) * kPi;
+    const float ph = (2.0f * kPi) * u2;
+    float s_, c_;
+    dsincos(th, &s_, &c_);
+    const float ct = -c_;
+    const float st = sqrtf(sse_max(1.0f - ct * ct, 0.0f));
+    compose_dir(iv, st, ct, ph, out);
+}
+
+// ---- sun: SunLight, src/KernelSampler.cpp:318-345 --------------------------
+__device__ __forceinline__ float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+__device__ __forceinline__ bool sun_hit(const DevParams &P, const float v[3]) {
+    return dot3(v, P.sun_dir) > P.sun_cos;
+}
+
+__device__ __forceinline__ void sun_sample(const DevParams &P, float u1, float u2, float out[3]) {
+    const float ctm = P.sun_cos;
+    const float ct = (1.0f - u1) + u1 * ctm;
+    const float st = sqrtf(1.0f - ct * ct);
+    const float ph = (2.0f * kPi) * u2;
+    compose_dir(P.sun_dir, st, ct, ph, out);
+}
+
+// ---- Hosek-Wilkie sky radiance as the reference evaluates it (src/kernel.cpp:329-360)
+__device__ __forceinline__ float3 sky_eval(const DevParams &P, const float rd[3]) {
+    const float *sd = P.sun_dir;
+    const float rdz = rd[2];
+    const float sth = sqrtf(1.0f - rd[2] * rd[2]);
+    const float cth = rdz;
+    const float slth = sqrtf(1.0f - sd[2] * sd[2]);
+    const float clth = sd[2];
+    const float slph = sd[1];
+    const float clph = sd[0];
+    const float rdd = rd[0] / rd[1];
+    const float acr = 1.0f / sqrtf(rdd * rdd + 1.0f);
+    const float czp = acr * (rdd * slph + clph);
+    const float cph = (sth * slth) * czp + cth * clth;
+    const float gmma = acos_ref(cph);
+    const float gacs = sse_max(sse_min(cph, 1.0f), 0.0f);
+    const float thcs = sse_max(rdz, 0.0f);
+    const float raym = gacs * gacs;
+    float out[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float *c = P.sky_cfg[i];
+        const float expm = dexp(c[4] * gmma);
+        const float miem = (1.0f + raym) / dpow((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs, 1.5f);
+        const float zenh = sqrtf(thcs);
+        float ca = (1.0f + c[0] * dexp(c[1] / (thcs + 0.01f))) *
+                   ((((c[2] + c[3] * expm) + c[5] * raym) + c[6] * miem) + c[7] * zenh);
+        ca = ca * P.sky_rad[i];
+        out[i] = 1e-3f * dpow(ca, 2.2f);
+    }
+    return make_float3(out[0], out[1], out[2]);
+}
+
+// ---- camera ray, K_ParallelRender (src/kernel.cpp:461-474) -----------------
+__device__ __forceinline__ bool camera_ray(const DevParams &P, uint32_t px, uint32_t py, float ro[3], float rd[3]) {
+    const float hx = 0.0f - (((2.0f * ((float)px + 0.5f)) / (float)P.w) - 1.0f);
+    const float hy = 0.0f - (((2.0f * ((float)py + 0.5f)) / (float)P.h) - 1.0f);
+    const float *V = P.viewi, *Q = P.proji;
+    float rv[3], d[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) rv[k] = ((hx * Q[k] + hy * Q[4 + k]) + 0.0f * Q[8 + k]) + 1.0f * Q[12 + k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = ((rv[0] * V[k] + rv[1] * V[4 + k]) + rv[2] * V[8 + k]) + 0.0f * V[12 + k];
+    const float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        rd[k] = d[k] / len;
+        ro[k] = V[12 + k];
+    }
+    return (hx > -1.0f && hx < 1.0f) && (hy > -1.0f && hy < 1.0f);
+}
+
+// ---- free-flight tracking of one segment (src/kernel.cpp:197-317) ----------
+// Returns true when the segment leaves the volume without a real collision;
+// td receives the distance of the collision (or of the last leaf exit).
+__device__ __forceinline__ bool track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
+                                      Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
+    Trav T;
+    trav_init(T, S, ro, rd, cnt);
+    ++cnt.vertices;
+    float td = 0.0f;
+    uint32_t leaf;
+    float tra, trb;
+    uint32_t budget = kStepBudget;
+    while (trav_next(T, S, nstack, leaf, tra, trb, cnt)) {
+        if (!(td < depth)) break;
+        const float4 ce = __ldg(&S.leaf[2 * leaf]);
+        const float4 meta = __ldg(&S.leaf[2 * leaf + 1]);
+        const float smax = meta.x;
+        const float *brick = S.bricks + (size_t)__float_as_uint(meta.y) * kBrick;
+        const float lo = td;
+        const float tr0 = tra - td, tr1 = trb - td;
+        // src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
+        // fog leaves, so the masked selects are bitwise blends: past the leaf
+        // entry, td keeps all but its lowest bit and s0 becomes the lowest bit
+        // of tr0 (0 or the smallest denormal).
+        float s0;
+        if (tra > td) {
+            td = tra;
+            s0 = tr0;
+        } else {
+            td = __uint_as_float((__float_as_uint(td) & ~1u) | (__float_as_uint(tra) & 1u));
+            s0 = __uint_as_float(__float_as_uint(tr0) & 1u);
+        }
+        const float denom = P.sigma_e * smax;
+        float sr = -dlog(g.uniform()) / denom;
+        for (;;) {
+            const float sc = s0 + sr;
+            td = lo + sc;
+            if (!(sc < tr1)) {
+                td = trb;
+                break;
+            }
+            bool rm = sc > tr0;
+            float rho = -1.0f;
+            if (rm) {
+                const float rc[3] = {ro[0] + rd[0] * td, ro[1] + rd[1] * td, ro[2] + rd[2] * td};
+                rho = sample_voxel_space(rc, brick, ce);
+                ++cnt.density_lookups;
+            }
+            const float q = g.uniform();
+            rm = rm && (rho / smax < q);
+            if (!rm) {
+                td_out = td;
+                return false;
+            }
+            if (--budget == 0) {
+                ++cnt.gave_up;
+                td_out = td;
+                return true;
+            }
+            sr = sr - dlog(g.uniform()) / denom;
+        }
+    }
+    td_out = td;
+    return true;
+}
+
+// ---- one camera path sample: SampleVolume recursion as a loop --------------
+// (src/kernel.cpp:128-445; see the CPU restatement for the derivation)
+__device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
+                                            uint32_t py, uint64_t seed, uint64_t sample, float4 &sun_acc,
+                                            float4 &sky_acc, uint32_t *nstack, Count &cnt) {
+    float ro[3], rd[3];
+    sun_acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    sky_acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!camera_ray(P, px, py, ro, rd)) return;
+    Rng g = rng_seed(seed, (uint64_t)py * P.w + px, sample);
+    const float f = P.albedo;
+    float T0 = 1.0f, T1 = 1.0f, T2 = 1.0f;
+    const float depth0 = P.depth ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
+    for (uint32_t r = 0;; ++r) {
+        float td;
+        const bool esc = track(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+        if (r == 0) sun_acc.w = sky_acc.w = esc ? 0.0f : 1.0f;
+        if (esc) {
+            if (r > 0) {
+                if (sun_hit(P, rd)) {
+                    sun_acc.x = sun_acc.x + T0 * P.sun_color[0];
+                    sun_acc.y = sun_acc.y + T1 * P.sun_color[1];
+                    sun_acc.z = sun_acc.z + T2 * P.sun_color[2];
+                } else {
+                    sun_acc.x = sun_acc.x + T0 * 0.0f;
+                    sun_acc.y = sun_acc.y + T1 * 0.0f;
+                    sun_acc.z = sun_acc.z + T2 * 0.0f;
+                }
+                const float3 sky = sky_eval(P, rd);
+                sky_acc.x = sky_acc.x + T0 * sky.x;
+                sky_acc.y = sky_acc.y + T1 * sky.y;
+                sky_acc.z = sky_acc.z + T2 * sky.z;
+            }
+            break;
+        }
+        if (r >= P.scattevs) break;
+        float srd[3], lrd[3], rc[3];
+        const float u1 = g.uniform(), u2 = g.uniform();
+        mie_sample(M, rd, u1, u2, srd);
+        const float u3 = g.uniform(), u4 = g.uniform();
+        sun_sample(P, u3, u4, lrd);
+        const float3 p1 = mie_eval_rgb(M, dot3(srd, rd));
+        const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
+        const float3 p3 = mie_eval_rgb(M, dot3(lrd, rd));
+        const float q1 = sun_hit(P, srd) ? P.sun_pdf : 0.0f;
+        cnt.mie_evals += 3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+        float tds;
+        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt)) {
+            const bool hit = sun_hit(P, lrd);
+            const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
+                        s2 = hit ? P.sun_color[2] : 0.0f;
+            sun_acc.x = sun_acc.x + (T0 * ((p3.x / (p3.x + p2)) * f)) * s0;
+            sun_acc.y = sun_acc.y + (T1 * ((p3.y / (p3.y + p2)) * f)) * s1;
+            sun_acc.z = sun_acc.z + (T2 * ((p3.z / (p3.z + p2)) * f)) * s2;
+        }
+        T0 = T0 * ((p1.x / (p1.x + q1)) * f);
+        T1 = T1 * ((p1.y / (p1.y + q1)) * f);
+        T2 = T2 * ((p1.z / (p1.z + q1)) * f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ro[k] = rc[k];
+            rd[k] = srd[k];
+        }
+    }
+}
+
+}  // namespace dr

@@ -1,0 +1,25 @@
+// Kernel launchers (host side, C++ linkage, internal to the library).
+#pragma once
+#include <cuda_runtime.h>
+#include "dr_internal.h"
+
+namespace dr {
+
+constexpr int kRenderBlock = 128;
+
+cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                               float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
+cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
+                              uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts, cudaStream_t st);
+cudaError_t launch_probe_density(const DevScene &S, const uint32_t *nodes, const float *pts, uint32_t n, float *out,
+                                 cudaStream_t st);
+cudaError_t launch_probe_paths(const DevScene &S, const DevParams &P, const void *mie_pack, const uint32_t *px,
+                               const uint32_t *py, const uint64_t *sample, uint32_t n, uint64_t seed,
+                               float4 *out_sun, float4 *out_sky, DevCounters *C, cudaStream_t st);
+cudaError_t launch_probe_sampler(const DevParams &P, const void *mie_pack, uint32_t what, const float *in, uint32_t n,
+                                 float *out, cudaStream_t st);
+cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
+                                       uint32_t n_rays, uint64_t nsamp, uint64_t seed, unsigned long long *escapes,
+                                       cudaStream_t st);
+
+}  // namespace dr

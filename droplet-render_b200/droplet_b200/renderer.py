@@ -1,0 +1,195 @@
+"""The plain single-frame renderer: RenderKernel on one B200.
+
+Mirrors the reference's RenderKernel (src/kernel.h:11-59):
+    Initialize(scene, ..., scattevs, sigma_s, sigma_a, tilex, tiley, w, h)
+        -> Renderer(device).upload(octree) + set_params(RenderSettings)
+    Render(x0, y0, tilew, tileh, samples) -> render_tile(...): sums over
+        `samples` path samples per pixel, sun buffer (phb[0]) and sky buffer
+        (phb[1]) as float4 tiles.
+All work runs in the native library on the GPU; there is no host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .scene import Octree
+from .sky import SkyState
+
+
+@dataclass
+class PhaseTable:
+    """Tabulated RGB phase function: pdf and CDF over the scattering angle,
+    index 0 = backscatter (the layout of src/KernelSampler.cpp:8-141)."""
+
+    pdf: np.ndarray  # (n, 3) float32
+    cdf: np.ndarray  # (n, 3) float32
+
+    @staticmethod
+    def load(path: str) -> "PhaseTable":
+        z = np.load(path)
+        return PhaseTable(np.ascontiguousarray(z["pdf"], np.float32), np.ascontiguousarray(z["cdf"], np.float32))
+
+
+@dataclass
+class RenderSettings:
+    sigma_s: float
+    sigma_a: float
+    scattevs: int
+    sun_dir: np.ndarray
+    sun_color: np.ndarray
+    sun_angle: float
+    sky: SkyState
+    phase: PhaseTable
+    viewi: np.ndarray
+    proji: np.ndarray
+    w: int
+    h: int
+    depth: np.ndarray | None = None
+    phase_mode: int = N.DR_PHASE_MIE_REFERENCE
+    _keep: list = field(default_factory=list, repr=False)
+
+    def to_c(self) -> N.DrRenderParams:
+        p = N.DrRenderParams()
+        p.sigma_s, p.sigma_a, p.scattevs = float(self.sigma_s), float(self.sigma_a), int(self.scattevs)
+        p.sun_dir[:] = [float(v) for v in np.asarray(self.sun_dir, np.float32)]
+        p.sun_color[:] = [float(v) for v in np.asarray(self.sun_color, np.float32)]
+        p.sun_angle = float(self.sun_angle)
+        for i in range(3):
+            p.sky_configs[i][:] = [float(v) for v in self.sky.configs[i]]
+        p.sky_radiances[:] = [float(v) for v in self.sky.radiances]
+        pdf = np.ascontiguousarray(self.phase.pdf, np.float32)
+        cdf = np.ascontiguousarray(self.phase.cdf, np.float32)
+        self._keep = [pdf, cdf]
+        p.mie_pdf, p.mie_cdf, p.mie_n = pdf.ctypes.data, cdf.ctypes.data, len(pdf)
+        p.phase_mode = int(self.phase_mode)
+        p.viewi[:] = [float(v) for v in np.asarray(self.viewi, np.float32).ravel()]
+        p.proji[:] = [float(v) for v in np.asarray(self.proji, np.float32).ravel()]
+        p.w, p.h = int(self.w), int(self.h)
+        if self.depth is not None:
+            d = np.ascontiguousarray(self.depth, np.float32).reshape(-1)
+            if d.size != self.w * self.h:
+                raise ValueError("depth must hold w*h values")
+            self._keep.append(d)
+            p.depth = d.ctypes.data
+        else:
+            p.depth = None
+        return p
+
+
+class Renderer:
+    def __init__(self, device: int = 0):
+        self._ctx = C.c_void_p()
+        N.check(N.lib().dr_create(int(device), C.byref(self._ctx)))
+        self.device = device
+        self.sample_base = 0
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._ctx
+
+    def close(self):
+        if self._ctx:
+            N.lib().dr_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, oc: Octree):
+        nodes = np.ascontiguousarray(oc.nodes)
+        bricks = np.ascontiguousarray(oc.bricks, np.float32)
+        d = N.DrSceneDesc(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+        N.check(N.lib().dr_upload_scene(self._ctx, C.byref(d)))
+
+    def set_params(self, s: RenderSettings):
+        p = s.to_c()
+        N.check(N.lib().dr_set_params(self._ctx, C.byref(p)))
+        self.settings = s
+
+    def render_tile(self, x0: int, y0: int, tw: int, th: int, spp: int, seed: int = 0, sample_base: int | None = None):
+        """Sums over `spp` samples: (sun, sky) arrays of shape (th, tw, 4).  Without an
+        explicit sample_base each call continues the stream (new, independent samples)."""
+        base = self.sample_base if sample_base is None else int(sample_base)
+        sun = np.zeros((th, tw, 4), np.float32)
+        sky = np.zeros((th, tw, 4), np.float32)
+        N.check(N.lib().dr_render_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, sun.ctypes.data,
+                                       sky.ctypes.data))
+        if sample_base is None:
+            self.sample_base += spp
+        return sun, sky
+
+    def render_tile_async(self, x0, y0, tw, th, spp, seed, sample_base, sun_dev_ptr: int, sky_dev_ptr: int,
+                          stream_ptr: int = 0):
+        N.check(N.lib().dr_render_tile_async(self._ctx, x0, y0, tw, th, spp, int(seed), int(sample_base),
+                                             C.c_void_p(sun_dev_ptr), C.c_void_p(sky_dev_ptr),
+                                             C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def synchronize(self):
+        N.check(N.lib().dr_synchronize(self._ctx))
+
+    def counters(self) -> dict:
+        c = N.DrCounters()
+        N.check(N.lib().dr_get_counters(self._ctx, C.byref(c)))
+        return c.as_dict()
+
+    def reset_counters(self):
+        N.check(N.lib().dr_reset_counters(self._ctx))
+
+    # ---- parity probes ---------------------------------------------------------
+    def probe_leaf_sequence(self, ro, rd, maxn: int = 256):
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        n = len(ro)
+        nodes = np.zeros((n, maxn), np.uint32)
+        a = np.zeros((n, maxn), np.float32)
+        b = np.zeros((n, maxn), np.float32)
+        cnt = np.zeros(n, np.uint32)
+        N.check(N.lib().dr_probe_leaf_sequence(self._ctx, ro.ctypes.data, rd.ctypes.data, n, maxn, nodes.ctypes.data,
+                                               a.ctypes.data, b.ctypes.data, cnt.ctypes.data))
+        return nodes, a, b, cnt
+
+    def probe_density(self, leaf_nodes, points):
+        leaf_nodes = np.ascontiguousarray(leaf_nodes, np.uint32)
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.float32)
+        N.check(N.lib().dr_probe_density(self._ctx, leaf_nodes.ctypes.data, pts.ctypes.data, len(pts),
+                                         out.ctypes.data))
+        return out
+
+    def probe_paths(self, px, py, sample, seed: int):
+        px = np.ascontiguousarray(px, np.uint32)
+        py = np.ascontiguousarray(py, np.uint32)
+        sm = np.ascontiguousarray(sample, np.uint64)
+        n = len(px)
+        a = np.zeros((n, 4), np.float32)
+        b = np.zeros((n, 4), np.float32)
+        N.check(N.lib().dr_probe_paths(self._ctx, px.ctypes.data, py.ctypes.data, sm.ctypes.data, n, int(seed),
+                                       a.ctypes.data, b.ctypes.data))
+        return a, b
+
+    def probe_sampler(self, what: int, inputs: np.ndarray, n: int):
+        x = np.ascontiguousarray(inputs, np.float32).reshape(-1)
+        out = np.zeros(n if what == N.DR_PROBE_MIE_THETA else 3 * n, np.float32)
+        N.check(N.lib().dr_probe_sampler(self._ctx, int(what), x.ctypes.data, int(n), out.ctypes.data))
+        return out if what == N.DR_PROBE_MIE_THETA else out.reshape(n, 3)
+
+    def probe_transmittance(self, ro, rd, nsamp: int, seed: int = 0):
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        out = np.zeros(len(ro), np.float64)
+        N.check(N.lib().dr_probe_transmittance(self._ctx, ro.ctypes.data, rd.ctypes.data, len(ro), int(nsamp),
+                                               int(seed), out.ctypes.data))
+        return out

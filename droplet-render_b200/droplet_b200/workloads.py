@@ -1,0 +1,276 @@
+"""Seeded synthetic density fields for the benchmark and tests.
+
+Recipe (one "puff"): density(p) = max(0, 1 - |p - c| / R) * fBm(p), where fBm
+is 4-octave gradient noise (base frequency 4, lacunarity 2, gain 0.5, amp 1)
+and the total is clamped to [0, 1].  The noise is Perlin's improved gradient
+noise (Perlin 2002: quintic fade, 12 cube-edge gradients selected by the low
+hash bits); its "seed" selects the permutation table, drawn with
+numpy.random.default_rng(seed).permutation(256).  Voxel (i, j, k) of an n^3
+grid on the unit cube sits at world (i, j, k) / n, as the reference's
+uniform-scale transform places it.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def perm_table(seed: int) -> np.ndarray:
+    p = np.random.default_rng(seed).permutation(256).astype(np.int64)
+    return np.concatenate([p, p])
+
+
+def _fade(t):
+    return t * t * t * (t * (t * 6.0 - 15.0) + 10.0)
+
+
+def _grad(h, x, y, z):
+    h = h & 15
+    u = np.where(h < 8, x, y)
+    v = np.where(h < 4, y, np.where((h == 12) | (h == 14), x, z))
+    return np.where(h & 1, -u, u) + np.where(h & 2, -v, v)
+
+
+def perlin(x, y, z, perm):
+    """Improved gradient noise at float64 points (arrays of one shape)."""
+    xf, yf, zf = np.floor(x), np.floor(y), np.floor(z)
+    X = xf.astype(np.int64) & 255
+    Y = yf.astype(np.int64) & 255
+    Z = zf.astype(np.int64) & 255
+    x, y, z = x - xf, y - yf, z - zf
+    u, v, w = _fade(x), _fade(y), _fade(z)
+    A = perm[X] + Y
+    AA = perm[A] + Z
+    AB = perm[A + 1] + Z
+    B = perm[X + 1] + Y
+    BA = perm[B] + Z
+    BB = perm[B + 1] + Z
+
+    def lerp(t, a, b):
+        return a + t * (b - a)
+
+    return lerp(
+        w,
+        lerp(v, lerp(u, _grad(perm[AA], x, y, z), _grad(perm[BA], x - 1, y, z)),
+             lerp(u, _grad(perm[AB], x, y - 1, z), _grad(perm[BB], x - 1, y - 1, z))),
+        lerp(v, lerp(u, _grad(perm[AA + 1], x, y, z - 1), _grad(perm[BA + 1], x - 1, y, z - 1)),
+             lerp(u, _grad(perm[AB + 1], x, y - 1, z - 1), _grad(perm[BB + 1], x - 1, y - 1, z - 1))),
+    )
+
+
+def fbm(x, y, z, seed: int, octaves: int = 4, freq: float = 4.0, lacunarity: float = 2.0, gain: float = 0.5):
+    perm = perm_table(seed)
+    s = np.zeros_like(x)
+    amp = 1.0
+    for _ in range(octaves):
+        s += amp * perlin(x * freq, y * freq, z * freq, perm)
+        freq *= lacunarity
+        amp *= gain
+    return s
+
+
+@dataclass
+class Puff:
+    center: tuple
+    radius: float
+    seed: int
+
+
+@dataclass
+class FieldRecipe:
+    n: int                       # grid edge (voxels)
+    puffs: list = field(default_factory=list)
+    extent: tuple = (1.0, 1.0, 1.0)  # fraction of the unit cube covered per axis (slabs)
+
+    @property
+    def voxel_size(self) -> float:
+        return 1.0 / self.n
+
+
+def config0_recipe(n: int = 64, seed: int = 1) -> FieldRecipe:
+    """Single puff at the cube centre, radius 0.4."""
+    return FieldRecipe(n, [Puff((0.5, 0.5, 0.5), 0.4, seed)])
+
+
+def cumulus_recipe(n: int = 512) -> FieldRecipe:
+    """The config-0 puff plus three offset, scaled copies (radii 0.15-0.3, seeds 2-4)."""
+    return FieldRecipe(
+        n,
+        [
+            Puff((0.5, 0.5, 0.5), 0.4, 1),
+            Puff((0.3, 0.42, 0.58), 0.25, 2),
+            Puff((0.72, 0.56, 0.54), 0.22, 3),
+            Puff((0.52, 0.38, 0.74), 0.15, 4),
+        ],
+    )
+
+
+# Scene setup shared by the configurations: camera 2.5 units from the cube
+# centre with a 40 degree vertical field of view, sun at 30 degrees elevation
+# (white, intensity 1 and cone half-angle 0.010 rad, the reference UI
+# defaults, addon/panel.py:360-362), Hosek sky with turbidity 3 and ground
+# albedo 0.3.
+CENTER = (0.5, 0.5, 0.5)
+CAMERA = {"distance": 2.5, "azimuth": -90.0, "elevation": 10.0, "fov": 40.0}
+SUN = {"elevation": 30.0, "azimuth": 30.0, "color": (1.0, 1.0, 1.0), "angle": 0.010}
+SKY = {"turbidity": 3.0, "albedo": 0.3}
+MEDIA = {
+    "c0": {"sigma_t": 20.0, "albedo": 0.99, "scattevs": 8},
+    "c1": {"sigma_t": 60.0, "albedo": 0.999, "scattevs": 64},
+}
+
+
+def medium(name: str):
+    """(sigma_s, sigma_a, scattevs) in binary32 for a named configuration."""
+    m = MEDIA[name]
+    st = np.float32(m["sigma_t"])
+    ss = np.float32(m["sigma_t"] * m["albedo"])
+    return float(ss), float(np.float32(st - ss)), int(m["scattevs"])
+
+
+def eval_blocks_numpy(recipe: FieldRecipe, block_origins: np.ndarray, chunk: int = 2048) -> np.ndarray:
+    """Density of 8^3 blocks (x fastest) at the given block origins; float32."""
+    o_all = np.asarray(block_origins, np.int64).reshape(-1, 3)
+    if len(o_all) > chunk:
+        return np.concatenate([eval_blocks_numpy(recipe, o_all[c:c + chunk], chunk)
+                               for c in range(0, len(o_all), chunk)])
+    s = recipe.voxel_size
+    o = o_all
+    k, j, i = np.meshgrid(np.arange(8), np.arange(8), np.arange(8), indexing="ij")
+    ii = (o[:, 0, None] + i.reshape(1, -1)).astype(np.float64)
+    jj = (o[:, 1, None] + j.reshape(1, -1)).astype(np.float64)
+    kk = (o[:, 2, None] + k.reshape(1, -1)).astype(np.float64)
+    x, y, z = ii * s, jj * s, kk * s
+    total = np.zeros_like(x)
+    for p in recipe.puffs:
+        r = np.sqrt((x - p.center[0]) ** 2 + (y - p.center[1]) ** 2 + (z - p.center[2]) ** 2)
+        env = np.maximum(0.0, 1.0 - r / p.radius)
+        m = env > 0
+        if m.any():
+            total[m] += env[m] * fbm(x[m], y[m], z[m], p.seed)
+    return np.clip(total, 0.0, 1.0).astype(np.float32)
+
+
+def eval_blocks_torch(recipe: FieldRecipe, block_origins: np.ndarray, device="cuda", chunk: int = 8192) -> np.ndarray:
+    """eval_blocks_numpy with torch float64 tensors (same operations in the same
+    order, so the same values), for building large fields quickly on a GPU."""
+    import torch
+
+    s = recipe.voxel_size
+    org_all = torch.as_tensor(np.asarray(block_origins, np.int64).reshape(-1, 3), device=device)
+    k, j, i = torch.meshgrid(torch.arange(8, device=device), torch.arange(8, device=device),
+                             torch.arange(8, device=device), indexing="ij")
+    i, j, k = i.reshape(1, -1), j.reshape(1, -1), k.reshape(1, -1)
+    perms = {p.seed: torch.as_tensor(perm_table(p.seed), device=device) for p in recipe.puffs}
+
+    def grad(h, x, y, z):
+        h = h & 15
+        u = torch.where(h < 8, x, y)
+        v = torch.where(h < 4, y, torch.where((h == 12) | (h == 14), x, z))
+        return torch.where((h & 1) != 0, -u, u) + torch.where((h & 2) != 0, -v, v)
+
+    def fade(t):
+        return t * t * t * (t * (t * 6.0 - 15.0) + 10.0)
+
+    def lerp(t, a, b):
+        return a + t * (b - a)
+
+    def perlin_t(x, y, z, perm):
+        xf, yf, zf = torch.floor(x), torch.floor(y), torch.floor(z)
+        X = xf.long() & 255
+        Y = yf.long() & 255
+        Z = zf.long() & 255
+        x, y, z = x - xf, y - yf, z - zf
+        u, v, w = fade(x), fade(y), fade(z)
+        A = perm[X] + Y
+        AA = perm[A] + Z
+        AB = perm[A + 1] + Z
+        B = perm[X + 1] + Y
+        BA = perm[B] + Z
+        BB = perm[B + 1] + Z
+        return lerp(w,
+                    lerp(v, lerp(u, grad(perm[AA], x, y, z), grad(perm[BA], x - 1, y, z)),
+                         lerp(u, grad(perm[AB], x, y - 1, z), grad(perm[BB], x - 1, y - 1, z))),
+                    lerp(v, lerp(u, grad(perm[AA + 1], x, y, z - 1), grad(perm[BA + 1], x - 1, y, z - 1)),
+                         lerp(u, grad(perm[AB + 1], x, y - 1, z - 1), grad(perm[BB + 1], x - 1, y - 1, z - 1))))
+
+    out = []
+    for c0 in range(0, org_all.shape[0], chunk):
+        o = org_all[c0:c0 + chunk]
+        x = (o[:, 0:1] + i).double() * s
+        y = (o[:, 1:2] + j).double() * s
+        z = (o[:, 2:3] + k).double() * s
+        total = torch.zeros_like(x)
+        for p in recipe.puffs:
+            r = torch.sqrt((x - p.center[0]) ** 2 + (y - p.center[1]) ** 2 + (z - p.center[2]) ** 2)
+            env = torch.clamp(1.0 - r / p.radius, min=0.0)
+            m = env > 0
+            if bool(m.any()):
+                xs, ys, zs = x[m], y[m], z[m]
+                acc = torch.zeros_like(xs)
+                amp, freq = 1.0, 4.0
+                for _ in range(4):
+                    acc += amp * perlin_t(xs * freq, ys * freq, zs * freq, perms[p.seed])
+                    freq *= 2.0
+                    amp *= 0.5
+                total[m] += env[m] * acc
+        out.append(torch.clamp(total, 0.0, 1.0).float().cpu().numpy())
+    return np.concatenate(out) if out else np.zeros((0, 512), np.float32)
+
+
+def sparse_field_fast(recipe: FieldRecipe):
+    """sparse_field using a CUDA device when torch sees one, numpy otherwise."""
+    try:
+        import torch
+
+        use_cuda = torch.cuda.is_available()
+    except Exception:
+        use_cuda = False
+    if not use_cuda:
+        return sparse_field(recipe)
+    org = candidate_blocks(recipe)
+    vals = eval_blocks_torch(recipe, org)
+    nz = (vals != 0).any(1)
+    return np.ascontiguousarray(org[nz]), np.ascontiguousarray(vals[nz])
+
+
+def candidate_blocks(recipe: FieldRecipe) -> np.ndarray:
+    """Origins of the 8^3 blocks that intersect any puff's bounding sphere."""
+    n, s = recipe.n, recipe.voxel_size
+    nb = (n + 7) // 8
+    g = np.arange(nb) * 8
+    bx, by, bz = np.meshgrid(g, g, g, indexing="ij")
+    org = np.stack([bx.ravel(), by.ravel(), bz.ravel()], -1)
+    keep = np.zeros(len(org), bool)
+    lo = org * s
+    hi = (org + 7) * s
+    for p in recipe.puffs:
+        c = np.asarray(p.center)
+        d = np.maximum(0.0, np.maximum(lo - c, c - hi))
+        keep |= np.sqrt((d ** 2).sum(-1)) < p.radius
+    return org[keep].astype(np.int32)
+
+
+def sparse_field(recipe: FieldRecipe):
+    """(block_origins int32 (B,3), block_values float32 (B,512)) of the non-empty blocks."""
+    org = candidate_blocks(recipe)
+    vals = eval_blocks_numpy(recipe, org) if len(org) else np.zeros((0, 512), np.float32)
+    nz = (vals != 0).any(1)
+    return np.ascontiguousarray(org[nz]), np.ascontiguousarray(vals[nz])
+
+
+def dense_to_blocks(grid: np.ndarray):
+    """Dense (nz, ny, nx) -> ... ; grid indexed [x, y, z] with shape multiple of 8."""
+    g = np.asarray(grid, np.float32)
+    nx, ny, nz = g.shape
+    px, py, pz = (-nx) % 8, (-ny) % 8, (-nz) % 8
+    if px or py or pz:
+        g = np.pad(g, ((0, px), (0, py), (0, pz)))
+    bx, by, bz = g.shape[0] // 8, g.shape[1] // 8, g.shape[2] // 8
+    b = g.reshape(bx, 8, by, 8, bz, 8).transpose(0, 2, 4, 5, 3, 1)  # (bx,by,bz, z, y, x)
+    b = b.reshape(bx * by * bz, 512)
+    ox, oy, oz = np.meshgrid(np.arange(bx) * 8, np.arange(by) * 8, np.arange(bz) * 8, indexing="ij")
+    org = np.stack([ox.ravel(), oy.ravel(), oz.ravel()], -1).astype(np.int32)
+    nzm = (b != 0).any(1)
+    return np.ascontiguousarray(org[nzm]), np.ascontiguousarray(b[nzm])

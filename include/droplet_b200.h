@@ -1,0 +1,178 @@
+/* droplet_b200 — B200 (sm_100a) implementation of droplet-render's volumetric
+ * path-tracing hot path, exposed as a plain C ABI (no CUDA or torch types).
+ *
+ * Each entry point names the reference interface it replaces.  The reference
+ * renderer is RenderKernel (src/kernel.h:11-59) driven from the CPython module
+ * libdroplet (src/main.cpp:64-771); its scene is the octree + 8^3 brick pool of
+ * class Scene (src/scene.h:146-159).
+ *
+ * Conventions
+ *  - Every function returns DR_OK (0) or a negative DR_ERR_* code; the text
+ *    of the last error on the calling thread is returned by dr_last_error().
+ *  - Host pointers unless a name ends in _dev; a stream argument is a
+ *    cudaStream_t passed as void* (NULL = the context's own stream).
+ *  - Images are float4 per pixel (r, g, b, alpha), row-major within a tile.
+ */
+#ifndef DROPLET_B200_H
+#define DROPLET_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DR_OK 0
+#define DR_ERR_INVALID (-1)   /* bad argument or descriptor */
+#define DR_ERR_CUDA (-2)      /* CUDA runtime failure (message has the CUDA error) */
+#define DR_ERR_STATE (-3)     /* call out of order (no scene, no parameters, busy) */
+#define DR_ERR_NOMEM (-4)     /* host or device allocation failed */
+#define DR_ERR_GAVE_UP (-5)   /* a kernel hit its iteration budget and stopped */
+#define DR_ERR_NODEVICE (-6)  /* no CUDA device */
+
+#define DR_NONE 0xffffffffu
+
+/* Octree node record, identical to the reference's OctreeStructure
+ * (src/scene.h:21-31): 64 bytes. */
+typedef struct {
+    float ce[4];        /* center x, y, z; half extent */
+    uint32_t chn[8];    /* child node index, 0 = none; child i sits at offset (i&1, i>>1&1, i>>2) */
+    uint32_t volx[2];   /* brick index in the [SDF, FOG] pools or DR_NONE */
+    float qval[2];      /* per-leaf query value; FOG: max density (majorant), floor 0.01 */
+} dr_node;
+
+/* A built scene: what Scene::Initialize leaves in Scene::ob / Scene::pvol
+ * (src/scene.cpp:840-917). */
+typedef struct {
+    dr_node *nodes;
+    uint32_t n_nodes;
+    float *bricks;      /* FOG brick pool: n_leaves * lvoxc^3 floats, x fastest */
+    uint32_t n_leaves;
+    uint32_t lvoxc;     /* samples per brick edge (8) */
+    uint32_t mlevel;    /* octree depth; leaves sit at level mlevel-1 */
+} dr_octree;
+
+/* Scene description handed to dr_upload_scene (same fields as dr_octree). */
+typedef struct {
+    const dr_node *nodes;
+    uint32_t n_nodes;
+    const float *bricks;
+    uint32_t n_leaves;
+    uint32_t lvoxc;
+} dr_scene_desc;
+
+#define DR_PHASE_MIE_REFERENCE 0u  /* the reference's tabulated sampler (src/KernelSampler.cpp:257-285) */
+#define DR_PHASE_MIE_EXACT 1u      /* exact inverse CDF of the tabulated phase x sin(theta) */
+
+/* Everything RenderKernel::Initialize receives (src/kernel.cpp:497-534) plus
+ * the sun light (src/main.cpp:374-404) and the sky state the reference
+ * hard-codes (src/kernel.cpp:521-526). */
+typedef struct {
+    float sigma_s, sigma_a;        /* macroscopic cross sections (msigmas, msigmaa) */
+    uint32_t scattevs;             /* max scattering events */
+    float sun_dir[3];              /* unit vector towards the sun */
+    float sun_color[3];            /* colour * intensity */
+    float sun_angle;               /* cone half angle, radians */
+    double sky_configs[3][9];      /* cooked Hosek-Wilkie RGB state (ArHosekSkyModelState.configs) */
+    double sky_radiances[3];       /* ArHosekSkyModelState.radiances */
+    const float *mie_pdf;          /* mie_n RGB entries, index 0 = backscatter */
+    const float *mie_cdf;          /* mie_n RGB entries */
+    uint32_t mie_n;                /* 256 for the reference table; 2..4096 */
+    uint32_t phase_mode;           /* DR_PHASE_* */
+    float viewi[16];               /* inverse view matrix, rows r[0..3] */
+    float proji[16];               /* inverse projection matrix, rows r[0..3] */
+    uint32_t w, h;                 /* full image size */
+    const float *depth;            /* optional w*h compositing depth (KERNEL_DEPTHCOMP), or NULL */
+} dr_render_params;
+
+/* In-kernel counters accumulated over all launches since the last reset. */
+typedef struct {
+    uint64_t paths;            /* camera path samples started */
+    uint64_t vertices;         /* traced segments: camera + continuation + shadow */
+    uint64_t node_visits;      /* octree node records examined */
+    uint64_t density_lookups;  /* trilinear brick lookups */
+    uint64_t mie_evals;        /* phase table evaluations and samples */
+    uint64_t gave_up;          /* paths stopped by the iteration budget */
+} dr_counters;
+
+typedef struct dr_ctx dr_ctx;
+
+/* ---- library ------------------------------------------------------------- */
+int dr_version(void);
+const char *dr_last_error(void);
+int dr_device_count(int *count);
+
+/* ---- context: replaces the module globals gpkernel/gpscene (src/main.cpp:16-18) */
+int dr_create(int device, dr_ctx **out);
+int dr_destroy(dr_ctx *ctx);                 /* DRE_EndRender, src/main.cpp:688-716 */
+
+/* ---- scene --------------------------------------------------------------- */
+/* Host octree build from sparse 8^3 blocks (OpenVDB-leaf shaped input):
+ * Scene::Initialize + S_Create leaf/octree/brick stages (src/scene.cpp:676-762,
+ * 840-908, BuildPath 267-305).  Voxel (i,j,k) sits at world (i,j,k)*voxel_size
+ * and is active when non-zero.  block_origin: 3 int32 per block, multiples of 8,
+ * non-negative; block_values: 512 floats per block (x fastest).  Free the
+ * result with dr_octree_free. */
+int dr_build_octree(const int32_t *block_origin, const float *block_values, uint32_t n_blocks, float voxel_size,
+                    uint32_t maxdepth, int nthreads, dr_octree *out);
+void dr_octree_free(dr_octree *oct);
+
+/* Copies nodes and bricks to the device (the reference reads Scene::ob/pvol
+ * in place, src/kernel.cpp:225-305). */
+int dr_upload_scene(dr_ctx *ctx, const dr_scene_desc *scene);
+
+/* ---- render settings: RenderKernel::Initialize (src/kernel.cpp:497-534) ---- */
+int dr_set_params(dr_ctx *ctx, const dr_render_params *params);
+
+/* Hosek-Wilkie state cook (src/ArHosekSkyModel.cpp:147-339) from the RGB
+ * dataset supplied by the caller: dataset_rgb[c] holds 2*10*6*9 doubles and
+ * dataset_rad[c] 2*10*6 doubles per channel c. */
+int dr_sky_cook(const double *const dataset_rgb[3], const double *const dataset_rad[3], double turbidity,
+                double albedo, double elevation, double configs[3][9], double radiances[3]);
+
+/* ---- render: RenderKernel::Render (src/kernel.cpp:536-567) ---------------- */
+/* Renders tile (x0, y0, tw, th) with spp samples per pixel and writes the SUMS
+ * over those samples into sun_out (phb[0]) and sky_out (phb[1]), tw*th float4
+ * each.  As in the reference only the even part of an odd tile is rendered
+ * (2x2 pixel blocks); pixels outside the image or not rendered are 0.
+ * Path (pixel p = py*w + px, sample s) draws from stream (seed, p, sample_base + s).
+ * Blocking; host buffers. */
+int dr_render_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
+                   uint64_t sample_base, float *sun_out, float *sky_out);
+/* Same on device buffers, enqueued on stream (NULL = context stream); returns
+ * without waiting. */
+int dr_render_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
+                         uint64_t seed, uint64_t sample_base, float *sun_out_dev, float *sky_out_dev, void *stream);
+/* Waits for all work on the context stream. */
+int dr_synchronize(dr_ctx *ctx);
+
+/* ---- counters ------------------------------------------------------------ */
+int dr_get_counters(dr_ctx *ctx, dr_counters *out);
+int dr_reset_counters(dr_ctx *ctx);
+
+/* ---- parity probes (test support; they run the same device code) --------- */
+/* Leaf sequence of one ray: node ids and (tr0, tr1); returns the count in *n.
+ * src/KernelOctree.cpp:230-349. */
+int dr_probe_leaf_sequence(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n_rays, uint32_t maxn,
+                           uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts);
+/* SampleVoxelSpace at n points inside leaf nodes[i] (src/kernel.cpp:96-126). */
+int dr_probe_density(dr_ctx *ctx, const uint32_t *nodes, const float *points, uint32_t n, float *out);
+/* Per-path sample (sun rgba, sky rgba) for n (px, py, sample) triples. */
+int dr_probe_paths(dr_ctx *ctx, const uint32_t *px, const uint32_t *py, const uint64_t *sample, uint32_t n,
+                   uint64_t seed, float *out_sun, float *out_sky);
+/* Phase / sun / sky evaluations for n directions (see DR_PROBE_*). */
+#define DR_PROBE_MIE_EVAL_RGB 0u   /* in: ct[n]            out: 3n */
+#define DR_PROBE_MIE_SAMPLE 1u     /* in: iv[3n],u1[n],u2[n] out: 3n */
+#define DR_PROBE_SUN_SAMPLE 2u     /* in: u1[n],u2[n]      out: 3n */
+#define DR_PROBE_SKY 3u            /* in: rd[3n]           out: 3n */
+#define DR_PROBE_MIE_THETA 4u      /* in: u1[n]            out: n (theta / pi) */
+int dr_probe_sampler(dr_ctx *ctx, uint32_t what, const float *in, uint32_t n, float *out);
+/* Fraction of nsamp delta-tracked segments along each ray that escape. */
+int dr_probe_transmittance(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,
+                           uint64_t seed, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,295 @@
+"""ctypes access to the two CPU checkers (TEST INFRASTRUCTURE ONLY)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libdroplet_ref.so")
+PORT_LIB = os.path.join(HERE, "_port", "liboracle_port.so")
+NODE_DTYPE = np.dtype([("ce", "<f4", 4), ("chn", "<u4", 8), ("volx", "<u4", 2), ("qval", "<f4", 2)])
+assert NODE_DTYPE.itemsize == 64
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def port_available() -> bool:
+    return os.path.exists(PORT_LIB)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("sigma_s", C.c_float), ("sigma_a", C.c_float), ("scattevs", C.c_uint32),
+        ("sun_dir", C.c_float * 3), ("sun_color", C.c_float * 3), ("sun_cos_angle", C.c_float),
+        ("sky_cfg", (C.c_float * 9) * 3), ("sky_rad", C.c_float * 3),
+        ("mie_pdf", C.c_void_p), ("mie_cdf", C.c_void_p), ("mie_n", C.c_uint32),
+        ("viewi", C.c_float * 16), ("proji", C.c_float * 16), ("w", C.c_uint32), ("h", C.c_uint32),
+        ("depth", C.c_float),
+    ]
+
+
+class OrcScene(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("n_nodes", C.c_uint32), ("bricks", C.c_void_p), ("n_leaves", C.c_uint32),
+                ("lvoxc", C.c_uint32)]
+
+
+class OrcCounters(C.Structure):
+    _fields_ = [("vertices", C.c_uint64), ("node_visits", C.c_uint64), ("density_lookups", C.c_uint64),
+                ("mie_evals", C.c_uint64), ("paths", C.c_uint64)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+class Port:
+    """The C restatement (oracle/port)."""
+
+    def __init__(self, path: str = PORT_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle port not built: {path} (make -C oracle port)")
+        L = C.CDLL(path)
+        vp, u32, f32 = C.c_void_p, C.c_uint32, C.c_float
+        L.orc_build_octree.argtypes = [vp, vp, u32, f32, u32, C.POINTER(vp), C.POINTER(u32), C.POINTER(vp),
+                                       C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
+        L.orc_build_octree.restype = C.c_int
+        L.orc_free.argtypes = [vp]
+        L.orc_leaf_sequence.argtypes = [vp, vp, vp, u32, vp, vp, vp]
+        L.orc_leaf_sequence.restype = u32
+        L.orc_point_lookup.argtypes = [vp, vp, C.POINTER(C.c_int)]
+        L.orc_point_lookup.restype = u32
+        L.orc_sample_voxel_space.argtypes = [vp, vp, vp, u32]
+        L.orc_sample_voxel_space.restype = f32
+        L.orc_mie_eval_rgb.argtypes = [C.POINTER(OrcParams), f32, vp]
+        L.orc_mie_sample_theta_scan.argtypes = [C.POINTER(OrcParams), f32]
+        L.orc_mie_sample_theta_scan.restype = f32
+        L.orc_mie_sample_theta_bisect.argtypes = [C.POINTER(OrcParams), f32]
+        L.orc_mie_sample_theta_bisect.restype = f32
+        L.orc_mie_sample.argtypes = [C.POINTER(OrcParams), vp, f32, f32, vp]
+        L.orc_sun_sample.argtypes = [C.POINTER(OrcParams), f32, f32, vp]
+        L.orc_sky_eval.argtypes = [C.POINTER(OrcParams), vp, vp]
+        L.orc_camera_ray.argtypes = [C.POINTER(OrcParams), u32, u32, vp, vp, C.POINTER(C.c_int)]
+        L.orc_optical_depth.argtypes = [C.POINTER(OrcScene), vp, vp, C.c_double]
+        L.orc_optical_depth.restype = C.c_double
+        L.orc_optical_depth_grad.argtypes = [C.POINTER(OrcScene), vp, vp, C.c_double, vp]
+        L.orc_render_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
+                                         C.c_uint64, C.c_uint64, vp, vp, C.POINTER(OrcCounters), C.c_int]
+        L.orc_render_tile_mt.restype = C.c_int
+        L.orc_render_path.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, C.c_uint64, C.c_uint64,
+                                      vp, vp, C.POINTER(OrcCounters)]
+        L.orc_transmittance_mc.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), vp, vp, C.c_uint64, C.c_uint64]
+        L.orc_transmittance_mc.restype = C.c_double
+        self.L = L
+
+    # -- scene build -------------------------------------------------------------
+    def build_octree(self, block_origin: np.ndarray, block_values: np.ndarray, voxel_size: float, maxdepth: int = 12):
+        org = np.ascontiguousarray(block_origin, np.int32)
+        vals = np.ascontiguousarray(block_values, np.float32)
+        pn, pb = C.c_void_p(), C.c_void_p()
+        nn, nl, lv, ml = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        rc = self.L.orc_build_octree(_p(org), _p(vals), len(org), voxel_size, maxdepth, C.byref(pn), C.byref(nn),
+                                     C.byref(pb), C.byref(nl), C.byref(lv), C.byref(ml))
+        if rc != 0:
+            raise ValueError(f"orc_build_octree failed ({rc})")
+        nodes = np.frombuffer(C.string_at(pn, nn.value * 64), NODE_DTYPE).copy()
+        bricks = np.frombuffer(C.string_at(pb, nl.value * lv.value ** 3 * 4), np.float32).copy()
+        self.L.orc_free(pn)
+        self.L.orc_free(pb)
+        return nodes, bricks.reshape(nl.value, lv.value ** 3), int(ml.value)
+
+    @staticmethod
+    def scene(nodes: np.ndarray, bricks: np.ndarray) -> OrcScene:
+        return OrcScene(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+
+    def leaf_sequence(self, nodes, ro, rd, maxn=4096):
+        ro = np.ascontiguousarray(ro, np.float32)
+        rd = np.ascontiguousarray(rd, np.float32)
+        n_ = np.zeros(maxn, np.uint32)
+        a = np.zeros(maxn, np.float32)
+        b = np.zeros(maxn, np.float32)
+        k = self.L.orc_leaf_sequence(_p(nodes), _p(ro), _p(rd), maxn, _p(n_), _p(a), _p(b))
+        return n_[:k], a[:k], b[:k]
+
+    def point_lookup(self, nodes, p):
+        d = C.c_int()
+        p = np.ascontiguousarray(p, np.float64)
+        r = self.L.orc_point_lookup(_p(nodes), _p(p), C.byref(d))
+        return int(r), int(d.value)
+
+    def sample_voxel_space(self, p, brick, ce):
+        p = np.ascontiguousarray(p, np.float32)
+        brick = np.ascontiguousarray(brick, np.float32)
+        ce = np.ascontiguousarray(ce, np.float32)
+        return float(self.L.orc_sample_voxel_space(_p(p), _p(brick), _p(ce), 8))
+
+    @staticmethod
+    def params(cfg: dict, keep: list) -> OrcParams:
+        """OrcParams from a render configuration dict (see tests' helpers)."""
+        P = OrcParams()
+        P.sigma_s, P.sigma_a, P.scattevs = cfg["sigma_s"], cfg["sigma_a"], cfg["scattevs"]
+        P.sun_dir[:] = [float(v) for v in cfg["sun_dir"]]
+        P.sun_color[:] = [float(v) for v in cfg["sun_color"]]
+        P.sun_cos_angle = float(np.cos(np.float32(cfg["sun_angle"]), dtype=np.float32)) \
+            if "sun_cos" not in cfg else float(cfg["sun_cos"])
+        cfgs = np.asarray(cfg["sky_configs"], np.float64).astype(np.float32)
+        for i in range(3):
+            P.sky_cfg[i][:] = [float(v) for v in cfgs[i]]
+        P.sky_rad[:] = [float(v) for v in np.asarray(cfg["sky_radiances"], np.float64).astype(np.float32)]
+        pdf = np.ascontiguousarray(cfg["mie_pdf"], np.float32)
+        cdf = np.ascontiguousarray(cfg["mie_cdf"], np.float32)
+        keep += [pdf, cdf]
+        P.mie_pdf, P.mie_cdf, P.mie_n = pdf.ctypes.data, cdf.ctypes.data, len(pdf)
+        P.viewi[:] = [float(v) for v in cfg["viewi"]]
+        P.proji[:] = [float(v) for v in cfg["proji"]]
+        P.w, P.h = cfg["w"], cfg["h"]
+        P.depth = float(np.finfo(np.float32).max)
+        return P
+
+    def render_tile(self, S, P, x0, y0, tw, th, spp, seed, sample_base=0, threads=0):
+        sun = np.zeros((th, tw, 4), np.float32)
+        sky = np.zeros((th, tw, 4), np.float32)
+        cnt = OrcCounters()
+        nt = threads if threads > 0 else (os.cpu_count() or 1)
+        self.L.orc_render_tile_mt(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base, _p(sun), _p(sky),
+                                  C.byref(cnt), nt)
+        return sun, sky, cnt.as_dict()
+
+    def render_path(self, S, P, px, py, seed, sample):
+        a = np.zeros(4, np.float32)
+        b = np.zeros(4, np.float32)
+        cnt = OrcCounters()
+        self.L.orc_render_path(C.byref(S), C.byref(P), px, py, seed, sample, _p(a), _p(b), C.byref(cnt))
+        return a, b, cnt.as_dict()
+
+
+class Reference:
+    """The reference's own sources compiled unmodified (oracle/_ref)."""
+
+    def __init__(self, path: str = REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference oracle not built: {path} (make -C oracle ref)")
+        L = C.CDLL(path)
+        vp, u32, f32, f64 = C.c_void_p, C.c_uint32, C.c_float, C.c_double
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_scene_create.argtypes = [vp, u32, vp, u32, u32]
+        L.ref_scene_create.restype = vp
+        L.ref_scene_destroy.argtypes = [vp]
+        L.ref_leaf_sequence.argtypes = [vp, C.c_int, vp, vp, u32, vp, vp, vp]
+        L.ref_leaf_sequence.restype = u32
+        L.ref_sky_state.argtypes = [f64, f64, f64, vp, vp]
+        L.ref_solar_elevation.argtypes = [vp]
+        L.ref_solar_elevation.restype = f32
+        L.ref_render.argtypes = [vp, vp, vp, vp, vp, f32, f64, f64, u32, f32, f32, u32, u32, u32, u32, u32, u32, u32,
+                                 vp, vp]
+        L.ref_render.restype = C.c_int
+        L.ref_sample_voxel_space.argtypes = [vp, vp, vp, u32]
+        L.ref_sample_voxel_space.restype = f32
+        L.ref_mie_table_size.restype = u32
+        L.ref_mie_tables.argtypes = [vp, vp]
+        L.ref_mie_eval.argtypes = [vp, u32, vp, vp]
+        L.ref_mie_sample.argtypes = [vp, vp, vp, u32, vp]
+        L.ref_sun_ops.argtypes = [vp, vp, f32, vp, vp, vp, u32, vp, vp, vp]
+        L.ref_rng_draw.argtypes = [vp, u32, vp]
+        self.L = L
+
+    def set_threads(self, n: int):
+        self.L.ref_set_threads(int(n))
+
+    def scene(self, nodes: np.ndarray, bricks: np.ndarray):
+        nodes = np.ascontiguousarray(nodes)
+        bricks = np.ascontiguousarray(bricks, np.float32)
+        return _RefScene(self, self.L.ref_scene_create(_p(nodes), len(nodes), _p(bricks), len(bricks), 8))
+
+    def mie_tables(self):
+        n = self.L.ref_mie_table_size()
+        pdf = np.zeros((n, 3), np.float32)
+        cdf = np.zeros((n, 3), np.float32)
+        self.L.ref_mie_tables(_p(pdf), _p(cdf))
+        return pdf, cdf
+
+    def sky_state(self, turbidity, albedo, elevation):
+        cfg = np.zeros((3, 9), np.float64)
+        rad = np.zeros(3, np.float64)
+        self.L.ref_sky_state(turbidity, albedo, elevation, _p(cfg), _p(rad))
+        return cfg, rad
+
+    def solar_elevation(self, sun_dir):
+        s = np.ascontiguousarray(sun_dir, np.float32)
+        return float(self.L.ref_solar_elevation(_p(s)))
+
+    def sample_voxel_space(self, p, brick, ce):
+        p = np.ascontiguousarray(p, np.float32)
+        brick = np.ascontiguousarray(brick, np.float32)
+        ce = np.ascontiguousarray(ce, np.float32)
+        return float(self.L.ref_sample_voxel_space(_p(p), _p(brick), _p(ce), 8))
+
+    def mie_eval(self, ct):
+        ct = np.ascontiguousarray(ct, np.float32)
+        s = np.zeros(len(ct), np.float32)
+        rgb = np.zeros((len(ct), 3), np.float32)
+        self.L.ref_mie_eval(_p(ct), len(ct), _p(s), _p(rgb))
+        return s, rgb
+
+    def mie_sample(self, iv, u1, u2):
+        iv = np.ascontiguousarray(iv, np.float32)
+        u1 = np.ascontiguousarray(u1, np.float32)
+        u2 = np.ascontiguousarray(u2, np.float32)
+        out = np.zeros((len(u1), 3), np.float32)
+        self.L.ref_mie_sample(_p(iv), _p(u1), _p(u2), len(u1), _p(out))
+        return out
+
+    def sun_ops(self, sun_dir, color, angle, v, u1, u2):
+        d = np.ascontiguousarray(sun_dir, np.float32)
+        c = np.ascontiguousarray(color, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        u1 = np.ascontiguousarray(u1, np.float32)
+        u2 = np.ascontiguousarray(u2, np.float32)
+        n = len(u1)
+        ev = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        smp = np.zeros((n, 3), np.float32)
+        self.L.ref_sun_ops(_p(d), _p(c), angle, _p(v), _p(u1), _p(u2), n, _p(ev), _p(pdf), _p(smp))
+        return ev, pdf, smp
+
+
+class _RefScene:
+    def __init__(self, ref: Reference, handle):
+        self.ref = ref
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.L.ref_scene_destroy(self.h)
+            self.h = None
+
+    def leaf_sequence(self, ro, rd, full=False, maxn=4096):
+        ro = np.ascontiguousarray(ro, np.float32)
+        rd = np.ascontiguousarray(rd, np.float32)
+        n_ = np.zeros(maxn, np.uint32)
+        a = np.zeros(maxn, np.float32)
+        b = np.zeros(maxn, np.float32)
+        k = self.ref.L.ref_leaf_sequence(self.h, 1 if full else 0, _p(ro), _p(rd), maxn, _p(n_), _p(a), _p(b))
+        return n_[:k], a[:k], b[:k]
+
+    def render(self, cfg: dict, x0, y0, tw, th, spp):
+        """RenderKernel::Render over one tile; returns (sun, sky) float4 tiles (sums over spp)."""
+        viewi = np.ascontiguousarray(cfg["viewi"], np.float32)
+        proji = np.ascontiguousarray(cfg["proji"], np.float32)
+        sd = np.ascontiguousarray(cfg["sun_dir"], np.float32)
+        sc = np.ascontiguousarray(cfg["sun_color"], np.float32)
+        sun = np.zeros((th, tw, 4), np.float32)
+        sky = np.zeros((th, tw, 4), np.float32)
+        rc = self.ref.L.ref_render(self.h, _p(viewi), _p(proji), _p(sd), _p(sc), float(cfg["sun_angle"]),
+                                   float(cfg["turbidity"]), float(cfg["ground_albedo"]), int(cfg["scattevs"]),
+                                   float(cfg["sigma_s"]), float(cfg["sigma_a"]), int(cfg["w"]), int(cfg["h"]),
+                                   x0, y0, tw, th, spp, _p(sun), _p(sky))
+        if rc != 0:
+            raise RuntimeError("ref_render failed")
+        return sun, sky

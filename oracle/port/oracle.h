@@ -1,0 +1,122 @@
+/* ORACLE TEST INFRASTRUCTURE — CPU restatement of droplet-render's volumetric
+ * path-tracing hot path.  Only tests, the smoke check and the CPU-baseline leg
+ * of the benchmark may load it; the product never links it.
+ *
+ * Every function cites the reference file:line it restates.  Octree traversal,
+ * leaf indexing and brick lookups repeat the reference's binary32 operations in
+ * the same order; the estimator is the reference's (src/kernel.cpp:128-445)
+ * written as a loop, drawing from a per-path PCG32 stream instead of the
+ * reference's thread-order-seeded packet Tausworthe generator.
+ */
+#ifndef DR_ORACLE_H
+#define DR_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_NONE 0xffffffffu
+#define ORC_SDF 0
+#define ORC_FOG 1
+#define ORC_MAX_DEPTH 16
+
+/* src/scene.h:21-31 OctreeStructure, 64 bytes. */
+typedef struct {
+    float ce[4];        /* center.xyz, half extent */
+    uint32_t chn[8];    /* child node index, 0 = none; child i offset (i&1, i>>1&1, i>>2) */
+    uint32_t volx[2];   /* brick index per buffer or ORC_NONE */
+    float qval[2];      /* per-leaf majorant (FOG: max density, floor 0.01) */
+} orc_node;
+
+typedef struct {
+    const orc_node *nodes;
+    uint32_t n_nodes;
+    const float *bricks;   /* FOG bricks, lvoxc^3 floats each, z-major then y then x */
+    uint32_t n_leaves;
+    uint32_t lvoxc;
+} orc_scene;
+
+typedef struct {
+    /* medium */
+    float sigma_s, sigma_a;
+    uint32_t scattevs;
+    /* sun: src/KernelSampler.cpp:305-345 */
+    float sun_dir[3], sun_color[3], sun_cos_angle;
+    /* Hosek sky, as the reference kernel consumes it (binary32 copies of the
+     * cooked double state, src/kernel.cpp:343-358) */
+    float sky_cfg[3][9], sky_rad[3];
+    /* Mie tables: 256 RGB entries each, index 0 = backscatter */
+    const float *mie_pdf, *mie_cdf;
+    uint32_t mie_n;
+    /* camera: rows r[0..3] of the inverse view / projection matrices */
+    float viewi[16], proji[16];
+    uint32_t w, h;
+    float depth;           /* compositing depth (FLT_MAX when unused) */
+} orc_params;
+
+typedef struct {
+    uint64_t vertices;       /* traced segments: camera, continuation and shadow */
+    uint64_t node_visits;    /* octree node records examined by the traverser */
+    uint64_t density_lookups;/* trilinear brick lookups */
+    uint64_t mie_evals;      /* phase table evaluations + phase samples */
+    uint64_t paths;
+} orc_counters;
+
+/* ---- scene build: src/scene.cpp:267-305, 676-762, 840-908 ---------------- */
+/* Sparse input in the shape of OpenVDB leaves: n_blocks blocks of 8^3 values
+ * (x fastest within a block's z-major order), block origins in voxel units
+ * (multiples of 8).  Voxel (i,j,k) sits at world (i,j,k)*s; a voxel is active
+ * iff its value is non-zero.  Returns 0 on success. */
+int orc_build_octree(const int32_t *block_origin, const float *block_values, uint32_t n_blocks, float s,
+                     uint32_t maxdepth, orc_node **out_nodes, uint32_t *n_nodes, float **out_bricks,
+                     uint32_t *n_leaves, uint32_t *out_lvoxc, uint32_t *out_mlevel);
+void orc_free(void *p);
+
+/* ---- traversal: src/KernelOctree.cpp ------------------------------------- */
+uint32_t orc_leaf_sequence(const orc_node *nodes, const float ro[3], const float rd[3], uint32_t maxn,
+                           uint32_t *out_nodes, float *out_tr0, float *out_tr1);
+/* FP64 point location: the leaf whose box contains p, descending by
+ * child bit (p > center) per axis, src/scene.cpp:285 numbering.  Returns the
+ * node index or ORC_NONE; *depth receives the level reached. */
+uint32_t orc_point_lookup(const orc_node *nodes, const double p[3], int *depth);
+
+/* ---- samplers ------------------------------------------------------------ */
+float orc_sample_voxel_space(const float p[3], const float *brick, const float ce[4], uint32_t lvoxc);
+void orc_mie_eval_rgb(const orc_params *P, float ct, float out[3]);
+float orc_mie_eval(const orc_params *P, float ct);
+float orc_mie_sample_theta_scan(const orc_params *P, float u1);   /* reference linear scan */
+float orc_mie_sample_theta_bisect(const orc_params *P, float u1); /* same bin by bisection */
+void orc_mie_sample(const orc_params *P, const float iv[3], float u1, float u2, float out[3]);
+void orc_sun_eval(const orc_params *P, const float rd[3], float out[3]);
+float orc_sun_pdf(const orc_params *P, const float v[3]);
+void orc_sun_sample(const orc_params *P, float u1, float u2, float out[3]);
+void orc_sky_eval(const orc_params *P, const float rd[3], float out[3]);
+void orc_camera_ray(const orc_params *P, uint32_t px, uint32_t py, float ro[3], float rd[3], int *in_frame);
+
+/* ---- FP64 checks --------------------------------------------------------- */
+/* Optical depth integral of the brick density along ro + t rd, t in [0, tmax],
+ * leaf by leaf, exact Gauss-Legendre on every brick-cell segment. */
+double orc_optical_depth(const orc_scene *S, const double ro[3], const double rd[3], double tmax);
+
+/* ---- estimator ----------------------------------------------------------- */
+/* Free-flight tracking of one segment (src/kernel.cpp:197-317, fog leaves).
+ * Returns 1 when the ray leaves the volume without a real collision. */
+int orc_track(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], void *rng,
+              float *td, orc_counters *cnt);
+/* One tile of RenderKernel::Render (src/kernel.cpp:447-487, 536-567): sums of
+ * spp path samples per pixel into out_sun/out_sky (float4, row-major tile).
+ * Path (pixel p = py*w + px, sample s) draws from PCG32 stream
+ * (seed, p, sample_base + s). */
+int orc_render_tile(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                    uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
+                    orc_counters *cnt);
+/* A single path sample, for per-path comparisons. */
+void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
+                     uint64_t sample, float out_sun[4], float out_sky[4], orc_counters *cnt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

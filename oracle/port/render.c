@@ -1,0 +1,243 @@
+/* ORACLE TEST INFRASTRUCTURE — the reference estimator (SampleVolume,
+ * src/kernel.cpp:128-445) restated as an iterative per-path loop.
+ *
+ * Recursion unrolled: SampleVolume(r) returns, per sample,
+ *   escaped & r>0 : sun(rd) into the sun buffer, sky(rd) into the sky buffer
+ *   collided & r<scattevs : (S1 w1 + S2 w2) sigma_s/sigma_t, where S1 is the
+ *       continuation SampleVolume(r+1) along the phase sample and S2 the
+ *       shadow SampleVolume(scattevs) along the sun sample (sky of S2 dropped)
+ *   otherwise 0;  alpha = 1 iff the camera segment collided (r = 0).
+ * Written as a throughput loop: shadow rays add T * w2 * f * sun(lrd) when
+ * they escape, T *= w1 * f, f = sigma_s/sigma_t (src/kernel.cpp:387-441).
+ *
+ * Tracking (src/kernel.cpp:207-317, fog-only leaves): a leaf ahead of the
+ * current position is entered at its entry distance (empty space skipped);
+ * a leaf the ray is already inside continues from the current position; a
+ * candidate with sc <= tr0 collides without a density lookup; otherwise it is
+ * accepted when rho/smax >= q.
+ */
+#include "oracle.h"
+#include "orc_math.h"
+#include <math.h>
+#include <float.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+size_t orc_trav_size(void);
+void orc_trav_init(void *T, const orc_node *nodes, const float ro[3], const float rd[3]);
+int orc_trav_next(void *T, const orc_node *nodes, uint32_t *node, float *tr0, float *tr1, uint64_t *visits);
+
+static inline float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static int track_depth(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], orc_rng *g,
+                       float depth, float *td_out, orc_counters *cnt) {
+    const float sigma_e = P->sigma_a + P->sigma_s;
+    const uint32_t N = S->lvoxc, lv3 = N * N * N;
+    _Alignas(16) unsigned char tbuf[2048];
+    void *T = tbuf;
+    orc_trav_init(T, S->nodes, ro, rd);
+    if (cnt) cnt->vertices++;
+    float td = 0.0f;
+    uint32_t node;
+    float tra, trb;
+    for (;;) {
+        if (!orc_trav_next(T, S->nodes, &node, &tra, &trb, cnt ? &cnt->node_visits : 0)) break;
+        if (!(td < depth)) break;
+        const orc_node *o = &S->nodes[node];
+        const float lo = td;
+        const float tr0 = tra - td, tr1 = trb - td;
+        const float smax = o->qval[ORC_FOG];
+        /* src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
+         * fog leaves, so the masked selects below are bitwise blends: past the
+         * leaf entry, td keeps all but its lowest bit and s0 becomes the lowest
+         * bit of tr0 (0 or the smallest denormal). */
+        float s0;
+        if (tra > td) {
+            td = tra;
+            s0 = tr0;
+        } else {
+            td = orc_u2f((orc_f2u(td) & ~1u) | (orc_f2u(tra) & 1u));
+            s0 = orc_u2f(orc_f2u(tr0) & 1u);
+        }
+        const float *brick = S->bricks + (size_t)o->volx[ORC_FOG] * lv3;
+        const float denom = sigma_e * smax;
+        float sr = -orc_log(orc_rng_uniform(g)) / denom;
+        for (;;) {
+            const float sc = s0 + sr;
+            td = lo + sc;
+            if (!(sc < tr1)) {
+                td = trb;
+                break;
+            }
+            int rm = sc > tr0;
+            float rho = -1.0f;
+            if (rm) {
+                float rc[3];
+                for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+                rho = orc_sample_voxel_space(rc, brick, o->ce, N);
+                if (cnt) cnt->density_lookups++;
+            }
+            const float q = orc_rng_uniform(g);
+            rm = rm && (rho / smax < q);
+            if (!rm) {
+                *td_out = td;
+                return 0;
+            }
+            sr = sr - orc_log(orc_rng_uniform(g)) / denom;
+        }
+    }
+    *td_out = td;
+    return 1;
+}
+
+int orc_track(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], void *rng, float *td,
+              orc_counters *cnt) {
+    return track_depth(S, P, ro, rd, (orc_rng *)rng, FLT_MAX, td, cnt);
+}
+
+void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
+                     uint64_t sample, float out_sun[4], float out_sky[4], orc_counters *cnt) {
+    for (int k = 0; k < 4; ++k) out_sun[k] = out_sky[k] = 0.0f;
+    float ro[3], rd[3];
+    int inf;
+    orc_camera_ray(P, px, py, ro, rd, &inf);
+    if (!inf) return;
+    orc_rng g;
+    orc_rng_seed(&g, seed, (uint64_t)py * P->w + px, sample);
+    if (cnt) cnt->paths++;
+    const float f = P->sigma_s / (P->sigma_a + P->sigma_s);
+    float T[3] = {1.0f, 1.0f, 1.0f};
+    uint32_t r = 0;
+    for (;;) {
+        float td;
+        int esc = track_depth(S, P, ro, rd, &g, r == 0 ? P->depth : FLT_MAX, &td, cnt);
+        if (r == 0) out_sun[3] = out_sky[3] = esc ? 0.0f : 1.0f;
+        if (esc) {
+            if (r > 0) {
+                float sun[3], sky[3];
+                orc_sun_eval(P, rd, sun);
+                orc_sky_eval(P, rd, sky);
+                for (int k = 0; k < 3; ++k) {
+                    out_sun[k] = out_sun[k] + T[k] * sun[k];
+                    out_sky[k] = out_sky[k] + T[k] * sky[k];
+                }
+            }
+            break;
+        }
+        if (r >= P->scattevs) break;
+        float srd[3], lrd[3], p1[3], p3[3], rc[3];
+        const float u1 = orc_rng_uniform(&g), u2 = orc_rng_uniform(&g);
+        orc_mie_sample(P, rd, u1, u2, srd);
+        const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
+        orc_sun_sample(P, u3, u4, lrd);
+        orc_mie_eval_rgb(P, dot3(srd, rd), p1);
+        const float p2 = orc_sun_pdf(P, lrd);
+        orc_mie_eval_rgb(P, dot3(lrd, rd), p3);
+        const float q1 = orc_sun_pdf(P, srd);
+        if (cnt) cnt->mie_evals += 3;
+        for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+        float tds;
+        if (track_depth(S, P, rc, lrd, &g, FLT_MAX, &tds, cnt)) {
+            float sun[3];
+            orc_sun_eval(P, lrd, sun);
+            for (int k = 0; k < 3; ++k) out_sun[k] = out_sun[k] + (T[k] * ((p3[k] / (p3[k] + p2)) * f)) * sun[k];
+        }
+        for (int k = 0; k < 3; ++k) {
+            T[k] = T[k] * ((p1[k] / (p1[k] + q1)) * f);
+            ro[k] = rc[k];
+            rd[k] = srd[k];
+        }
+        ++r;
+    }
+}
+
+typedef struct {
+    const orc_scene *S;
+    const orc_params *P;
+    uint32_t x0, y0, tw, th, spp, rows;
+    uint64_t seed, base;
+    float *sun, *sky;
+    orc_counters cnt;
+    int next_row_mod, nthreads, tid;
+} tile_job;
+
+static void *tile_worker(void *arg) {
+    tile_job *J = (tile_job *)arg;
+    const uint32_t cols = 2 * (J->tw / 2);
+    for (uint32_t j = (uint32_t)J->tid; j < J->rows; j += (uint32_t)J->nthreads) {
+        for (uint32_t i = 0; i < cols; ++i) {
+            float acc_sun[4] = {0, 0, 0, 0}, acc_sky[4] = {0, 0, 0, 0};
+            int any = 0;
+            for (uint32_t s = 0; s < J->spp; ++s) {
+                float a[4], b[4];
+                float ro[3], rd[3];
+                int inf;
+                orc_camera_ray(J->P, J->x0 + i, J->y0 + j, ro, rd, &inf);
+                if (!inf) break;
+                any = 1;
+                orc_render_path(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, a, b, &J->cnt);
+                for (int k = 0; k < 4; ++k) {
+                    acc_sun[k] += a[k];
+                    acc_sky[k] += b[k];
+                }
+            }
+            if (any) {
+                memcpy(&J->sun[4 * ((size_t)j * J->tw + i)], acc_sun, 16);
+                memcpy(&J->sky[4 * ((size_t)j * J->tw + i)], acc_sky, 16);
+            }
+        }
+    }
+    return 0;
+}
+
+int orc_render_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                       uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
+                       orc_counters *cnt, int nthreads) {
+    memset(out_sun, 0, sizeof(float) * 4 * (size_t)tw * th);
+    memset(out_sky, 0, sizeof(float) * 4 * (size_t)tw * th);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    tile_job jobs[256];
+    pthread_t th_ids[256];
+    for (int t = 0; t < nthreads; ++t) {
+        tile_job *J = &jobs[t];
+        memset(J, 0, sizeof(*J));
+        J->S = S; J->P = P; J->x0 = x0; J->y0 = y0; J->tw = tw; J->th = th; J->spp = spp;
+        J->rows = 2 * (th / 2); J->seed = seed; J->base = sample_base; J->sun = out_sun; J->sky = out_sky;
+        J->nthreads = nthreads; J->tid = t;
+    }
+    for (int t = 1; t < nthreads; ++t) pthread_create(&th_ids[t], 0, tile_worker, &jobs[t]);
+    tile_worker(&jobs[0]);
+    for (int t = 1; t < nthreads; ++t) pthread_join(th_ids[t], 0);
+    if (cnt) {
+        for (int t = 0; t < nthreads; ++t) {
+            cnt->vertices += jobs[t].cnt.vertices;
+            cnt->node_visits += jobs[t].cnt.node_visits;
+            cnt->density_lookups += jobs[t].cnt.density_lookups;
+            cnt->mie_evals += jobs[t].cnt.mie_evals;
+            cnt->paths += jobs[t].cnt.paths;
+        }
+    }
+    return 0;
+}
+
+int orc_render_tile(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                    uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
+                    orc_counters *cnt) {
+    return orc_render_tile_mt(S, P, x0, y0, tw, th, spp, seed, sample_base, out_sun, out_sky, cnt, 1);
+}
+
+/* Fraction of nrays x nsamp delta-tracked segments from ro along rd that
+ * escape, using streams (seed, ray, sample).  Used by the transmittance gate. */
+double orc_transmittance_mc(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3],
+                            uint64_t seed, uint64_t nsamp) {
+    uint64_t esc = 0;
+    for (uint64_t s = 0; s < nsamp; ++s) {
+        orc_rng g;
+        orc_rng_seed(&g, seed, 0, s);
+        float td;
+        esc += (uint64_t)track_depth(S, P, ro, rd, &g, FLT_MAX, &td, 0);
+    }
+    return (double)esc / (double)nsamp;
+}

@@ -1,0 +1,217 @@
+/* ORACLE TEST INFRASTRUCTURE — restatement of the reference's per-vertex
+ * samplers with the same binary32 operation order (no fused multiply-adds:
+ * the reference's SSE4 build evaluates madd/msub as separate mul and add).
+ *
+ *   SampleVoxelSpace          src/kernel.cpp:96-126
+ *   MiePhase::Evaluate/RGB    src/KernelSampler.cpp:214-255
+ *   MiePhase::Sample          src/KernelSampler.cpp:257-285 (linear scan)
+ *   SamplingBasis             src/KernelSampler.cpp:145-154
+ *   SunLight Evaluate/Pdf/Sample src/KernelSampler.cpp:318-345
+ *   Hosek sky radiance        src/kernel.cpp:329-360
+ *   camera ray                src/kernel.cpp:461-474
+ * Transcendentals (log, exp, pow, sin, cos) come from orc_math.h and differ
+ * from the reference's SSE approximations by a few ulps.
+ */
+#include "oracle.h"
+#include "orc_math.h"
+#include <math.h>
+#include <float.h>
+
+static inline float sse_max(float a, float b) { return a > b ? a : b; } /* _mm_max_ps(a,b) */
+static inline float sse_min(float a, float b) { return a < b ? a : b; } /* _mm_min_ps(a,b) */
+static inline float lerp_ref(float a, float b, float t) { return t * (b - a) + a; } /* t.madd(b-a, a) */
+
+float orc_sample_voxel_space(const float p[3], const float *v, const float ce[4], uint32_t N) {
+    const float nv = (float)N;
+    const float nm1 = nv - 1.0f;
+    const float top = (float)(N - 1);
+    uint32_t ia[3], ib[3];
+    float nl[3];
+    for (int k = 0; k < 3; ++k) {
+        float ni = ((-0.5f * ((ce[k] - ce[3]) - p[k])) * nm1) / ce[3];
+        float nf = sse_max(floorf(ni), 0.0f);
+        float nc = sse_min(ceilf(ni), nm1);
+        nl[k] = ni - nf;
+        nc = sse_max(sse_min(nc, top), 0.0f);
+        nf = sse_max(sse_min(nf, top), 0.0f);
+        ia[k] = (uint32_t)nf;
+        ib[k] = (uint32_t)nc;
+    }
+    const uint32_t N2 = N * N;
+#define V(z, y, x) v[(z) * N2 + (y) * N + (x)]
+    float u0 = lerp_ref(V(ia[2], ia[1], ia[0]), V(ia[2], ia[1], ib[0]), nl[0]);
+    float u1 = lerp_ref(V(ia[2], ib[1], ia[0]), V(ia[2], ib[1], ib[0]), nl[0]);
+    float u2 = lerp_ref(V(ib[2], ia[1], ia[0]), V(ib[2], ia[1], ib[0]), nl[0]);
+    float u3 = lerp_ref(V(ib[2], ib[1], ia[0]), V(ib[2], ib[1], ib[0]), nl[0]);
+#undef V
+    float v0 = lerp_ref(u0, u1, nl[1]);
+    float v1 = lerp_ref(u2, u3, nl[1]);
+    return lerp_ref(v0, v1, nl[2]);
+}
+
+static inline float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* index of the lower table entry and the lerp weight, src/KernelSampler.cpp:232-239 */
+static void mie_index(const orc_params *P, float ct, uint32_t *X, float *t) {
+    float ct1 = sse_max(sse_min(ct, 1.0f), -1.0f);       /* saturate2 */
+    float a = orc_acos_ref(0.0f - ct1) / ORC_PI;
+    float b = (float)P->mie_n * a;
+    float c = floorf(b);
+    c = sse_min(c, (float)(P->mie_n - 2));
+    c = sse_max(c, 0.0f);
+    *t = b - c;
+    *X = (uint32_t)c;
+}
+
+void orc_mie_eval_rgb(const orc_params *P, float ct, float out[3]) {
+    uint32_t X;
+    float t;
+    mie_index(P, ct, &X, &t);
+    for (int k = 0; k < 3; ++k) out[k] = lerp_ref(P->mie_pdf[3 * X + k], P->mie_pdf[3 * (X + 1) + k], t);
+}
+
+float orc_mie_eval(const orc_params *P, float ct) {
+    uint32_t X;
+    float t;
+    mie_index(P, ct, &X, &t);
+    return lerp_ref(P->mie_pdf[3 * X], P->mie_pdf[3 * (X + 1)], t);
+}
+
+/* interpolated red CDF value at scan step i, src/KernelSampler.cpp:262-267 */
+static inline float mie_scan_cdf(const orc_params *P, float ub, uint32_t i, float *t_out) {
+    const uint32_t n = P->mie_n;
+    float b = sse_max(ub, (float)i);
+    float c = sse_min(floorf(b), (float)(n - 1));
+    float t = b - c;
+    *t_out = t;
+    return lerp_ref(P->mie_cdf[3 * i], P->mie_cdf[3 * (i + 1)], t);
+}
+
+float orc_mie_sample_theta_scan(const orc_params *P, float u1) {
+    const uint32_t n = P->mie_n;
+    float th = 0.0f;
+    float ub = (float)n * u1;
+    for (uint32_t i = 0; i < n - 1; ++i) {
+        float t;
+        float cdf = mie_scan_cdf(P, ub, i, &t);
+        int m = cdf < u1;
+        float s = (float)i / (float)n + t / (float)n;
+        if (m) th = s;
+        else break;
+    }
+    return th;
+}
+
+/* The scan's predicate is non-decreasing in i, so the first failing step is
+ * found by bisection; the result equals the scan's whenever that holds. */
+float orc_mie_sample_theta_bisect(const orc_params *P, float u1) {
+    const uint32_t n = P->mie_n;
+    float ub = (float)n * u1;
+    uint32_t lo = 0, hi = n - 1; /* first i in [0, n-1) with !(cdf < u1), or n-1 */
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        float t;
+        if (mie_scan_cdf(P, ub, mid, &t) < u1) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0) return 0.0f;
+    float t;
+    (void)mie_scan_cdf(P, ub, lo - 1, &t);
+    return (float)(lo - 1) / (float)n + t / (float)n;
+}
+
+/* SamplingBasis, src/KernelSampler.cpp:145-154 */
+static void sampling_basis(const float iv[3], float b1[3], float b2[3]) {
+    float len = sqrtf(iv[0] * iv[0] + 0.0f * 0.0f + iv[2] * iv[2]);
+    b1[0] = (0.0f - iv[2]) / len;
+    b1[1] = 0.0f / len;
+    b1[2] = iv[0] / len;
+    b2[0] = iv[1] * b1[2] - iv[2] * b1[1];
+    b2[1] = iv[2] * b1[0] - iv[0] * b1[2];
+    b2[2] = iv[0] * b1[1] - iv[1] * b1[0];
+}
+
+static void compose_dir(const float b1[3], const float b2[3], const float iv[3], float st, float ct, float ph,
+                        float out[3]) {
+    float sph, cph;
+    orc_sincos(ph, &sph, &cph);
+    for (int k = 0; k < 3; ++k) out[k] = ((b1[k] * st) * cph + (b2[k] * st) * sph) + iv[k] * ct;
+}
+
+void orc_mie_sample(const orc_params *P, const float iv[3], float u1, float u2, float out[3]) {
+    float th = orc_mie_sample_theta_bisect(P, u1) * ORC_PI;
+    float ph = (2.0f * ORC_PI) * u2;
+    float b1[3], b2[3];
+    sampling_basis(iv, b1, b2);
+    float s_, c_;
+    orc_sincos(th, &s_, &c_);
+    float ct = -c_; /* -cos_ps(): sign flip of the __m128 */
+    float st = sqrtf(sse_max(1.0f - ct * ct, 0.0f));
+    compose_dir(b1, b2, iv, st, ct, ph, out);
+}
+
+void orc_sun_eval(const orc_params *P, const float rd[3], float out[3]) {
+    int lt = dot3(rd, P->sun_dir) > P->sun_cos_angle;
+    for (int k = 0; k < 3; ++k) out[k] = lt ? P->sun_color[k] : 0.0f;
+}
+
+float orc_sun_pdf(const orc_params *P, const float v[3]) {
+    float ctm = P->sun_cos_angle;
+    int lt = dot3(v, P->sun_dir) > ctm;
+    return lt ? 1.0f / ((2.0f * ORC_PI) * (1.0f - ctm * ctm)) : 0.0f;
+}
+
+void orc_sun_sample(const orc_params *P, float u1, float u2, float out[3]) {
+    float ctm = P->sun_cos_angle;
+    float ct = (1.0f - u1) + u1 * ctm;
+    float st = sqrtf(1.0f - ct * ct);
+    float ph = (2.0f * ORC_PI) * u2;
+    float b1[3], b2[3];
+    sampling_basis(P->sun_dir, b1, b2);
+    compose_dir(b1, b2, P->sun_dir, st, ct, ph, out);
+}
+
+void orc_sky_eval(const orc_params *P, const float rd[3], float out[3]) {
+    const float *sd = P->sun_dir;
+    float rdz = rd[2];
+    float sth = sqrtf(1.0f - rd[2] * rd[2]);
+    float cth = rdz;
+    float slth = sqrtf(1.0f - sd[2] * sd[2]);
+    float clth = sd[2];
+    float slph = sd[1];
+    float clph = sd[0];
+    float rdd = rd[0] / rd[1];
+    float acr = 1.0f / sqrtf(rdd * rdd + 1.0f);
+    float czp = acr * (rdd * slph + clph);
+    float cph = (sth * slth) * czp + cth * clth;
+    float gmma = orc_acos_ref(cph);
+    float gacs = sse_max(sse_min(cph, 1.0f), 0.0f);
+    float thcs = sse_max(rdz, 0.0f);
+    float raym = gacs * gacs;
+    for (int i = 0; i < 3; ++i) {
+        const float *c = P->sky_cfg[i];
+        float expm = orc_exp(c[4] * gmma);
+        float miem = (1.0f + raym) / orc_pow((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs, 1.5f);
+        float zenh = sqrtf(thcs);
+        float ca = (1.0f + c[0] * orc_exp(c[1] / (thcs + 0.01f))) *
+                   ((((c[2] + c[3] * expm) + c[5] * raym) + c[6] * miem) + c[7] * zenh);
+        ca = ca * P->sky_rad[i];
+        out[i] = 1e-3f * orc_pow(ca, 2.2f);
+    }
+}
+
+/* K_ParallelRender ray generation for pixel (px, py), src/kernel.cpp:461-474 */
+void orc_camera_ray(const orc_params *P, uint32_t px, uint32_t py, float ro[3], float rd[3], int *in_frame) {
+    float hx = 0.0f - (((2.0f * ((float)px + 0.5f)) / (float)P->w) - 1.0f);
+    float hy = 0.0f - (((2.0f * ((float)py + 0.5f)) / (float)P->h) - 1.0f);
+    const float *V = P->viewi, *Q = P->proji;
+    float rv[4], d[3];
+    for (int k = 0; k < 4; ++k) rv[k] = ((hx * Q[k] + hy * Q[4 + k]) + 0.0f * Q[8 + k]) + 1.0f * Q[12 + k];
+    for (int k = 0; k < 3; ++k) d[k] = ((rv[0] * V[k] + rv[1] * V[4 + k]) + rv[2] * V[8 + k]) + 0.0f * V[12 + k];
+    float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int k = 0; k < 3; ++k) {
+        rd[k] = d[k] / len;
+        ro[k] = V[12 + k];
+    }
+    *in_frame = (hx > -1.0f && hx < 1.0f) && (hy > -1.0f && hy < 1.0f);
+}

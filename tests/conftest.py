@@ -1,0 +1,118 @@
+"""Shared test setup.
+
+Markers: `gpu` tests need a B200 and call the product through its C ABI; the
+rest run on the CPU (oracle pins, host builder, library loading, boundary).
+The CPU checkers live in oracle/ (test infrastructure only).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "droplet-render_b200")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from droplet_b200 import camera as cam  # noqa: E402
+from droplet_b200 import workloads as W  # noqa: E402
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); calls the product through its C ABI")
+
+
+def golden(name: str):
+    path = os.path.join(GOLDEN, name)
+    if name.endswith(".json"):
+        with open(path) as f:
+            return json.load(f)
+    with np.load(path) as z:  # materialise: NpzFile re-reads members on each access
+        return {k: np.ascontiguousarray(z[k]) for k in z.files}
+
+
+def golden_octree():
+    from oracle.oracle import NODE_DTYPE
+
+    z = golden("c0_octree.npz")
+    return z["nodes"].view(NODE_DTYPE).reshape(-1), z["bricks"], int(z["mlevel"].reshape(-1)[0])
+
+
+def mie_table():
+    z = golden("mie_reference_table.npz")
+    return np.ascontiguousarray(z["pdf"], np.float32), np.ascontiguousarray(z["cdf"], np.float32)
+
+
+def sky_state_c0():
+    for s in golden("sky_states.json"):
+        if s["note"] == "c0/c1 sun":
+            return np.asarray(s["configs"], np.float64), np.asarray(s["radiances"], np.float64)
+    raise KeyError("c0 sky state")
+
+
+def c0_cfg(w: int, h: int, medium: str = "c0") -> dict:
+    """Render configuration dict for config 0 at w x h (inputs from the fixtures)."""
+    pdf, cdf = mie_table()
+    cfgs, rads = sky_state_c0()
+    sd = cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"])
+    eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], W.CAMERA["azimuth"], W.CAMERA["elevation"])
+    viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], w, h)
+    ss, sa, ev = W.medium(medium)
+    return dict(sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=sd, sun_color=np.asarray(W.SUN["color"], np.float32),
+                sun_angle=W.SUN["angle"], turbidity=W.SKY["turbidity"], ground_albedo=W.SKY["albedo"],
+                sky_configs=cfgs, sky_radiances=rads, mie_pdf=pdf, mie_cdf=cdf, viewi=viewi, proji=proji, w=w, h=h)
+
+
+def settings_from_cfg(cfg: dict):
+    from droplet_b200.renderer import PhaseTable, RenderSettings
+    from droplet_b200.sky import SkyState
+
+    return RenderSettings(
+        sigma_s=cfg["sigma_s"], sigma_a=cfg["sigma_a"], scattevs=cfg["scattevs"], sun_dir=cfg["sun_dir"],
+        sun_color=cfg["sun_color"], sun_angle=cfg["sun_angle"],
+        sky=SkyState(np.asarray(cfg["sky_configs"]), np.asarray(cfg["sky_radiances"])),
+        phase=PhaseTable(cfg["mie_pdf"], cfg["mie_cdf"]), viewi=cfg["viewi"], proji=cfg["proji"], w=cfg["w"],
+        h=cfg["h"])
+
+
+@pytest.fixture(scope="session")
+def port():
+    from oracle import Port, port_available
+
+    if not port_available():
+        pytest.skip("oracle port not built (make -C oracle port)")
+    return Port()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle import Reference, ref_available
+
+    if not ref_available():
+        pytest.skip("reference oracle not built (needs the reference sources; make -C oracle ref)")
+    return Reference()
+
+
+@pytest.fixture(scope="session")
+def c0_octree():
+    return golden_octree()
+
+
+@pytest.fixture(scope="session")
+def gpu_renderer():
+    """A renderer on cuda:0 with the config-0 scene and 64x64 parameters."""
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree
+
+    nodes, bricks, mlevel = golden_octree()
+    r = Renderer(0)
+    r.upload(Octree(nodes.view(np.uint8).view(nodes.dtype), bricks, mlevel))
+    r.set_params(settings_from_cfg(c0_cfg(64, 64)))
+    yield r
+    r.close()
