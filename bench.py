@@ -40,7 +40,7 @@ from droplet_b200 import workloads as W  # noqa: E402
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 W_IMG, H_IMG, SPP = 1920, 1080, 64
 METRIC = "path-vertices/s (plain renderer, single large cumulus 512^3, 1920x1080, 64 spp)"
-CPU_CROP = 48  # reference / cpu_baseline sample: 48x48 centre crop at full spp
+CPU_CROP = 384  # reference / cpu_baseline sample: centre crop at full spp (about 10 s of 16 cores)
 
 
 def log(*a):
@@ -150,28 +150,40 @@ def profiled_traffic():
         return None
 
 
-def cpu_reference_sample(nodes, bricks, cfg, threads: int, steps: int = 1, warmup: int = 0):
-    """Times the reference renderer on the crop (one step = the crop at full spp);
-    the vertex count of a step comes from the CPU restatement on the same crop."""
-    from oracle import Port, Reference
+def cpu_reference_times(nodes, bricks, cfg, threads: int, steps: int = 1, warmup: int = 0):
+    """Wall times of the reference renderer (oracle/_ref) on the crop, one
+    RenderKernel::Render call of the crop at full spp per step."""
+    from oracle import Reference
 
     ref = Reference()
     ref.set_threads(threads)
     rs = ref.scene(nodes, bricks)
     x0, y0, tw, th = crop_box()
     for _ in range(warmup):
-        rs.render(cfg, x0, y0, tw // 4, th // 4, SPP)
+        rs.render(cfg, x0 + tw // 2, y0 + th // 2, 16, 16, SPP)
     times = []
     for _ in range(steps):
         t = time.perf_counter()
         rs.render(cfg, x0, y0, tw, th, SPP)
         times.append(time.perf_counter() - t)
+    return times
+
+
+def cpu_reference_time(nodes, bricks, cfg, threads: int) -> float:
+    return cpu_reference_times(nodes, bricks, cfg, threads, steps=1, warmup=1)[0]
+
+
+def port_vertices(nodes, bricks, cfg, threads: int) -> int:
+    """Vertices of the crop counted by the CPU restatement (same estimator)."""
+    from oracle import Port
+
     port = Port()
     keep = []
     P = port.params(cfg, keep)
     S = port.scene(nodes, bricks)
+    x0, y0, tw, th = crop_box()
     _, _, cnt = port.render_tile(S, P, x0, y0, tw, th, SPP, seed=99, threads=threads)
-    return cnt["vertices"], times
+    return cnt["vertices"]
 
 
 def run_reference(args):
@@ -182,8 +194,8 @@ def run_reference(args):
     cfg = frame_cfg(pdf, cdf, cfgs, rads)
     nodes, bricks, mlevel, occ = build_scene("oracle")
     threads = os.cpu_count() or 1
-    verts, times = cpu_reference_sample(nodes, bricks, cfg, threads, steps=max(1, args.steps),
-                                        warmup=min(args.warmup, 1))
+    times = cpu_reference_times(nodes, bricks, cfg, threads, steps=max(1, args.steps), warmup=min(args.warmup, 1))
+    verts = port_vertices(nodes, bricks, cfg, threads)
     dt = float(np.mean(times))
     value = verts / dt
     x0, y0, tw, th = crop_box()
@@ -226,26 +238,31 @@ def run_b200(args):
     r = Renderer(local)
     r.upload(Octree(nodes, bricks, mlevel))
     r.set_params(settings)
-    stream = torch.cuda.current_stream()
-    sun = torch.empty((H_IMG, W_IMG, 4), dtype=torch.float32, device="cuda")
+    # a dedicated stream: the kernel and the CUDA events that time it share it
+    stream = torch.cuda.Stream()
+    if args.crop:
+        X0, Y0, TW, TH = crop_box(args.crop)
+    else:
+        X0, Y0, TW, TH = 0, 0, W_IMG, H_IMG
+    sun = torch.empty((TH, TW, 4), dtype=torch.float32, device="cuda")
     sky = torch.empty_like(sun)
     seed = 1000 + rank
 
     def step(k):
-        r.render_tile_async(0, 0, W_IMG, H_IMG, SPP, seed, k * SPP, sun.data_ptr(), sky.data_ptr(),
-                            stream.cuda_stream)
+        r.render_tile_async(X0, Y0, TW, TH, SPP, seed, k * SPP, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
 
     # L2 (126 MB) is flushed between timed steps by writing a 256 MB buffer
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    for k in range(args.warmup):
-        step(k)
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            step(k)
     torch.cuda.synchronize()
     r.reset_counters()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local) as clocks, torch.cuda.stream(stream):
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
@@ -281,14 +298,14 @@ def run_b200(args):
     t0 = time.perf_counter()
     for k in range(e2e_steps):
         r.set_params(settings)
-        a, b = r.render_tile(0, 0, W_IMG, H_IMG, SPP, seed=seed + 7, sample_base=k * SPP)
+        a, b = r.render_tile(X0, Y0, TW, TH, SPP, seed=seed, sample_base=(args.warmup + k) * SPP)
     t_e2e = (time.perf_counter() - t0)
     if world > 1:
         t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = float(t.item())
     e2e_value = (verts / args.steps) * e2e_steps / t_e2e  # same work per frame
-    d2h = 2 * H_IMG * W_IMG * 16
+    d2h = 2 * TH * TW * 16
 
     peak, peak_kind = measured_peak()
     bytes_per_step = (64.0 * cnt["node_visits"] + 32.0 * cnt["density_lookups"] + 24.0 * cnt["mie_evals"]) / args.steps
@@ -304,12 +321,16 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             threads = os.cpu_count() or 1
-            v_cpu, times = cpu_reference_sample(nodes, bricks, cfg, threads)
-            dt_cpu = times[0]
             x0, y0, tw, th = crop_box()
+            dt_cpu = cpu_reference_time(nodes, bricks, cfg, threads)
+            # the reference is not instrumented: its vertex count is this GPU's
+            # count on the same crop (the same estimator in expectation)
+            r.reset_counters()
+            r.render_tile(x0, y0, tw, th, SPP, seed=seed, sample_base=0)
+            v_cpu = r.counters()["vertices"]
             cpu = {"value": v_cpu / dt_cpu, "unit": "vertices/s", "cores": threads, "kind": "reference",
-                   "sample": f"{tw}x{th} centre crop at {SPP} spp, one run ({dt_cpu:.1f}s); vertices counted by "
-                             f"the CPU restatement on the same crop"}
+                   "sample": f"{tw}x{th} centre crop of the frame at {SPP} spp, one run of the reference renderer "
+                             f"({dt_cpu:.1f}s); vertex count measured by the GPU renderer on the same crop"}
         except Exception as e:  # the reference oracle needs oracle/_ref
             cpu = {"value": None, "unit": "vertices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
@@ -345,6 +366,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--crop", type=int, default=0, help="render only an NxN centre crop per step (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -16,7 +16,7 @@ Fixtures (all produced by the reference, none hand-written):
   ref_samplers.npz         reference Mie evaluate/sample, sun sample and brick
                            lookups (SampleVoxelSpace) on fixed inputs
   ref_c0_images.npz        two independent reference renders of config 0 at
-                           128x128, 4096 spp (sums), for the image parity gate
+                           128x128, 65536 spp (sums), for the image parity gate
 """
 from __future__ import annotations
 
@@ -114,7 +114,7 @@ def main():
 
     # two independent reference renders of config 0 at 128x128
     w = h = 128
-    spp = 4096
+    spp = 65536
     cfg = c0_config(ref, w, h, pdf, cdf)
     ref.set_threads(0)
     t = time.time()

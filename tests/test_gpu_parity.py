@@ -6,7 +6,7 @@ Bars (written into each test):
   * octree leaf sequences and (tr0, tr1), brick lookups, Mie table lookups: bit-exact;
   * whole path samples against the CPU restatement on the same streams: bit-exact;
   * images against the reference: relative bias <= 1% after removing the
-    reference's own Monte Carlo noise (two independent 4096-spp runs);
+    reference's own Monte Carlo noise (two independent 65536-spp runs);
   * transmittance against FP64 quadrature: <= 1e-4 relative.
 """
 import ctypes as C
@@ -24,6 +24,16 @@ def bits(a):
     return np.ascontiguousarray(a, np.float32).view(np.uint32)
 
 
+def same_floats(a, b):
+    """Bit-identical, except that any NaN matches any NaN: exactly axis-parallel
+    rays give NaN intervals on both sides, and the host's default NaN (sign bit
+    set) differs from the device's canonical NaN."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    nan = np.isnan(a) & np.isnan(b)
+    return a.shape == b.shape and bool(((a.view(np.uint32) == b.view(np.uint32)) | nan).all())
+
+
 def test_leaf_sequences_bit_exact_vs_reference_vectors(gpu_renderer):
     z = golden("ref_leaf_sequences.npz")
     maxn = z["nodes"].shape[1]
@@ -32,8 +42,8 @@ def test_leaf_sequences_bit_exact_vs_reference_vectors(gpu_renderer):
     for i in range(len(cnt)):
         k = int(cnt[i])
         assert np.array_equal(nodes[i, :k], z["nodes"][i, :k])
-        assert np.array_equal(bits(a[i, :k]), bits(z["tr0"][i, :k]))
-        assert np.array_equal(bits(b[i, :k]), bits(z["tr1"][i, :k]))
+        assert same_floats(a[i, :k], z["tr0"][i, :k])
+        assert same_floats(b[i, :k], z["tr1"][i, :k])
 
 
 def test_leaf_sequences_bit_exact_vs_port_random_rays(gpu_renderer, port):
@@ -51,7 +61,7 @@ def test_leaf_sequences_bit_exact_vs_port_random_rays(gpu_renderer, port):
         k = int(cnt[i])
         assert k == len(pn)
         assert np.array_equal(nodes[i, :k], pn)
-        assert np.array_equal(bits(a[i, :k]), bits(pa)) and np.array_equal(bits(b[i, :k]), bits(pb))
+        assert same_floats(a[i, :k], pa) and same_floats(b[i, :k], pb)
 
 
 def test_brick_lookup_bit_exact_vs_reference_vectors(gpu_renderer):
@@ -149,8 +159,8 @@ def _rel(x, y):
 
 
 def test_image_parity_vs_reference_renders():
-    """Config 0 at 128x128: GPU at 65536 spp against two independent reference
-    renders at 4096 spp.  The reference's own noise is measured from A vs B;
+    """Config 0 at 128x128: GPU at 2^18 spp against two independent, converged
+    reference renders at 65536 spp.  The reference's own noise is measured from A vs B;
     the remaining relative bias must stay within 1% for both buffers."""
     from droplet_b200.renderer import Renderer
     from droplet_b200.scene import Octree
@@ -162,11 +172,11 @@ def test_image_parity_vs_reference_renders():
     with Renderer(0) as r:
         r.upload(Octree(nodes, bricks, mlevel))
         r.set_params(settings_from_cfg(c0_cfg(w, w)))
-        spp_g = 65536
+        spp_g = 1 << 18
         sun = np.zeros((w, w, 4), np.float64)
         sky = np.zeros((w, w, 4), np.float64)
-        for k in range(spp_g // 8192):
-            a, b = r.render_tile(0, 0, w, w, 8192, seed=2024, sample_base=k * 8192)
+        for k in range(spp_g // 16384):
+            a, b = r.render_tile(0, 0, w, w, 16384, seed=2024, sample_base=k * 16384)
             sun += a
             sky += b
         cnt = r.counters()
