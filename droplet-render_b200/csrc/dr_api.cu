@@ -531,4 +531,23 @@ int dr_probe_transmittance(dr_ctx *c, const float *ro, const float *rd, uint32_t
     return DR_OK;
 }
 
+int dr_transmittance_noalloc(dr_ctx *c, const float *ro_dev, const float *rd_dev, uint32_t n_rays, uint64_t nsamp,
+                             uint64_t seed, double *out_dev, void *stream) {
+    if (!c || !ro_dev || !rd_dev || !out_dev || n_rays == 0 || nsamp == 0)
+        return need(false, DR_ERR_INVALID, "dr_transmittance_noalloc: bad argument");
+    if (n_rays > noalloc_max_rays())
+        return need(false, DR_ERR_INVALID,
+                    "dr_transmittance_noalloc: n_rays exceeds DR_NOALLOC_MAX_RAYS (65536); split the batch");
+    if (!c->has_scene || !c->has_params)
+        return need(false, DR_ERR_STATE, "dr_transmittance_noalloc: upload a scene and set parameters first");
+    DeviceGuard g(c->device);
+    unsigned long long *scratch = nullptr;
+    DR_CUDA(noalloc_scratch(c->device, &scratch), "dr_transmittance_noalloc: scratch address");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    DR_CUDA(launch_transmittance_noalloc(c->scene, c->params, scratch, ro_dev, rd_dev, n_rays, nsamp, seed, out_dev,
+                                         st),
+            "dr_transmittance_noalloc: launch");
+    return DR_OK;
+}
+
 }  // extern "C"

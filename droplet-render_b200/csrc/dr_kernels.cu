@@ -1,5 +1,6 @@
 // Kernels of the droplet_b200 hot path and their launchers.
 #include <cstdio>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "dr_device.cuh"
 #include "dr_kernels.h"
@@ -232,6 +233,56 @@ __global__ void probe_transmittance_kernel(DevScene S, DevParams P, const float 
         esc += track(S, P, o, d, g, 3.402823466e+38f, td, nstack, cnt) ? 1u : 0u;
     }
     atomicAdd(&escapes[r], (unsigned long long)esc);
+}
+
+// ---- transmittance without allocation ----------------------------------------------
+// Scratch of the allocation-free entry point: one escape counter per ray in a
+// file-scope device array (512 KB on every GPU that loads the library, for the
+// life of the process).  Every call shares it, so calls that overlap on the
+// GPU race; each call clears the counters it uses before counting.
+constexpr uint32_t kNoAllocMaxRays = 65536;
+static __device__ __align__(256) unsigned long long g_noalloc_escapes[kNoAllocMaxRays];
+
+__global__ void noalloc_clear_kernel(unsigned long long *escapes, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) escapes[i] = 0ull;
+}
+
+__global__ void noalloc_finish_kernel(const unsigned long long *escapes, uint32_t n, uint64_t nsamp, double *out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)escapes[i] / (double)nsamp;
+}
+
+uint32_t noalloc_max_rays() { return kNoAllocMaxRays; }
+
+// Device address of the scratch array, looked up once per device (with that
+// device current) and cached.
+static std::mutex g_noalloc_mu;
+static unsigned long long *g_noalloc_ptr[64] = {nullptr};
+
+cudaError_t noalloc_scratch(int device, unsigned long long **out) {
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_escapes);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[device] = static_cast<unsigned long long *>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+
+cudaError_t launch_transmittance_noalloc(const DevScene &S, const DevParams &P, unsigned long long *scratch,
+                                         const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,
+                                         uint64_t seed, double *out, cudaStream_t st) {
+    noalloc_clear_kernel<<<(n_rays + 255) / 256, 256, 0, st>>>(scratch, n_rays);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = launch_probe_transmittance(S, P, ro, rd, n_rays, nsamp, seed, scratch, st);
+    if (e != cudaSuccess) return e;
+    noalloc_finish_kernel<<<(n_rays + 255) / 256, 256, 0, st>>>(scratch, n_rays, nsamp, out);
+    return cudaGetLastError();
 }
 
 // ---- launchers ------------------------------------------------------------------

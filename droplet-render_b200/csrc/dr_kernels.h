@@ -22,4 +22,11 @@ cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, co
                                        uint32_t n_rays, uint64_t nsamp, uint64_t seed, unsigned long long *escapes,
                                        cudaStream_t st);
 
+// Allocation-free transmittance: scratch in a file-scope device array.
+uint32_t noalloc_max_rays();
+cudaError_t noalloc_scratch(int device, unsigned long long **out);
+cudaError_t launch_transmittance_noalloc(const DevScene &S, const DevParams &P, unsigned long long *scratch,
+                                         const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,
+                                         uint64_t seed, double *out, cudaStream_t st);
+
 }  // namespace dr

@@ -148,7 +148,13 @@ SIGNATURES = {
         C.c_int,
         [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p],
     ),
+    "dr_transmittance_noalloc": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p],
+    ),
 }
+
+DR_NOALLOC_MAX_RAYS = 65536
 
 _lib = None
 _lock = threading.Lock()

@@ -172,6 +172,32 @@ int dr_probe_sampler(dr_ctx *ctx, uint32_t what, const float *in, uint32_t n, fl
 int dr_probe_transmittance(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,
                            uint64_t seed, double *out);
 
+/* ---- transmittance for callers that cannot allocate ------------------------
+ * This entry point has no counterpart in the reference.  It serves callers that
+ * cannot let this library allocate device memory.  One example is an
+ * application that owns the GPU's memory budget, such as a host renderer
+ * sharing the device.  Another is a caller whose other streams cannot afford
+ * the device-wide synchronisation that cudaMalloc and cudaFree can cause.
+ *
+ * The call allocates nothing.  The caller passes device buffers for the rays
+ * (ro_dev and rd_dev, 3 floats per ray) and for the result (out_dev, one double
+ * per ray).  The result is the fraction of nsamp delta-tracked segments that
+ * escape, drawn from the same streams as dr_probe_transmittance.
+ *
+ * The per-ray counters live in a fixed device array of DR_NOALLOC_MAX_RAYS
+ * entries (512 KB).  Every GPU that loads the library holds it until the
+ * process exits.  Larger batches are rejected with DR_ERR_INVALID.
+ *
+ * The first call on a device looks up the array's address and caches it, so
+ * make that first call before any stream capture.  All calls share the array,
+ * so calls that overlap on the GPU race.
+ *
+ * The work is enqueued on `stream` (NULL = the context stream) and the call
+ * returns without waiting. */
+#define DR_NOALLOC_MAX_RAYS 65536u
+int dr_transmittance_noalloc(dr_ctx *ctx, const float *ro_dev, const float *rd_dev, uint32_t n_rays, uint64_t nsamp,
+                             uint64_t seed, double *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
