@@ -247,6 +247,18 @@ def run_b200(args):
     sun = torch.empty((TH, TW, 4), dtype=torch.float32, device="cuda")
     sky = torch.empty_like(sun)
     seed = 1000 + rank
+    tuning = {"kernel": "persistent", "choice": list(r.get_tuning()), "tuned": False}
+    if args.tuning:
+        r.set_tuning(*[int(v) for v in args.tuning.split(",")])
+        tuning = {"choice": list(r.get_tuning()), "tuned": False, "fixed": True}
+    elif not args.no_tune:
+        from droplet_b200 import autotune
+
+        t = time.time()
+        best, table = autotune.tune(r, (X0, Y0, TW, TH), 8, key=f"c1-{TW}x{TH}", use_cache=False)
+        tuning = {"choice": list(best), "tuned": True, "seconds": round(time.time() - t, 2),
+                  "candidates_ms_at_8spp": [[c, round(ms, 3)] for c, ms in table]}
+        log(f"autotune: best {best} in {time.time() - t:.1f}s")
 
     def step(k):
         r.render_tile_async(X0, Y0, TW, TH, SPP, seed, k * SPP, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
@@ -342,7 +354,8 @@ def run_b200(args):
             "config": {"workload": "c1 single large cumulus 512^3 (plain renderer)", "image": [W_IMG, H_IMG],
                        "spp": SPP, "scattevs": 64, "sigma_t": 60.0, "albedo": 0.999, "leaves": int(len(bricks)),
                        "nodes": int(len(nodes)), "octree_depth": int(mlevel), "occupancy": occ,
-                       "l2": "flushed between steps (256 MB write)"},
+                       "l2": "flushed between steps (256 MB write)", "region": [X0, Y0, TW, TH],
+                       "tuning": tuning},
             "e2e": {"value": e2e_value, "unit": "vertices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "gpu_launches": args.steps,
@@ -367,6 +380,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--crop", type=int, default=0, help="render only an NxN centre crop per step (profiling)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal (no tuning)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

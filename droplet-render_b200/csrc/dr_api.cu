@@ -76,6 +76,10 @@ struct dr_ctx {
     DevBuf<DevCounters> counters;
     DevBuf<float4> tile_sun, tile_sky;
     DevBuf<unsigned char> scratch;
+    DevBuf<WorkQueue> work;
+    DevBuf<uint32_t> macro, cells;
+    bool use_grid = true;
+    Tuning tuning{0u, 128u, 0u, 8u, 0u};
     std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)
 };
 
@@ -137,6 +141,7 @@ int dr_create(int device, dr_ctx **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = c->counters.reserve(1);
     if (e == cudaSuccess) e = cudaMemset(c->counters.p, 0, sizeof(DevCounters));
+    if (e == cudaSuccess) e = c->work.reserve(1);
     if (e != cudaSuccess) {
         int r = cuda_fail(e, "dr_create");
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -163,6 +168,9 @@ int dr_destroy(dr_ctx *c) {
         c->tile_sun.release();
         c->tile_sky.release();
         c->scratch.release();
+        c->work.release();
+        c->macro.release();
+        c->cells.release();
         if (c->stream) cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -227,10 +235,61 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
             child[8 * (size_t)i + k] = is_leaf(ch) ? (ch | kLeafBit) : ch;
         }
     }
+    // Leaf grid for the cell-walk traversal: valid when the tree is a tree (each
+    // node reached once from the root) and every leaf sits at the same depth.
+    std::vector<uint32_t> macro, cells;
+    uint32_t levels = 0, n = 0, mdim = 0;
+    {
+        struct Item { uint32_t node, depth, x, y, z; };
+        std::vector<Item> stack{{0u, 0u, 0u, 0u, 0u}};
+        std::vector<uint8_t> seen(s->n_nodes, 0);
+        std::vector<Item> leaves;
+        bool ok = true;
+        int leaf_depth = -1;
+        while (!stack.empty() && ok) {
+            Item it = stack.back();
+            stack.pop_back();
+            if (seen[it.node] || it.depth > 11) { ok = false; break; }
+            seen[it.node] = 1;
+            if (is_leaf(it.node)) {
+                if (leaf_depth < 0) leaf_depth = (int)it.depth;
+                if ((int)it.depth != leaf_depth) ok = false;
+                leaves.push_back(it);
+                continue;
+            }
+            for (uint32_t k = 0; k < 8; ++k) {
+                const uint32_t ch = N[it.node].chn[k];
+                if (ch) stack.push_back({ch, it.depth + 1, 2 * it.x + (k & 1), 2 * it.y + ((k >> 1) & 1), 2 * it.z + (k >> 2)});
+            }
+        }
+        if (ok && leaf_depth >= 1) {
+            levels = (uint32_t)leaf_depth;
+            n = 1u << levels;
+            mdim = n >= 8 ? n / 8 : 1;
+            macro.assign((size_t)mdim * mdim * mdim, kNone);
+            for (const Item &lf : leaves) {
+                const size_t m = ((size_t)(lf.z >> 3) * mdim + (lf.y >> 3)) * mdim + (lf.x >> 3);
+                if (macro[m] == kNone) {
+                    macro[m] = (uint32_t)(cells.size() / 512);
+                    cells.resize(cells.size() + 512, kNone);
+                }
+                cells[(size_t)macro[m] * 512 + (lf.z & 7) * 64 + (lf.y & 7) * 8 + (lf.x & 7)] = lf.node;
+            }
+        } else {
+            macro.assign(1, kNone);
+        }
+        if (cells.empty()) cells.assign(512, kNone);
+    }
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t nb = (size_t)s->n_leaves * kBrick;
     DR_CUDA(cudaStreamSynchronize(c->stream), "dr_upload_scene: sync");
+    DR_CUDA(c->macro.reserve(macro.size()), "dr_upload_scene: alloc grid");
+    DR_CUDA(c->cells.reserve(cells.size()), "dr_upload_scene: alloc grid");
+    DR_CUDA(cudaMemcpyAsync(c->macro.p, macro.data(), macro.size() * 4, cudaMemcpyHostToDevice, c->stream),
+            "dr_upload_scene: copy grid");
+    DR_CUDA(cudaMemcpyAsync(c->cells.p, cells.data(), cells.size() * 4, cudaMemcpyHostToDevice, c->stream),
+            "dr_upload_scene: copy grid");
     DR_CUDA(c->child.reserve((size_t)s->n_nodes * 2), "dr_upload_scene: alloc nodes");
     DR_CUDA(c->leaf.reserve((size_t)s->n_nodes * 2), "dr_upload_scene: alloc leaves");
     DR_CUDA(c->bricks.reserve(nb + 1), "dr_upload_scene: alloc bricks");
@@ -248,6 +307,11 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
     for (int k = 0; k < 4; ++k) c->scene.root_ce[k] = N[0].ce[k];
     c->scene.n_nodes = s->n_nodes;
     c->scene.n_leaves = s->n_leaves;
+    c->scene.macro = c->macro.p;
+    c->scene.cells = c->cells.p;
+    c->scene.levels = c->use_grid ? levels : 0u;
+    c->scene.n = n;
+    c->scene.mdim = mdim;
     c->leaf_flag.assign(s->n_nodes, 0);
     for (uint32_t i = 0; i < s->n_nodes; ++i) c->leaf_flag[i] = is_leaf(i) ? 1 : 0;
     c->has_scene = true;
@@ -343,9 +407,37 @@ int dr_render_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint3
     const size_t bytes = (size_t)tw * th * sizeof(float4);
     DR_CUDA(cudaMemsetAsync(sun_dev, 0, bytes, st), "render: clear");
     DR_CUDA(cudaMemsetAsync(sky_dev, 0, bytes, st), "render: clear");
-    DR_CUDA(launch_render_tile(c->scene, c->params, A, c->mie_pack.p, (float4 *)sun_dev, (float4 *)sky_dev,
-                               c->counters.p, st),
-            "render: launch");
+    if (c->tuning.kernel == DR_KERNEL_PER_PATH) {
+        DR_CUDA(launch_render_tile(c->scene, c->params, A, c->mie_pack.p, (float4 *)sun_dev, (float4 *)sky_dev,
+                                   c->counters.p, st),
+                "render: launch");
+    } else {
+        DR_CUDA(launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, (float4 *)sun_dev, (float4 *)sky_dev,
+                                         c->counters.p, c->work.p, c->tuning, c->device, st),
+                "render: launch");
+    }
+    return DR_OK;
+}
+
+int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
+    if (!c || !t) return need(false, DR_ERR_INVALID, "dr_set_tuning: null argument");
+    if (t->kernel > DR_KERNEL_PER_PATH || t->event_batch > 32 || t->blocks_per_sm > 64 || t->traversal > 1)
+        return need(false, DR_ERR_INVALID,
+                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1");
+    c->tuning.kernel = t->kernel;
+    c->tuning.block = kPersistentBlock;
+    c->tuning.blocks_per_sm = t->blocks_per_sm;
+    c->tuning.event_batch = t->event_batch;
+    c->tuning.traversal = t->traversal;
+    return DR_OK;
+}
+
+int dr_get_tuning(dr_ctx *c, dr_tuning *t) {
+    if (!c || !t) return need(false, DR_ERR_INVALID, "dr_get_tuning: null argument");
+    t->kernel = c->tuning.kernel;
+    t->blocks_per_sm = c->tuning.blocks_per_sm;
+    t->event_batch = c->tuning.event_batch;
+    t->traversal = c->tuning.traversal;
     return DR_OK;
 }
 

@@ -323,6 +323,178 @@ __device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *
     }
 }
 
+// ---- cell walk: the same leaf sequence without a stack -----------------------
+// When every leaf sits at one depth L, the Revelles traversal above visits leaf
+// cells of a 2^L grid.  Every t value it compares is a plane value: the root's
+// (t0, t1) per axis, or a midpoint 0.5f*(lo + hi) of two coarser planes, so
+// plane(k, i) for plane index i in [0, 2^L] is recomputed exactly by descending
+// the binary subdivision (grid_plane).  In the mirrored frame:
+//  * the first leaf is the cell containing te = max(t0) (first_node picks, at
+//    every level, the upper half of axis k iff tm_k < te);
+//  * leaving a cell, next_node moves across the exit plane with the smallest t,
+//    ties going to z, then y, then x; this choice is the same at every tree
+//    level, since an ancestor's exit planes are never nearer than the cell's;
+//  * entering the sibling subtree (2^t cells per axis, t = trailing zeros of the
+//    new index), first_node's descent gives, in every other axis k, the cell
+//    holding te = the crossed plane's t; that is the current cell unless its
+//    entry plane equals te (a tie), which is the only case that re-descends;
+//  * a cell is reported when it holds a leaf and no exit plane is negative (the
+//    reference prunes nodes with any t1 < 0).
+// Rays with a zero direction component give NaN planes, for which the tree's
+// tie handling differs level by level: they use the stack traversal.  Empty
+// 8^3 macro cells are crossed in one step with their macro-level exit planes.
+struct Walk {
+    float t0r[3], t1r[3];
+    float N[3], X[3];      // entry / exit planes of the current cell
+    uint32_t c[3];         // current leaf cell, mirrored frame
+    uint32_t a;            // mirror bits, x = 4, y = 2, z = 1
+    bool macro_mode;       // current macro cell is empty: step at macro granularity
+    bool check;            // current cell not yet examined
+};
+
+// Plane value of plane index i in [0, n] between the root planes (lo, hi).
+__device__ __forceinline__ float grid_plane(float lo, float hi, uint32_t i, uint32_t n) {
+    if (i == 0) return lo;
+    if (i >= n) return hi;
+    uint32_t base = 0, span = n;
+    for (int it = 0; it < 16; ++it) {
+        span >>= 1;
+        const float mid = 0.5f * (lo + hi);
+        const uint32_t m = base + span;
+        if (i == m) return mid;
+        if (i < m) {
+            hi = mid;
+        } else {
+            lo = mid;
+            base = m;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ float sel3(int k, float a, float b, float c) { return k == 0 ? a : (k == 1 ? b : c); }
+
+// first_node's descent inside [base, base + 2^t) of one axis for entry te:
+// the cell index and its entry / exit planes.
+__device__ __forceinline__ void grid_descend(float r0, float r1, uint32_t base, uint32_t t, float te, uint32_t n,
+                                             uint32_t &c, float &N, float &X) {
+    float lo = grid_plane(r0, r1, base, n), hi = grid_plane(r0, r1, base + (1u << t), n);
+    uint32_t cc = base, span = 1u << t;
+    for (uint32_t l = 0; l < t; ++l) {
+        span >>= 1;
+        const float mid = 0.5f * (lo + hi);
+        if (mid < te) {
+            lo = mid;
+            cc += span;
+        } else {
+            hi = mid;
+        }
+    }
+    c = cc;
+    N = lo;
+    X = hi;
+}
+
+__device__ __forceinline__ uint32_t grid_macro(const Walk &W, const DevScene &S) {
+    const uint32_t x = ((W.a & 4u) ? S.n - 1 - W.c[0] : W.c[0]) >> 3;
+    const uint32_t y = ((W.a & 2u) ? S.n - 1 - W.c[1] : W.c[1]) >> 3;
+    const uint32_t z = ((W.a & 1u) ? S.n - 1 - W.c[2] : W.c[2]) >> 3;
+    return __ldg(&S.macro[((size_t)z * S.mdim + y) * S.mdim + x]);
+}
+
+__device__ __forceinline__ void grid_macro_planes(Walk &W, const DevScene &S) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t b = ((W.c[k] >> 3) + 1) << 3;
+        W.X[k] = grid_plane(W.t0r[k], W.t1r[k], b < S.n ? b : S.n, S.n);
+    }
+}
+
+// Returns 0: no leaf on this ray, 1: walk ready, 2: use the stack traversal.
+__device__ __forceinline__ uint32_t walk_init(Walk &W, const DevScene &S, const float ro[3], const float rd[3],
+                                              Count &cnt) {
+    float ros[3], rds[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ros[k] = (ro[k] - S.root_ce[k]) + S.root_ce[3];
+        rds[k] = rd[k];
+    }
+    uint32_t a = 0;
+    if (rds[0] < 0.0f) { ros[0] = 2.0f * S.root_ce[3] - ros[0]; rds[0] = -rds[0]; a |= 4; }
+    if (rds[1] < 0.0f) { ros[1] = 2.0f * S.root_ce[3] - ros[1]; rds[1] = -rds[1]; a |= 2; }
+    if (rds[2] < 0.0f) { ros[2] = 2.0f * S.root_ce[3] - ros[2]; rds[2] = -rds[2]; a |= 1; }
+    const float mx = 2.0f * S.root_ce[3];
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        W.t0r[k] = (0.0f - ros[k]) / rds[k];
+        W.t1r[k] = (mx - ros[k]) / rds[k];
+        finite = finite && (rds[k] != 0.0f) && isfinite(W.t0r[k]) && isfinite(W.t1r[k]);
+    }
+    if (!finite || S.levels == 0) return 2u;
+    W.a = a;
+    if (!(std_max(std_max(W.t0r[0], W.t0r[1]), W.t0r[2]) < std_min(std_min(W.t1r[0], W.t1r[1]), W.t1r[2])))
+        return 0u;
+    if (W.t1r[0] < 0.0f || W.t1r[1] < 0.0f || W.t1r[2] < 0.0f) return 0u;
+    ++cnt.node_visits;  // the root
+    const float te = std_max(std_max(W.t0r[0], W.t0r[1]), W.t0r[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) grid_descend(W.t0r[k], W.t1r[k], 0u, S.levels, te, S.n, W.c[k], W.N[k], W.X[k]);
+    W.macro_mode = grid_macro(W, S) == kNone;
+    if (W.macro_mode) grid_macro_planes(W, S);
+    W.check = true;
+    return 1u;
+}
+
+// One step of the walk.  Returns 1 with a reported leaf, 0 after moving to the
+// next cell (call again), 2 when the ray leaves the root box.
+__device__ __forceinline__ uint32_t walk_step(Walk &W, const DevScene &S, uint32_t &leaf, float &tra, float &trb,
+                                              Count &cnt) {
+    if (W.check) {
+        W.check = false;
+        if (!W.macro_mode) {
+            const uint32_t blk = grid_macro(W, S);
+            const uint32_t x = ((W.a & 4u) ? S.n - 1 - W.c[0] : W.c[0]) & 7u;
+            const uint32_t y = ((W.a & 2u) ? S.n - 1 - W.c[1] : W.c[1]) & 7u;
+            const uint32_t z = ((W.a & 1u) ? S.n - 1 - W.c[2] : W.c[2]) & 7u;
+            const uint32_t id = __ldg(&S.cells[(size_t)blk * 512u + z * 64u + y * 8u + x]);
+            ++cnt.node_visits;
+            if (id != kNone && !(W.X[0] < 0.0f) && !(W.X[1] < 0.0f) && !(W.X[2] < 0.0f)) {
+                leaf = id;
+                tra = std_max(std_max(W.N[0], W.N[1]), W.N[2]);
+                trb = std_min(std_min(W.X[0], W.X[1]), W.X[2]);
+                return 1u;
+            }
+        }
+    }
+    const int ax = (W.X[0] < W.X[1]) ? ((W.X[0] < W.X[2]) ? 0 : 2) : ((W.X[1] < W.X[2]) ? 1 : 2);
+    const uint32_t cax = ax == 0 ? W.c[0] : (ax == 1 ? W.c[1] : W.c[2]);
+    const uint32_t b = W.macro_mode ? ((cax >> 3) + 1) << 3 : cax + 1;
+    if (b >= S.n) return 2u;
+    const float Xa = sel3(ax, W.X[0], W.X[1], W.X[2]);
+    const uint32_t t = (uint32_t)(__ffs((int)b) - 1);
+    const bool was_macro = W.macro_mode;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k == ax) {
+            W.c[k] = b;
+            W.N[k] = Xa;
+        } else if (was_macro || (t != 0u && !(W.N[k] < Xa))) {
+            grid_descend(W.t0r[k], W.t1r[k], W.c[k] & ~((1u << t) - 1u), t, Xa, S.n, W.c[k], W.N[k], W.X[k]);
+        }
+    }
+    W.macro_mode = grid_macro(W, S) == kNone;
+    if (W.macro_mode) {
+        grid_macro_planes(W, S);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k == ax) W.X[k] = grid_plane(W.t0r[k], W.t1r[k], b + 1u, S.n);
+    }
+    W.check = true;
+    return 0u;
+}
+
 // ---- brick lookup: SampleVoxelSpace, src/kernel.cpp:96-126 ----------------
 __device__ __forceinline__ float sample_voxel_space(const float p[3], const float *__restrict__ v, const float4 ce) {
     const float nm1 = (float)kLvox - 1.0f;

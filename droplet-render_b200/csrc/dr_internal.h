@@ -32,6 +32,15 @@ struct DevScene {
     float root_ce[4];
     uint32_t n_nodes;
     uint32_t n_leaves;
+    // Leaf grid for the cell-walk traversal (all leaves at one depth):
+    // n = 2^levels leaf cells per axis; macro cells of 8^3 leaf cells;
+    // macro[mz][my][mx] = block index or kNone (no leaf in the macro cell);
+    // cells[block*512 + z*64 + y*8 + x] = leaf node id or kNone.
+    const uint32_t *macro;
+    const uint32_t *cells;
+    uint32_t levels;     // leaf depth below the root (0 = no grid; stack traversal only)
+    uint32_t n;          // leaf cells per axis
+    uint32_t mdim;       // macro cells per axis
 };
 
 struct DevParams {
@@ -59,6 +68,20 @@ struct TileArgs {
 
 struct DevCounters {
     unsigned long long paths, vertices, node_visits, density_lookups, mie_evals, gave_up;
+};
+
+// Launch-shape choices of the persistent renderer (chosen by the autotuner).
+struct Tuning {
+    uint32_t kernel;        // 0 = persistent path kernel, 1 = one thread per path
+    uint32_t block;         // threads per block (multiple of 32)
+    uint32_t blocks_per_sm; // 0 = as many as fit
+    uint32_t event_batch;   // lanes of a warp that must be waiting before events run
+    uint32_t traversal;     // 0 = octree stack traversal, 1 = leaf-grid cell walk
+};
+
+// Work queue of the persistent kernel: next path index to hand out.
+struct WorkQueue {
+    unsigned long long next;
 };
 
 }  // namespace dr

@@ -122,24 +122,373 @@ __global__ void __launch_bounds__(kRenderBlock) render_tile_kernel(DevScene S, D
     warp_sum_counts(cnt, C, paths);
 }
 
+// ---- persistent path kernel ------------------------------------------------------
+// Each lane of a resident warp holds one path sample as a small state machine
+// and takes the next path from a global counter as soon as its path ends, so
+// lanes never idle behind a warp-mate's long path.  One loop iteration does
+// one unit of work per lane:
+//   kTrav  advance the octree traversal to the next leaf (then fall into kStep)
+//   kStep  one free-flight step of delta tracking inside the current leaf
+//   kEvent a segment ended (escape or collision): shade, start the next segment
+// Events are the long, divergent part (phase/sun sampling, sky radiance); a
+// warp runs them only when at least `event_batch` of its lanes wait on one, or
+// when nothing else is left, so the common tracking step stays converged.
+// Per path, the operations and random draws are those of path_sample()/track():
+// a path's result is bit-identical to the one-thread-per-path kernel.
+enum : uint32_t { kFetch = 0, kTrav = 1, kStep = 2, kEvent = 3, kDone = 4 };
+enum : uint32_t { kSegMain = 0, kSegShadow = 1 };
+
+template <bool WALK> struct SegTrav;
+template <> struct SegTrav<true> { Walk w; };
+template <> struct SegTrav<false> { Trav t; };
+
+template <bool WALK>
+struct PathLane {
+    // path
+    uint32_t px, py;
+    Rng g;
+    float ro[3], rd[3];
+    float T[3];
+    float4 sun, sky;
+    uint32_t r, seg;
+    float srd[3], tn[3], sw[3];  // pending continuation while the shadow segment runs
+    // segment
+    SegTrav<WALK> st;
+    uint32_t wmode;  // 0 no leaf on the ray, 1 cell walk, 2 stack traversal in local memory, 3 stack traversal
+    float td, depth;
+    uint32_t budget;
+    bool esc;
+    // leaf
+    float lo, tr0, tr1, trb, s0, sr, smax, denom;
+    float4 ce;
+    const float *brick;
+};
+
+// Stack traversal for the rare segments the cell walk does not take (a zero
+// direction component).  Its state lives in local memory; arguments and results
+// travel by value so that no lane state has its address taken.
+struct SlowLeaf {
+    uint32_t ok, leaf, visits;
+    float tra, trb;
+};
+
+__device__ __noinline__ uint32_t slow_init(Trav *T, DevScene S, float ox, float oy, float oz, float dx, float dy,
+                                           float dz) {
+    const float o[3] = {ox, oy, oz}, d[3] = {dx, dy, dz};
+    Count c;
+    c.zero();
+    trav_init(*T, S, o, d, c);
+    return c.node_visits;
+}
+
+__device__ __noinline__ SlowLeaf slow_next(Trav *T, DevScene S, uint32_t *nstack) {
+    SlowLeaf r;
+    Count c;
+    c.zero();
+    r.leaf = 0;
+    r.tra = r.trb = 0.0f;
+    r.ok = trav_next(*T, S, nstack, r.leaf, r.tra, r.trb, c) ? 1u : 0u;
+    r.visits = c.node_visits;
+    return r;
+}
+
+template <bool WALK>
+__device__ __forceinline__ void begin_segment(PathLane<WALK> &L, const DevScene &S, Count &cnt, uint32_t &state,
+                                              Trav *slow) {
+    if constexpr (WALK) {
+        L.wmode = walk_init(L.st.w, S, L.ro, L.rd, cnt);
+        if (L.wmode == 2u)
+            cnt.node_visits += slow_init(slow, S, L.ro[0], L.ro[1], L.ro[2], L.rd[0], L.rd[1], L.rd[2]);
+    } else {
+        trav_init(L.st.t, S, L.ro, L.rd, cnt);
+        L.wmode = L.st.t.active ? 3u : 0u;
+    }
+    ++cnt.vertices;
+    L.td = 0.0f;
+    L.budget = kStepBudget;
+    state = kTrav;
+}
+
+template <bool WALK>
+__device__ __forceinline__ void finish_path(PathLane<WALK> &L, const TileArgs &A, float4 *sun_out, float4 *sky_out) {
+    const bool any = (L.sun.x != 0.0f) | (L.sun.y != 0.0f) | (L.sun.z != 0.0f) | (L.sun.w != 0.0f) |
+                     (L.sky.x != 0.0f) | (L.sky.y != 0.0f) | (L.sky.z != 0.0f) | (L.sky.w != 0.0f);
+    if (any) {
+        const size_t o = (size_t)(L.py - A.y0) * A.tw + (L.px - A.x0);
+        atomicAdd(&sun_out[o], L.sun);
+        atomicAdd(&sky_out[o], L.sky);
+    }
+}
+
+// One traversal step.  Returns 0 after moving to another cell (call again), 1
+// when a leaf was entered and its free flight prepared, 2 when the segment has
+// no further leaf (or the depth mask stops it): the segment escaped.
+template <bool WALK>
+__device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
+                                              uint32_t *nstack, Trav *slow, Count &cnt) {
+    uint32_t leaf = 0;
+    float tra = 0.0f, trb = 0.0f;
+    uint32_t r;
+    if constexpr (!WALK) {
+        r = (L.wmode == 3u && trav_next(L.st.t, S, nstack, leaf, tra, trb, cnt)) ? 1u : 2u;
+    } else if (L.wmode == 1u) {
+        r = walk_step(L.st.w, S, leaf, tra, trb, cnt);
+    } else if (L.wmode == 2u) {
+        const SlowLeaf sl = slow_next(slow, S, nstack);
+        cnt.node_visits += sl.visits;
+        r = sl.ok ? 1u : 2u;
+        leaf = sl.leaf;
+        tra = sl.tra;
+        trb = sl.trb;
+    } else {
+        r = 2u;
+    }
+    if (r != 1u) return r;
+    if (!(L.td < L.depth)) return 2u;
+    L.ce = __ldg(&S.leaf[2 * leaf]);
+    const float4 meta = __ldg(&S.leaf[2 * leaf + 1]);
+    L.smax = meta.x;
+    L.brick = S.bricks + (size_t)__float_as_uint(meta.y) * kBrick;
+    L.lo = L.td;
+    L.tr0 = tra - L.td;
+    L.tr1 = trb - L.td;
+    L.trb = trb;
+    if (tra > L.td) {
+        L.td = tra;
+        L.s0 = L.tr0;
+    } else {
+        L.td = __uint_as_float((__float_as_uint(L.td) & ~1u) | (__float_as_uint(tra) & 1u));
+        L.s0 = __uint_as_float(__float_as_uint(L.tr0) & 1u);
+    }
+    L.denom = P.sigma_e * L.smax;
+    L.sr = -dlog(L.g.uniform()) / L.denom;
+    return 1u;
+}
+
+// One delta-tracking step.  Returns 0 = continue in this leaf, 1 = leaf left,
+// 2 = segment ended (collision, or the step budget ran out).
+template <bool WALK>
+__device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
+    const float sc = L.s0 + L.sr;
+    L.td = L.lo + sc;
+    if (!(sc < L.tr1)) {
+        L.td = L.trb;
+        return 1;
+    }
+    bool rm = sc > L.tr0;
+    float rho = -1.0f;
+    if (rm) {
+        const float rc[3] = {L.ro[0] + L.rd[0] * L.td, L.ro[1] + L.rd[1] * L.td, L.ro[2] + L.rd[2] * L.td};
+        rho = sample_voxel_space(rc, L.brick, L.ce);
+        ++cnt.density_lookups;
+    }
+    const float q = L.g.uniform();
+    rm = rm && (rho / L.smax < q);
+    if (!rm) {
+        L.esc = false;
+        return 2;
+    }
+    if (--L.budget == 0) {
+        ++cnt.gave_up;
+        L.esc = true;
+        return 2;
+    }
+    L.sr = L.sr - dlog(L.g.uniform()) / L.denom;
+    return 0;
+}
+
+// Segment end: the body of path_sample() between two track() calls.
+template <bool WALK>
+__device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
+                                        const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
+                                        uint32_t &state, Trav *slow) {
+    const float f = P.albedo;
+    if (L.seg == kSegShadow) {
+        if (L.esc) {
+            const bool hit = sun_hit(P, L.rd);
+            const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
+                        s2 = hit ? P.sun_color[2] : 0.0f;
+            L.sun.x = L.sun.x + L.sw[0] * s0;
+            L.sun.y = L.sun.y + L.sw[1] * s1;
+            L.sun.z = L.sun.z + L.sw[2] * s2;
+        }
+        for (int k = 0; k < 3; ++k) {
+            L.T[k] = L.tn[k];
+            L.rd[k] = L.srd[k];
+        }
+        L.r += 1;
+        L.seg = kSegMain;
+        L.depth = 3.402823466e+38f;
+        begin_segment(L, S, cnt, state, slow);
+        return;
+    }
+    if (L.r == 0) L.sun.w = L.sky.w = L.esc ? 0.0f : 1.0f;
+    if (L.esc) {
+        if (L.r > 0) {
+            if (sun_hit(P, L.rd)) {
+                L.sun.x = L.sun.x + L.T[0] * P.sun_color[0];
+                L.sun.y = L.sun.y + L.T[1] * P.sun_color[1];
+                L.sun.z = L.sun.z + L.T[2] * P.sun_color[2];
+            } else {
+                L.sun.x = L.sun.x + L.T[0] * 0.0f;
+                L.sun.y = L.sun.y + L.T[1] * 0.0f;
+                L.sun.z = L.sun.z + L.T[2] * 0.0f;
+            }
+            const float3 sky = sky_eval(P, L.rd);
+            L.sky.x = L.sky.x + L.T[0] * sky.x;
+            L.sky.y = L.sky.y + L.T[1] * sky.y;
+            L.sky.z = L.sky.z + L.T[2] * sky.z;
+        }
+        finish_path(L, A, sun_out, sky_out);
+        state = kFetch;
+        return;
+    }
+    if (L.r >= P.scattevs) {
+        finish_path(L, A, sun_out, sky_out);
+        state = kFetch;
+        return;
+    }
+    float lrd[3];
+    const float u1 = L.g.uniform(), u2 = L.g.uniform();
+    mie_sample(M, L.rd, u1, u2, L.srd);
+    const float u3 = L.g.uniform(), u4 = L.g.uniform();
+    sun_sample(P, u3, u4, lrd);
+    const float3 p1 = mie_eval_rgb(M, dot3(L.srd, L.rd));
+    const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
+    const float3 p3 = mie_eval_rgb(M, dot3(lrd, L.rd));
+    const float q1 = sun_hit(P, L.srd) ? P.sun_pdf : 0.0f;
+    cnt.mie_evals += 3;
+    L.sw[0] = L.T[0] * ((p3.x / (p3.x + p2)) * f);
+    L.sw[1] = L.T[1] * ((p3.y / (p3.y + p2)) * f);
+    L.sw[2] = L.T[2] * ((p3.z / (p3.z + p2)) * f);
+    L.tn[0] = L.T[0] * ((p1.x / (p1.x + q1)) * f);
+    L.tn[1] = L.T[1] * ((p1.y / (p1.y + q1)) * f);
+    L.tn[2] = L.T[2] * ((p1.z / (p1.z + q1)) * f);
+    for (int k = 0; k < 3; ++k) {
+        L.ro[k] = L.ro[k] + L.rd[k] * L.td;
+        L.rd[k] = lrd[k];
+    }
+    L.seg = kSegShadow;
+    L.depth = 3.402823466e+38f;
+    begin_segment(L, S, cnt, state, slow);
+}
+
+// Starts path number p; returns false when p lies outside the frame (no work).
+template <bool WALK>
+__device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const DevScene &S, const DevParams &P,
+                                           const TileArgs &A, Count &cnt, uint32_t &paths, uint32_t &state,
+                                           Trav *slow) {
+    const uint64_t pl = p / A.spp;
+    const uint32_t s = (uint32_t)(p - pl * A.spp);
+    const uint32_t pix = (uint32_t)pl;
+    L.px = A.x0 + pix % A.cols;
+    L.py = A.y0 + pix / A.cols;
+    if (!camera_ray(P, L.px, L.py, L.ro, L.rd)) return false;
+    ++paths;
+    L.T[0] = L.T[1] = L.T[2] = 1.0f;
+    L.sun = make_float4(0.f, 0.f, 0.f, 0.f);
+    L.sky = L.sun;
+    L.r = 0;
+    L.seg = kSegMain;
+    L.depth = P.depth ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
+    begin_segment(L, S, cnt, state, slow);
+    // A camera ray that misses the root box draws no random number: its
+    // sample is exactly zero.  Seed the stream only for rays that enter.
+    if (L.wmode != 0u) L.g = rng_seed(A.seed, (uint64_t)L.py * P.w + L.px, A.sample_base + s);
+    return true;
+}
+
+template <int MINB, bool WALK>
+__global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
+                                                                            const void *mie_pack, float4 *sun_out,
+                                                                            float4 *sky_out, DevCounters *C,
+                                                                            WorkQueue *Q, uint32_t event_batch) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    const bool staged = stage_mie(mie_pack, P.mie_n, smem, &mbar);
+    MieSmem M{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n};
+    Count cnt;
+    cnt.zero();
+    uint32_t paths = 0;
+    uint32_t nstack[kMaxDepth];
+    Trav slow[WALK ? 1 : 1];
+    PathLane<WALK> L;
+    uint32_t state = staged ? kFetch : kDone;
+    if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const unsigned FULL = 0xffffffffu;
+    for (;;) {
+        const uint32_t want = __ballot_sync(FULL, state == kFetch);
+        if (want) {
+            const uint32_t leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&Q->next, (unsigned long long)__popc(want));
+            base = __shfl_sync(FULL, base, leader);
+            if (state == kFetch) {
+                const uint64_t p = base + __popc(want & lt_mask);
+                if (p >= A.n_paths) state = kDone;
+                else if (!start_path(L, p, S, P, A, cnt, paths, state, slow)) state = kFetch;
+            }
+        }
+        if (__all_sync(FULL, state == kDone)) break;
+        const uint32_t ev = __ballot_sync(FULL, state == kEvent);
+        const uint32_t busy = __ballot_sync(FULL, state == kTrav || state == kStep);
+        if (ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0)) {
+            if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
+            continue;
+        }
+        if (state == kTrav) {
+            const uint32_t r = trav_step(L, S, P, nstack, slow, cnt);
+            if (r == 1u) {
+                state = kStep;
+            } else if (r == 2u) {
+                L.esc = true;
+                state = kEvent;
+            }
+        }
+        if (state == kStep) {
+            const uint32_t rs = track_step(L, cnt);
+            if (rs == 1) state = kTrav;
+            else if (rs == 2) state = kEvent;
+        }
+    }
+    warp_sum_counts(cnt, C, paths);
+}
+
 // ---- parity probes ------------------------------------------------------------
 __global__ void probe_leaf_kernel(DevScene S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
                                   uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const float o[3] = {ro[3 * r], ro[3 * r + 1], ro[3 * r + 2]}, d[3] = {rd[3 * r], rd[3 * r + 1], rd[3 * r + 2]};
-    Trav T;
     Count cnt;
     cnt.zero();
     uint32_t nstack[kMaxDepth];
-    trav_init(T, S, o, d, cnt);
-    uint32_t k = 0, leaf;
-    float a, b;
-    while (k < maxn && trav_next(T, S, nstack, leaf, a, b, cnt)) {
-        nodes[(size_t)r * maxn + k] = leaf;
-        tr0[(size_t)r * maxn + k] = a;
-        tr1[(size_t)r * maxn + k] = b;
-        ++k;
+    uint32_t k = 0, leaf = 0;
+    float a = 0.0f, b = 0.0f;
+    Walk W;
+    const uint32_t mode = walk_init(W, S, o, d, cnt);
+    if (mode == 1u) {
+        for (uint32_t guard = 0; k < maxn && guard < (1u << 22); ++guard) {
+            const uint32_t st = walk_step(W, S, leaf, a, b, cnt);
+            if (st == 2u) break;
+            if (st == 1u) {
+                nodes[(size_t)r * maxn + k] = leaf;
+                tr0[(size_t)r * maxn + k] = a;
+                tr1[(size_t)r * maxn + k] = b;
+                ++k;
+            }
+        }
+    } else if (mode == 2u) {
+        Trav T;
+        trav_init(T, S, o, d, cnt);
+        while (k < maxn && trav_next(T, S, nstack, leaf, a, b, cnt)) {
+            nodes[(size_t)r * maxn + k] = leaf;
+            tr0[(size_t)r * maxn + k] = a;
+            tr1[(size_t)r * maxn + k] = b;
+            ++k;
+        }
     }
     counts[r] = k;
 }
@@ -294,6 +643,51 @@ cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const Tile
     const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
     render_tile_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out, C);
+    return cudaGetLastError();
+}
+
+// Variants of the persistent kernel compiled for 4, 5, 6 and 8 resident
+// blocks per SM (fewer registers, some spilled to L1-resident local memory).
+using PersistentFn = void (*)(DevScene, DevParams, TileArgs, const void *, float4 *, float4 *, DevCounters *,
+                              WorkQueue *, uint32_t);
+static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal) {
+    if (traversal == 1u) {
+        if (minb >= 8) return render_persistent_kernel<8, true>;
+        if (minb >= 6) return render_persistent_kernel<6, true>;
+        if (minb >= 5) return render_persistent_kernel<5, true>;
+        return render_persistent_kernel<4, true>;
+    }
+    if (minb >= 8) return render_persistent_kernel<8, false>;
+    if (minb >= 6) return render_persistent_kernel<6, false>;
+    if (minb >= 5) return render_persistent_kernel<5, false>;
+    return render_persistent_kernel<4, false>;
+}
+
+int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persistent_variant(variant, traversal), kPersistentBlock,
+                                                      smem_bytes) !=
+        cudaSuccess)
+        return 1;
+    return nb > 0 ? nb : 1;
+}
+
+cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                     float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
+                                     const Tuning &tune, int device, cudaStream_t st) {
+    if (A.n_paths == 0) return cudaSuccess;
+    int sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    const size_t smem = mie_smem(P);
+    const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
+    const int maxb = persistent_max_blocks_per_sm(variant, tune.traversal, smem);
+    const int bps = tune.blocks_per_sm && (int)tune.blocks_per_sm < maxb ? (int)tune.blocks_per_sm : maxb;
+    e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t batch = tune.event_batch ? (tune.event_batch > 32 ? 32u : tune.event_batch) : 8u;
+    persistent_variant(variant, tune.traversal)<<<sms * bps, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q,
+                                                                          batch);
     return cudaGetLastError();
 }
 

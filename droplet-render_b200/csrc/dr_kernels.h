@@ -6,9 +6,16 @@
 namespace dr {
 
 constexpr int kRenderBlock = 128;
+constexpr int kPersistentBlock = 128;
 
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
+// Persistent path kernel; Q->next must be 0 (the launcher clears it on st).
+cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                     float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
+                                     const Tuning &tune, int device, cudaStream_t st);
+// Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
+int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
                               uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts, cudaStream_t st);
 cudaError_t launch_probe_density(const DevScene &S, const uint32_t *nodes, const float *pts, uint32_t n, float *out,

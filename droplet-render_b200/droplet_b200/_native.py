@@ -103,6 +103,11 @@ class DrCounters(C.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
+class DrTuning(C.Structure):
+    _fields_ = [("kernel", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("event_batch", C.c_uint32),
+                ("traversal", C.c_uint32)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "dr_version": (C.c_int, []),
@@ -132,6 +137,8 @@ SIGNATURES = {
          C.c_void_p, C.c_void_p],
     ),
     "dr_synchronize": (C.c_int, [C.c_void_p]),
+    "dr_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
+    "dr_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
     "dr_get_counters": (C.c_int, [C.c_void_p, C.POINTER(DrCounters)]),
     "dr_reset_counters": (C.c_int, [C.c_void_p]),
     "dr_probe_leaf_sequence": (

@@ -140,6 +140,15 @@ class Renderer:
     def synchronize(self):
         N.check(N.lib().dr_synchronize(self._ctx))
 
+    def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0):
+        t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal))
+        N.check(N.lib().dr_set_tuning(self._ctx, C.byref(t)))
+
+    def get_tuning(self):
+        t = N.DrTuning()
+        N.check(N.lib().dr_get_tuning(self._ctx, C.byref(t)))
+        return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal))
+
     def counters(self) -> dict:
         c = N.DrCounters()
         N.check(N.lib().dr_get_counters(self._ctx, C.byref(c)))

@@ -147,6 +147,21 @@ int dr_render_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uin
 /* Waits for all work on the context stream. */
 int dr_synchronize(dr_ctx *ctx);
 
+/* ---- launch shape (no reference counterpart: the reference schedules 2x2
+ * pixel blocks with TBB, src/kernel.cpp:453) ------------------------------- */
+#define DR_KERNEL_PERSISTENT 0u  /* resident warps take paths from a queue (default) */
+#define DR_KERNEL_PER_PATH 1u    /* one thread per path sample */
+typedef struct {
+    uint32_t kernel;         /* DR_KERNEL_* */
+    uint32_t blocks_per_sm;  /* persistent kernel: resident blocks per SM, 0 = as many as fit */
+    uint32_t event_batch;    /* persistent kernel: waiting lanes before a warp shades (1..32, 0 = 8) */
+    uint32_t traversal;      /* persistent kernel: DR_TRAVERSAL_* */
+} dr_tuning;
+#define DR_TRAVERSAL_STACK 0u  /* octree descent with a node stack (the reference's order) */
+#define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */
+int dr_set_tuning(dr_ctx *ctx, const dr_tuning *tuning);
+int dr_get_tuning(dr_ctx *ctx, dr_tuning *tuning);
+
 /* ---- counters ------------------------------------------------------------ */
 int dr_get_counters(dr_ctx *ctx, dr_counters *out);
 int dr_reset_counters(dr_ctx *ctx);

@@ -64,6 +64,63 @@ def test_leaf_sequences_bit_exact_vs_port_random_rays(gpu_renderer, port):
         assert same_floats(a[i, :k], pa) and same_floats(b[i, :k], pb)
 
 
+def _degenerate_rays(nodes, rng, n_random=4000):
+    """Rays that hit exact plane intersections: origins on leaf-cell corners,
+    edges and the root centre, diagonal and nearly axis-aligned directions."""
+    c = nodes["ce"][0][:3].astype(np.float64)
+    e = float(nodes["ce"][0][3])
+    leaf = nodes[nodes["volx"][:, 1] != 0xFFFFFFFF]
+    cell = 2.0 * float(leaf["ce"][0][3])
+    ro, rd = [], []
+    dirs = [(1, 1, 1), (1, 1, 0.5), (1, 0.5, 0.25), (-1, 1, 1), (1, -1, 1), (1, 1, -1), (-1, -1, -1), (1, 2, 4),
+            (2, 1, 1e-7), (1e-6, 1, 1), (1, 1e-6, 1e-6), (3, 2, 1)]
+    corners = [c, c - e, c - e + cell, c + 0.5 * cell, c - 0.25 * e]
+    for o in corners:
+        for d in dirs:
+            for back in (0.0, 1.5):
+                dd = np.asarray(d, np.float64)
+                dd = dd / np.linalg.norm(dd)
+                ro.append(o - back * dd)
+                rd.append(dd)
+    # random origins snapped to the leaf-cell lattice, random directions
+    k = rng.integers(-2, int(2 * e / cell) + 3, (n_random, 3))
+    o = (c - e) + k * cell
+    d = rng.normal(size=(n_random, 3))
+    ro += list(o)
+    rd += list(d / np.linalg.norm(d, axis=1, keepdims=True))
+    return np.asarray(ro, np.float32), np.asarray(rd, np.float32)
+
+
+@pytest.mark.parametrize("scene", ["c0", "cumulus128"])
+def test_cell_walk_matches_stack_traversal_on_degenerate_rays(port, scene):
+    """The GPU cell walk reports the same leaves and (tr0, tr1) as the
+    reference's stack traversal (CPU restatement), on rays through exact
+    plane intersections, for a depth-2 and a depth-4 leaf grid."""
+    from droplet_b200 import workloads as W
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree, build_octree
+
+    if scene == "c0":
+        nodes, bricks, mlevel = golden_octree()
+        oc = Octree(nodes, bricks, mlevel)
+    else:
+        rec = W.cumulus_recipe(128)
+        org, vals = W.sparse_field(rec)
+        oc = build_octree(org, vals, rec.voxel_size, 12)
+    rng = np.random.default_rng(5)
+    ro, rd = _degenerate_rays(oc.nodes, rng)
+    with Renderer(0) as r:
+        r.upload(oc)
+        r.set_params(settings_from_cfg(c0_cfg(64, 64)))
+        nodes_g, a, b, cnt = r.probe_leaf_sequence(ro, rd, 512)
+    for i in range(len(ro)):
+        pn, pa, pb = port.leaf_sequence(oc.nodes, ro[i], rd[i], 512)
+        k = int(cnt[i])
+        assert k == len(pn), (i, ro[i], rd[i], k, len(pn))
+        assert np.array_equal(nodes_g[i, :k], pn), (i, ro[i], rd[i])
+        assert same_floats(a[i, :k], pa) and same_floats(b[i, :k], pb), (i, ro[i], rd[i])
+
+
 def test_brick_lookup_bit_exact_vs_reference_vectors(gpu_renderer):
     z = golden("ref_samplers.npz")
     got = gpu_renderer.probe_density(z["leaf"], z["pts"])
@@ -152,6 +209,35 @@ def test_tile_render_matches_port_tile(gpu_renderer, port):
     # identical paths; only the order of the per-pixel float sums differs
     for g, p in ((sun, psun), (sky, psky)):
         assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30)
+
+
+def test_every_launch_shape_renders_the_same_paths(gpu_renderer, port):
+    """Persistent kernel variants (blocks per SM, event batch, stack or cell-walk
+    traversal) and the one-thread-per-path kernel trace identical paths: tiles
+    agree with the CPU restatement up to summation order, and the path counters
+    agree exactly.  Node visits are compared for the stack traversals only: the
+    cell walk visits grid cells, not octree nodes."""
+    nodes, bricks, _ = golden_octree()
+    cfg = c0_cfg(64, 64)
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    psun, psky, pcnt = port.render_tile(S, P, 4, 6, 56, 52, 40, seed=9, sample_base=3)
+    saved = gpu_renderer.get_tuning()
+    try:
+        for cand in [(0, 4, 1, 0), (0, 5, 8, 0), (0, 6, 16, 0), (0, 8, 32, 0), (0, 0, 0, 0),
+                     (0, 4, 1, 1), (0, 5, 8, 1), (0, 6, 16, 1), (0, 8, 32, 1), (1, 0, 0, 0)]:
+            gpu_renderer.set_tuning(*cand)
+            gpu_renderer.reset_counters()
+            sun, sky = gpu_renderer.render_tile(4, 6, 56, 52, 40, seed=9, sample_base=3)
+            cnt = gpu_renderer.counters()
+            for g, p in ((sun, psun), (sky, psky)):
+                assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), cand
+            keys = ("vertices", "density_lookups", "mie_evals", "paths") + (("node_visits",) if cand[3] == 0 else ())
+            for k in keys:
+                assert cnt[k] == pcnt[k], (cand, k, cnt[k], pcnt[k])
+    finally:
+        gpu_renderer.set_tuning(*saved)
 
 
 def _rel(x, y):
