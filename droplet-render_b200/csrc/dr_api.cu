@@ -26,6 +26,49 @@ int build_octree(const int32_t *org, const float *vals, uint32_t n_blocks, float
 int sky_cook(const double *const rgb[3], const double *const rad[3], double turbidity, double albedo,
              double elevation, double configs[3][9], double radiances[3]);
 
+// Exact-mode phase sampler table (DR_PHASE_MIE_EXACT).  Target density over
+// phi = acos(-ct): f(phi) sin(phi), f the red pdf column interpolated linearly
+// in phi as MiePhase::Evaluate does (src/KernelSampler.cpp:214-231; knots at
+// k pi / n, the last bin extrapolating the last two entries, clamped at 0).
+// Per bin k, in FP64: f0 = f(phi_k), beta = slope, mass
+//   M_k = S[(f0 + beta d) sin d - beta (1 - cos d)] + C[f0 (1 - cos d) + beta (sin d - d cos d)]
+// (the integral of f sin over the bin, d = pi/n, S, C = sin, cos phi_k).
+// Layout (float): per bin (cdf_k, f0, beta, M_k), (S, C, d, 0); then (1, 0, 0, 0).
+static void mie_exact_table(const float *pdf_rgb, uint32_t n, float *out) {
+    const double d = 3.14159265358979323846 / (double)n;
+    std::vector<double> mass(n);
+    double total = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        double fa = k + 1 < n ? (double)pdf_rgb[3 * k] : (double)pdf_rgb[3 * (n - 1)];
+        double fb = k + 1 < n ? (double)pdf_rgb[3 * (k + 1)]
+                              : 2.0 * (double)pdf_rgb[3 * (n - 1)] - (double)pdf_rgb[3 * (n - 2)];
+        fa = fa < 0.0 ? 0.0 : fa;
+        fb = fb < 0.0 ? 0.0 : fb;
+        const double beta = (fb - fa) / d, phi = d * (double)k;
+        const double S = std::sin(phi), C = std::cos(phi);
+        const double m = S * ((fa + beta * d) * std::sin(d) - beta * (1.0 - std::cos(d))) +
+                         C * (fa * (1.0 - std::cos(d)) + beta * (std::sin(d) - d * std::cos(d)));
+        mass[k] = m > 0.0 ? m : 0.0;
+        float *o = out + 8 * (size_t)k;
+        o[1] = (float)fa;
+        o[2] = (float)beta;
+        o[3] = (float)mass[k];
+        o[4] = (float)S;
+        o[5] = (float)C;
+        o[6] = (float)d;
+        o[7] = 0.0f;
+        total += mass[k];
+    }
+    double acc = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        out[8 * (size_t)k] = (float)(acc / total);
+        acc += mass[k];
+    }
+    float *e = out + 8 * (size_t)n;
+    e[0] = 1.0f;
+    e[1] = e[2] = e[3] = 0.0f;
+}
+
 static int cuda_fail(cudaError_t e, const char *what) {
     g_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
     return e == cudaErrorMemoryAllocation ? DR_ERR_NOMEM : DR_ERR_CUDA;
@@ -322,8 +365,13 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     if (!c || !p) return need(false, DR_ERR_INVALID, "dr_set_params: null argument");
     if (!p->mie_pdf || !p->mie_cdf || p->mie_n < 4 || p->mie_n > kMieMax || (p->mie_n % 4))
         return need(false, DR_ERR_INVALID, "dr_set_params: phase tables need 4 <= mie_n <= 4096, mie_n % 4 == 0");
-    if (p->phase_mode != DR_PHASE_MIE_REFERENCE)
+    if (p->phase_mode != DR_PHASE_MIE_REFERENCE && p->phase_mode != DR_PHASE_MIE_EXACT)
         return need(false, DR_ERR_INVALID, "dr_set_params: unknown phase mode");
+    if (p->phase_mode == DR_PHASE_MIE_EXACT && p->mie_n > 512)
+        return need(false, DR_ERR_INVALID, "dr_set_params: the exact phase sampler takes mie_n <= 512");
+    for (uint32_t i = 0; i < p->mie_n; ++i)
+        if (!(p->mie_pdf[3 * i] >= 0.0f) || !std::isfinite(p->mie_pdf[3 * i]))
+            return need(false, DR_ERR_INVALID, "dr_set_params: phase pdf must be finite and >= 0");
     if (p->w == 0 || p->h == 0) return need(false, DR_ERR_INVALID, "dr_set_params: empty image");
     if (p->scattevs > 100000u) return need(false, DR_ERR_INVALID, "dr_set_params: scattevs above 100000");
     if (!(p->sigma_s >= 0.0f) || !(p->sigma_a >= 0.0f) || !(p->sigma_s + p->sigma_a > 0.0f))
@@ -351,11 +399,23 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     std::memcpy(d.proji, p->proji, sizeof(d.proji));
     d.w = p->w;
     d.h = p->h;
-    std::vector<unsigned char> pack((size_t)p->mie_n * 20);
+    d.depthcomp = (p->flags & DR_KERNEL_DEPTHCOMP) ? 1u : 0u;
+    {
+        // RenderKernel::Shadow: zfar = (0,0,1,1) * projInv, clip_end = -zfar.z / zfar.w
+        const float zz = p->proji[8 + 2] + p->proji[12 + 2], zw = p->proji[8 + 3] + p->proji[12 + 3];
+        d.clip_end = -zz / zw;
+    }
+    const size_t n_ex = p->phase_mode == DR_PHASE_MIE_EXACT ? 8 * (size_t)p->mie_n + 4 : 0;
+    std::vector<unsigned char> pack((size_t)p->mie_n * 20 + 4 * n_ex);
     for (uint32_t i = 0; i < p->mie_n; ++i) {
         float4 v = make_float4(p->mie_pdf[3 * i], p->mie_pdf[3 * i + 1], p->mie_pdf[3 * i + 2], 0.0f);
         std::memcpy(&pack[16 * (size_t)i], &v, 16);
         std::memcpy(&pack[16 * (size_t)p->mie_n + 4 * (size_t)i], &p->mie_cdf[3 * i], 4);
+    }
+    if (n_ex) {
+        std::vector<float> ex(n_ex);
+        mie_exact_table(p->mie_pdf, p->mie_n, ex.data());
+        std::memcpy(&pack[20 * (size_t)p->mie_n], ex.data(), 4 * n_ex);
     }
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
@@ -416,6 +476,34 @@ int dr_render_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint3
                                          c->counters.p, c->work.p, c->tuning, c->device, st),
                 "render: launch");
     }
+    return DR_OK;
+}
+
+int dr_shadow_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
+                         uint64_t sample_base, float *out_dev, void *stream) {
+    if (!c || !out_dev) return need(false, DR_ERR_INVALID, "dr_shadow_tile_async: null argument");
+    TileArgs A;
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, A);
+    if (rc != DR_OK) return rc;
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    DR_CUDA(cudaMemsetAsync(out_dev, 0, (size_t)tw * th * sizeof(float4), st), "shadow: clear");
+    DR_CUDA(launch_shadow_tile(c->scene, c->params, A, (float4 *)out_dev, c->counters.p, st), "shadow: launch");
+    return DR_OK;
+}
+
+int dr_shadow_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
+                   uint64_t sample_base, float *out) {
+    if (!c || !out) return need(false, DR_ERR_INVALID, "dr_shadow_tile: null argument");
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const size_t n = (size_t)tw * th;
+    DR_CUDA(c->tile_sun.reserve(n), "shadow: alloc tile");
+    int rc = dr_shadow_tile_async(c, x0, y0, tw, th, spp, seed, sample_base, (float *)c->tile_sun.p, nullptr);
+    if (rc != DR_OK) return rc;
+    DR_CUDA(cudaMemcpyAsync(out, c->tile_sun.p, n * sizeof(float4), cudaMemcpyDeviceToHost, c->stream),
+            "shadow: copy out");
+    DR_CUDA(cudaStreamSynchronize(c->stream), "shadow: sync");
     return DR_OK;
 }
 
@@ -577,14 +665,16 @@ int dr_probe_paths(dr_ctx *c, const uint32_t *px, const uint32_t *py, const uint
 }
 
 int dr_probe_sampler(dr_ctx *c, uint32_t what, const float *in, uint32_t n, float *out) {
-    if (!c || !in || !out || n == 0 || what > DR_PROBE_MIE_THETA)
+    if (!c || !in || !out || n == 0 || what > DR_PROBE_MIE_EXACT_DIR)
         return need(false, DR_ERR_INVALID, "dr_probe_sampler: bad argument");
     if (!c->has_params) return need(false, DR_ERR_STATE, "dr_probe_sampler: no parameters");
+    if (what == DR_PROBE_MIE_EXACT_DIR && c->params.phase_mode != DR_PHASE_MIE_EXACT)
+        return need(false, DR_ERR_STATE, "dr_probe_sampler: the exact sampler needs DR_PHASE_MIE_EXACT");
     const size_t in_n = what == DR_PROBE_MIE_SAMPLE ? 5ull * n
                         : what == DR_PROBE_SUN_SAMPLE ? 2ull * n
                         : what == DR_PROBE_SKY ? 3ull * n
                         : (size_t)n;
-    const size_t out_n = what == DR_PROBE_MIE_THETA ? (size_t)n : 3ull * n;
+    const size_t out_n = what == DR_PROBE_MIE_THETA ? (size_t)n : what == DR_PROBE_MIE_EXACT_DIR ? 2ull * n : 3ull * n;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     Scratch S;

@@ -529,6 +529,7 @@ struct MieSmem {
     float4 *pdf;
     float *cdf;
     uint32_t n;
+    const float4 *ex;  // exact-mode sampler table (2n + 1 float4) or null
 };
 
 __device__ __forceinline__ float3 mie_eval_rgb(const MieSmem &M, float ct) {
@@ -581,7 +582,64 @@ __device__ __forceinline__ void compose_dir(const float iv[3], float st, float c
     for (int k = 0; k < 3; ++k) out[k] = ((b1[k] * st) * cph + (b2[k] * st) * sph) + iv[k] * ct;
 }
 
+// ---- exact-mode sampler (DR_PHASE_MIE_EXACT) ------------------------------------
+// Inverts the CDF of f(phi) sin(phi), phi = acos(-ct), f the red table column
+// interpolated linearly in phi as MiePhase::Evaluate does (knots k pi / n, the
+// last bin extrapolated).  Bin k: f = f0 + beta x on x = phi - phi_k in [0, pi/n],
+// mass H_k(x) = S[(f0 + beta x) sin x - beta (1 - cos x)] + C[f0 (1 - cos x) +
+// beta (sin x - x cos x)] with S, C = sin, cos(phi_k) (the integral of f sin).
+// Table per bin: (cdf_k, f0, beta, M_k), (S, C, pi/n, 0); then (1, 0, 0, 0).
+// The bin comes from bisection on cdf_k, x from 8 safeguarded Newton steps.
+
+// sin x, 1 - cos x and sin x - x cos x from their Taylor series (x <= pi/4)
+__device__ __forceinline__ void local_trig(float x, float &sx, float &omc, float &sxc) {
+    const float x2 = x * x;
+    sx = x * (1.0f - (x2 / 6.0f) * (1.0f - (x2 / 20.0f) * (1.0f - (x2 / 42.0f) * (1.0f - x2 / 72.0f))));
+    omc = (x2 / 2.0f) * (1.0f - (x2 / 12.0f) * (1.0f - (x2 / 30.0f) * (1.0f - (x2 / 56.0f) * (1.0f - x2 / 90.0f))));
+    sxc = ((x2 * x) / 3.0f) * (1.0f - (x2 / 10.0f) * (1.0f - (x2 / 28.0f) * (1.0f - x2 / 54.0f)));
+}
+
+__device__ __forceinline__ void mie_exact_dir(const float4 *ex, uint32_t n, float u1, float &ct, float &st) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (ex[2 * mid].x <= u1) lo = mid;
+        else hi = mid - 1;
+    }
+    const float4 a = ex[2 * lo], b = ex[2 * lo + 1];
+    const float c0 = a.x, c1 = ex[2 * (lo + 1)].x;
+    const float f0 = a.y, beta = a.z, mk = a.w, S = b.x, C = b.y, dx = b.z;
+    const float d = c1 - c0;
+    const float up = d > 0.0f ? (u1 - c0) / d : 0.5f;
+    const float m = up * mk;
+    float xl = 0.0f, xh = dx, x = up * dx;
+#pragma unroll 1
+    for (int it = 0; it < 8; ++it) {
+        float sx, omc, sxc;
+        local_trig(x, sx, omc, sxc);
+        const float fx = f0 + beta * x;
+        const float h = (S * (fx * sx - beta * omc) + C * (f0 * omc + beta * sxc)) - m;
+        const float hp = fx * (S * (1.0f - omc) + C * sx);
+        if (h > 0.0f) xh = x;
+        else xl = x;
+        float xn = hp > 0.0f ? x - h / hp : 0.5f * (xl + xh);
+        if (!(xn > xl && xn < xh)) xn = 0.5f * (xl + xh);
+        x = xn;
+    }
+    float sx, omc, sxc;
+    local_trig(x, sx, omc, sxc);
+    const float cx = 1.0f - omc;
+    ct = 0.0f - (C * cx - S * sx);
+    st = sse_max(S * cx + C * sx, 0.0f);
+}
+
 __device__ __forceinline__ void mie_sample(const MieSmem &M, const float iv[3], float u1, float u2, float out[3]) {
+    if (M.ex) {
+        float ct, st;
+        mie_exact_dir(M.ex, M.n, u1, ct, st);
+        compose_dir(iv, st, ct, (2.0f * kPi) * u2, out);
+        return;
+    }
     const float th = mie_theta_ref(M, u1) * kPi;
     const float ph = (2.0f * kPi) * u2;
     float s_, c_;
@@ -659,10 +717,16 @@ __device__ __forceinline__ bool camera_ray(const DevParams &P, uint32_t px, uint
 }
 
 // ---- free-flight tracking of one segment (src/kernel.cpp:197-317) ----------
-// Returns true when the segment leaves the volume without a real collision;
-// td receives the distance of the collision (or of the last leaf exit).
-__device__ __forceinline__ bool track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
-                                      Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
+// Returns kTrackEscaped when the segment leaves the volume (or passes `depth` at
+// a leaf boundary) without a real collision, kTrackCollided for a real
+// collision before `depth`, and kTrackCut for a collision at or beyond `depth`:
+// the reference re-evaluates its mask mm = td < depth on the next leaf step and
+// sets rm |= !mm after taking alpha from rm (src/kernel.cpp:214-217, 370-384),
+// so such a collision counts for coverage but does not scatter.  td receives
+// the distance of the collision (or of the last leaf exit).
+enum : uint32_t { kTrackCollided = 0, kTrackEscaped = 1, kTrackCut = 2 };
+__device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
+                                          Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
     Trav T;
     trav_init(T, S, ro, rd, cnt);
     ++cnt.vertices;
@@ -710,18 +774,18 @@ __device__ __forceinline__ bool track(const DevScene &S, const DevParams &P, con
             rm = rm && (rho / smax < q);
             if (!rm) {
                 td_out = td;
-                return false;
+                return td < depth ? kTrackCollided : kTrackCut;
             }
             if (--budget == 0) {
                 ++cnt.gave_up;
                 td_out = td;
-                return true;
+                return kTrackEscaped;
             }
             sr = sr - dlog(g.uniform()) / denom;
         }
     }
     td_out = td;
-    return true;
+    return kTrackEscaped;
 }
 
 // ---- one camera path sample: SampleVolume recursion as a loop --------------
@@ -736,12 +800,13 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
     Rng g = rng_seed(seed, (uint64_t)py * P.w + px, sample);
     const float f = P.albedo;
     float T0 = 1.0f, T1 = 1.0f, T2 = 1.0f;
-    const float depth0 = P.depth ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
+    const float depth0 = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
     for (uint32_t r = 0;; ++r) {
         float td;
-        const bool esc = track(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
-        if (r == 0) sun_acc.w = sky_acc.w = esc ? 0.0f : 1.0f;
-        if (esc) {
+        const uint32_t res = track(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+        if (r == 0) sun_acc.w = sky_acc.w = res == kTrackEscaped ? 0.0f : 1.0f;
+        if (res == kTrackCut) break;
+        if (res == kTrackEscaped) {
             if (r > 0) {
                 if (sun_hit(P, rd)) {
                     sun_acc.x = sun_acc.x + T0 * P.sun_color[0];
@@ -773,7 +838,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         float tds;
-        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt)) {
+        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped) {
             const bool hit = sun_hit(P, lrd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;
@@ -790,6 +855,38 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
             rd[k] = srd[k];
         }
     }
+}
+
+// ---- one shadow-pass sample: RenderKernel::Shadow (src/kernel.cpp:569-607) ----
+// The camera ray is cut at the pixel's depth when that lies before the far clip
+// plane; from there one shadow segment (SampleVolume with r = scattevs) runs
+// along a sun-cone sample.  A pixel without geometry before the far plane traces
+// nothing and keeps "not scattering".  The result is divided by
+// float4::load(&colour), whose w is 0: rgb = sun(lrd) / colour, alpha = 1/0 per
+// sample (0/0 only when scattevs == 0 and the segment escaped).
+__device__ __forceinline__ float4 shadow_sample(const DevScene &S, const DevParams &P, uint32_t px, uint32_t py,
+                                                uint64_t seed, uint64_t sample, const float ro[3], const float rd[3],
+                                                uint32_t *nstack, Count &cnt) {
+    const float depth = P.depth ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
+    const bool active = depth < P.clip_end;
+    Rng g = rng_seed(seed, (uint64_t)py * P.w + px, sample);
+    const float u3 = g.uniform(), u4 = g.uniform();
+    float lrd[3];
+    sun_sample(P, u3, u4, lrd);
+    uint32_t res = kTrackEscaped;
+    if (active) {
+        const float ro1[3] = {ro[0] + rd[0] * depth, ro[1] + rd[1] * depth, ro[2] + rd[2] * depth};
+        float td;
+        res = track(S, P, ro1, lrd, g, 3.402823466e+38f, td, nstack, cnt);
+    }
+    const bool esc = res == kTrackEscaped;
+    const bool lit = P.scattevs > 0u && esc && sun_hit(P, lrd);
+    float4 o;
+    o.x = __fdiv_rn(lit ? P.sun_color[0] : 0.0f, P.sun_color[0]);
+    o.y = __fdiv_rn(lit ? P.sun_color[1] : 0.0f, P.sun_color[1]);
+    o.z = __fdiv_rn(lit ? P.sun_color[2] : 0.0f, P.sun_color[2]);
+    o.w = __fdiv_rn((P.scattevs > 0u || !esc) ? 1.0f : 0.0f, 0.0f);
+    return o;
 }
 
 }  // namespace dr

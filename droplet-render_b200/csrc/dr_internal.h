@@ -56,6 +56,8 @@ struct DevParams {
     float viewi[16], proji[16];
     uint32_t w, h;
     const float *depth;       // w*h or null
+    uint32_t depthcomp;       // KERNEL_DEPTHCOMP: camera rays stop at depth
+    float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
 };
 
 struct TileArgs {

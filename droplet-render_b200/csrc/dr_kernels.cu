@@ -12,8 +12,17 @@ namespace dr {
 // red CDF x n (n % 4 == 0, so the block is a multiple of 16 bytes).  One thread
 // issues a bulk copy (cp.async.bulk, completion counted on an mbarrier); the
 // wait is bounded and reports a give-up instead of spinning forever.
-__device__ __forceinline__ bool stage_mie(const void *src, uint32_t n, unsigned char *smem, uint64_t *mbar) {
-    const uint32_t bytes = n * 20u;
+// Exact mode appends its sampler table: (2n + 1) float4 after the CDF.
+__device__ __forceinline__ uint32_t mie_bytes(const DevParams &P) {
+    return P.mie_n * 20u + (P.phase_mode == 1u ? (2u * P.mie_n + 1u) * 16u : 0u);
+}
+
+__device__ __forceinline__ MieSmem mie_view(const DevParams &P, unsigned char *smem) {
+    return MieSmem{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n,
+                   P.phase_mode == 1u ? reinterpret_cast<const float4 *>(smem + 20u * P.mie_n) : nullptr};
+}
+
+__device__ __forceinline__ bool stage_mie(const void *src, uint32_t bytes, unsigned char *smem, uint64_t *mbar) {
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
     const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
     if (threadIdx.x == 0) {
@@ -79,8 +88,8 @@ __global__ void __launch_bounds__(kRenderBlock) render_tile_kernel(DevScene S, D
                                                                    float4 *sky_out, DevCounters *C) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    const bool staged = stage_mie(mie_pack, P.mie_n, smem, &mbar);
-    MieSmem M{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n};
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
     Count cnt;
     cnt.zero();
     uint32_t nstack[kMaxDepth];
@@ -122,6 +131,46 @@ __global__ void __launch_bounds__(kRenderBlock) render_tile_kernel(DevScene S, D
     warp_sum_counts(cnt, C, paths);
 }
 
+// Shadow pass (RenderKernel::Shadow, src/kernel.cpp:569-607): one thread per
+// (pixel, sample), same pixel/sample layout and warp reduction as the render
+// kernel; the result goes to one tile (the reference writes phb[0] only).
+__global__ void __launch_bounds__(kRenderBlock) shadow_tile_kernel(DevScene S, DevParams P, TileArgs A, float4 *out,
+                                                                   DevCounters *C) {
+    Count cnt;
+    cnt.zero();
+    uint32_t nstack[kMaxDepth];
+    const uint64_t g = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
+    const bool valid = g < A.n_paths;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t pix = 0xffffffffu, paths = 0;
+    if (valid) {
+        const uint64_t pl = g / A.spp;
+        const uint32_t s = (uint32_t)(g - pl * A.spp);
+        pix = (uint32_t)pl;
+        const uint32_t i = pix % A.cols, j = pix / A.cols;
+        float ro[3], rd[3];
+        if (camera_ray(P, A.x0 + i, A.y0 + j, ro, rd)) {
+            paths = 1;
+            acc = shadow_sample(S, P, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, ro, rd, nstack, cnt);
+        } else {
+            pix = 0xfffffffeu;  // outside the frame: nothing is written, as in the reference
+        }
+    }
+    const uint32_t grp = __match_any_sync(0xffffffffu, pix);
+    if (grp == 0xffffffffu) {
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) acc = add4(acc, shfl_xor4(acc, m));
+        if ((threadIdx.x & 31) == 0 && pix < 0xfffffffeu) {
+            const uint32_t i = pix % A.cols, j = pix / A.cols;
+            atomicAdd(&out[(size_t)j * A.tw + i], acc);
+        }
+    } else if (pix < 0xfffffffeu) {
+        const uint32_t i = pix % A.cols, j = pix / A.cols;
+        atomicAdd(&out[(size_t)j * A.tw + i], acc);
+    }
+    warp_sum_counts(cnt, C, paths);
+}
+
 // ---- persistent path kernel ------------------------------------------------------
 // Each lane of a resident warp holds one path sample as a small state machine
 // and takes the next path from a global counter as soon as its path ends, so
@@ -157,7 +206,7 @@ struct PathLane {
     uint32_t wmode;  // 0 no leaf on the ray, 1 cell walk, 2 stack traversal in local memory, 3 stack traversal
     float td, depth;
     uint32_t budget;
-    bool esc;
+    uint32_t esc;  // segment result: kTrackCollided, kTrackEscaped or kTrackCut
     // leaf
     float lo, tr0, tr1, trb, s0, sr, smax, denom;
     float4 ce;
@@ -285,12 +334,12 @@ __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
     const float q = L.g.uniform();
     rm = rm && (rho / L.smax < q);
     if (!rm) {
-        L.esc = false;
+        L.esc = L.td < L.depth ? kTrackCollided : kTrackCut;
         return 2;
     }
     if (--L.budget == 0) {
         ++cnt.gave_up;
-        L.esc = true;
+        L.esc = kTrackEscaped;
         return 2;
     }
     L.sr = L.sr - dlog(L.g.uniform()) / L.denom;
@@ -304,7 +353,7 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
                                         uint32_t &state, Trav *slow) {
     const float f = P.albedo;
     if (L.seg == kSegShadow) {
-        if (L.esc) {
+        if (L.esc == kTrackEscaped) {
             const bool hit = sun_hit(P, L.rd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;
@@ -322,8 +371,8 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
         begin_segment(L, S, cnt, state, slow);
         return;
     }
-    if (L.r == 0) L.sun.w = L.sky.w = L.esc ? 0.0f : 1.0f;
-    if (L.esc) {
+    if (L.r == 0) L.sun.w = L.sky.w = L.esc == kTrackEscaped ? 0.0f : 1.0f;
+    if (L.esc == kTrackEscaped) {
         if (L.r > 0) {
             if (sun_hit(P, L.rd)) {
                 L.sun.x = L.sun.x + L.T[0] * P.sun_color[0];
@@ -343,7 +392,7 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
         state = kFetch;
         return;
     }
-    if (L.r >= P.scattevs) {
+    if (L.esc == kTrackCut || L.r >= P.scattevs) {
         finish_path(L, A, sun_out, sky_out);
         state = kFetch;
         return;
@@ -390,7 +439,7 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     L.sky = L.sun;
     L.r = 0;
     L.seg = kSegMain;
-    L.depth = P.depth ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
+    L.depth = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
     begin_segment(L, S, cnt, state, slow);
     // A camera ray that misses the root box draws no random number: its
     // sample is exactly zero.  Seed the stream only for rays that enter.
@@ -405,8 +454,8 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
                                                                             WorkQueue *Q, uint32_t event_batch) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    const bool staged = stage_mie(mie_pack, P.mie_n, smem, &mbar);
-    MieSmem M{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n};
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
     Count cnt;
     cnt.zero();
     uint32_t paths = 0;
@@ -443,7 +492,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
             if (r == 1u) {
                 state = kStep;
             } else if (r == 2u) {
-                L.esc = true;
+                L.esc = kTrackEscaped;
                 state = kEvent;
             }
         }
@@ -508,8 +557,8 @@ __global__ void probe_paths_kernel(DevScene S, DevParams P, const void *mie_pack
                                    float4 *out_sun, float4 *out_sky, DevCounters *C) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    const bool staged = stage_mie(mie_pack, P.mie_n, smem, &mbar);
-    MieSmem M{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n};
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt;
     cnt.zero();
@@ -529,8 +578,8 @@ __global__ void probe_sampler_kernel(DevParams P, const void *mie_pack, uint32_t
                                      float *out) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    const bool staged = stage_mie(mie_pack, P.mie_n, smem, &mbar);
-    MieSmem M{reinterpret_cast<float4 *>(smem), reinterpret_cast<float *>(smem + 16u * P.mie_n), P.mie_n};
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (!staged || i >= n) return;
     if (what == 0u) {
@@ -559,6 +608,11 @@ __global__ void probe_sampler_kernel(DevParams P, const void *mie_pack, uint32_t
         out[3 * i + 2] = s.z;
     } else if (what == 4u) {
         out[i] = mie_theta_ref(M, in[i]);
+    } else if (what == 5u && M.ex) {
+        float ct, st;
+        mie_exact_dir(M.ex, M.n, in[i], ct, st);
+        out[2 * i] = ct;
+        out[2 * i + 1] = st;
     }
 }
 
@@ -579,7 +633,7 @@ __global__ void probe_transmittance_kernel(DevScene S, DevParams P, const float 
     for (uint64_t s = c * 64; s < s1; ++s) {
         Rng g = rng_seed(seed, r, s);
         float td;
-        esc += track(S, P, o, d, g, 3.402823466e+38f, td, nstack, cnt) ? 1u : 0u;
+        esc += track(S, P, o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped ? 1u : 0u;
     }
     atomicAdd(&escapes[r], (unsigned long long)esc);
 }
@@ -635,7 +689,9 @@ cudaError_t launch_transmittance_noalloc(const DevScene &S, const DevParams &P, 
 }
 
 // ---- launchers ------------------------------------------------------------------
-static size_t mie_smem(const DevParams &P) { return (size_t)P.mie_n * 20u; }
+static size_t mie_smem(const DevParams &P) {
+    return (size_t)P.mie_n * 20u + (P.phase_mode == 1u ? (2u * (size_t)P.mie_n + 1u) * 16u : 0u);
+}
 
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st) {
@@ -643,6 +699,15 @@ cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const Tile
     const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
     render_tile_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out, C);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const TileArgs &A, float4 *out, DevCounters *C,
+                               cudaStream_t st) {
+    if (A.n_paths == 0) return cudaSuccess;
+    const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
+    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    shadow_tile_kernel<<<(unsigned)blocks, kRenderBlock, 0, st>>>(S, P, A, out, C);
     return cudaGetLastError();
 }
 

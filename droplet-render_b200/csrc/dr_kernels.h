@@ -10,6 +10,8 @@ constexpr int kPersistentBlock = 128;
 
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
+cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const TileArgs &A, float4 *out, DevCounters *C,
+                               cudaStream_t st);
 // Persistent path kernel; Q->next must be 0 (the launcher clears it on st).
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,

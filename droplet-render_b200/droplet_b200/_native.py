@@ -24,12 +24,14 @@ DR_NONE = 0xFFFFFFFF
 
 DR_PHASE_MIE_REFERENCE = 0
 DR_PHASE_MIE_EXACT = 1
+DR_KERNEL_DEPTHCOMP = 0x1
 
 DR_PROBE_MIE_EVAL_RGB = 0
 DR_PROBE_MIE_SAMPLE = 1
 DR_PROBE_SUN_SAMPLE = 2
 DR_PROBE_SKY = 3
 DR_PROBE_MIE_THETA = 4
+DR_PROBE_MIE_EXACT_DIR = 5
 
 
 class DrError(RuntimeError):
@@ -86,6 +88,7 @@ class DrRenderParams(C.Structure):
         ("w", C.c_uint32),
         ("h", C.c_uint32),
         ("depth", C.c_void_p),
+        ("flags", C.c_uint32),
     ]
 
 
@@ -135,6 +138,15 @@ SIGNATURES = {
         C.c_int,
         [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
          C.c_void_p, C.c_void_p],
+    ),
+    "dr_shadow_tile": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p],
+    ),
+    "dr_shadow_tile_async": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
+         C.c_void_p],
     ),
     "dr_synchronize": (C.c_int, [C.c_void_p]),
     "dr_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),

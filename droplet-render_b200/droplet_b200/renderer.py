@@ -48,7 +48,8 @@ class RenderSettings:
     proji: np.ndarray
     w: int
     h: int
-    depth: np.ndarray | None = None
+    depth: np.ndarray | None = None   # depth texture: distance along each camera ray (shadow pass, compositing)
+    depthcomp: bool = False           # KERNEL_DEPTHCOMP: camera rays stop at the depth texture
     phase_mode: int = N.DR_PHASE_MIE_REFERENCE
     _keep: list = field(default_factory=list, repr=False)
 
@@ -77,6 +78,7 @@ class RenderSettings:
             p.depth = d.ctypes.data
         else:
             p.depth = None
+        p.flags = N.DR_KERNEL_DEPTHCOMP if self.depthcomp else 0
         return p
 
 
@@ -130,6 +132,22 @@ class Renderer:
         if sample_base is None:
             self.sample_base += spp
         return sun, sky
+
+    def render_shadow_tile(self, x0: int, y0: int, tw: int, th: int, spp: int, seed: int = 0,
+                           sample_base: int | None = None):
+        """Shadow pass (RenderKernel::Shadow): per pixel the sum over `spp` sun-cone
+        samples of the shadow-segment result, shape (th, tw, 4); alpha is +inf as in
+        the reference.  Returns (shadow, zeros): the reference writes phb[0] only."""
+        base = self.sample_base if sample_base is None else int(sample_base)
+        out = np.zeros((th, tw, 4), np.float32)
+        N.check(N.lib().dr_shadow_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, out.ctypes.data))
+        if sample_base is None:
+            self.sample_base += spp
+        return out, np.zeros_like(out)
+
+    def shadow_tile_async(self, x0, y0, tw, th, spp, seed, sample_base, out_dev_ptr: int, stream_ptr: int = 0):
+        N.check(N.lib().dr_shadow_tile_async(self._ctx, x0, y0, tw, th, spp, int(seed), int(sample_base),
+                                             C.c_void_p(out_dev_ptr), C.c_void_p(stream_ptr) if stream_ptr else None))
 
     def render_tile_async(self, x0, y0, tw, th, spp, seed, sample_base, sun_dev_ptr: int, sky_dev_ptr: int,
                           stream_ptr: int = 0):
@@ -191,9 +209,10 @@ class Renderer:
 
     def probe_sampler(self, what: int, inputs: np.ndarray, n: int):
         x = np.ascontiguousarray(inputs, np.float32).reshape(-1)
-        out = np.zeros(n if what == N.DR_PROBE_MIE_THETA else 3 * n, np.float32)
+        width = {N.DR_PROBE_MIE_THETA: 1, N.DR_PROBE_MIE_EXACT_DIR: 2}.get(what, 3)
+        out = np.zeros(width * n, np.float32)
         N.check(N.lib().dr_probe_sampler(self._ctx, int(what), x.ctypes.data, int(n), out.ctypes.data))
-        return out if what == N.DR_PROBE_MIE_THETA else out.reshape(n, 3)
+        return out if width == 1 else out.reshape(n, width)
 
     def probe_transmittance(self, ro, rd, nsamp: int, seed: int = 0):
         ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)

@@ -144,13 +144,16 @@ def _parse(scene, data, tilex, tiley, w, h):
     vol = getattr(scene, "droplet_volume", None)
     if vol is None:
         _fail("scene.droplet_volume is missing (the node-tree/OpenVDB volume build is outside this library)")
+    # depth texture (src/main.cpp:596-614): read whenever one is supplied; camera
+    # rays stop at it only with depthcomp (KERNEL_DEPTHCOMP, src/main.cpp:635)
     depth = None
-    if bool(getattr(world, "depthcomp", False)) and getattr(scene, "droplet_depth", None) is not None:
+    if getattr(scene, "droplet_depth", None) is not None:
         depth = np.ascontiguousarray(scene.droplet_depth, np.float32).reshape(h, w)
+    depthcomp = bool(getattr(world, "depthcomp", False))
     return {
         "viewi": viewi, "proji": proji, "w": int(w), "h": int(h), "tilex": int(tilex), "tiley": int(tiley),
         "sun": suns[0], "scattevs": int(sam.scatterevs), "sigma_s": float(sam.msigmas), "sigma_a": float(sam.msigmaa),
-        "maxdepth": int(grid.maxdepth), "volume": vol, "depth": depth,
+        "maxdepth": int(grid.maxdepth), "volume": vol, "depth": depth, "depthcomp": depthcomp,
         "turbidity": float(getattr(world, "turbidity", 7.0)), "ground_albedo": float(getattr(world, "ground_albedo", 0.15)),
     }
 
@@ -196,7 +199,7 @@ def _build(job):
         st = RenderSettings(sigma_s=job["sigma_s"], sigma_a=job["sigma_a"], scattevs=job["scattevs"], sun_dir=sd,
                             sun_color=sc, sun_angle=sa, sky=_sky(sd, job["turbidity"], job["ground_albedo"]),
                             phase=PhaseTable(pdf, cdf), viewi=job["viewi"], proji=job["proji"], w=job["w"],
-                            h=job["h"], depth=job["depth"])
+                            h=job["h"], depth=job["depth"], depthcomp=job["depthcomp"])
         r = Renderer(_device)
         r.upload(oc)
         r.set_params(st)

@@ -63,7 +63,7 @@ typedef struct {
 } dr_scene_desc;
 
 #define DR_PHASE_MIE_REFERENCE 0u  /* the reference's tabulated sampler (src/KernelSampler.cpp:257-285) */
-#define DR_PHASE_MIE_EXACT 1u      /* exact inverse CDF of the tabulated phase x sin(theta) */
+#define DR_PHASE_MIE_EXACT 1u      /* exact inverse CDF of the tabulated phase x sin(theta); mie_n <= 512 */
 
 /* Everything RenderKernel::Initialize receives (src/kernel.cpp:497-534) plus
  * the sun light (src/main.cpp:374-404) and the sky state the reference
@@ -83,8 +83,10 @@ typedef struct {
     float viewi[16];               /* inverse view matrix, rows r[0..3] */
     float proji[16];               /* inverse projection matrix, rows r[0..3] */
     uint32_t w, h;                 /* full image size */
-    const float *depth;            /* optional w*h compositing depth (KERNEL_DEPTHCOMP), or NULL */
+    const float *depth;            /* optional w*h depth texture (distance along the camera ray), or NULL */
+    uint32_t flags;                /* DR_KERNEL_DEPTHCOMP: camera rays stop at depth (src/kernel.h:4) */
 } dr_render_params;
+#define DR_KERNEL_DEPTHCOMP 0x1u
 
 /* In-kernel counters accumulated over all launches since the last reset. */
 typedef struct {
@@ -144,6 +146,19 @@ int dr_render_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t 
  * without waiting. */
 int dr_render_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
                          uint64_t seed, uint64_t sample_base, float *sun_out_dev, float *sky_out_dev, void *stream);
+/* ---- shadow pass: RenderKernel::Shadow (src/kernel.cpp:569-607) ----------
+ * For each pixel of the tile whose depth-texture value lies before the far clip
+ * plane, spp shadow segments run from that point towards sun-cone samples; out
+ * (phb[0], tw*th float4) receives per pixel the SUM over samples of
+ * sun(lrd)/colour for segments that escape (pixels without such geometry count
+ * every sample as lit).  Alpha is +inf, as in the reference (its division by
+ * float4::load(&colour) has w = 0).  Sample s of pixel p draws from stream
+ * (seed, p, sample_base + s).  Blocking; host buffer. */
+int dr_shadow_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
+                   uint64_t sample_base, float *out);
+int dr_shadow_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
+                         uint64_t seed, uint64_t sample_base, float *out_dev, void *stream);
+
 /* Waits for all work on the context stream. */
 int dr_synchronize(dr_ctx *ctx);
 
@@ -182,6 +197,7 @@ int dr_probe_paths(dr_ctx *ctx, const uint32_t *px, const uint32_t *py, const ui
 #define DR_PROBE_SUN_SAMPLE 2u     /* in: u1[n],u2[n]      out: 3n */
 #define DR_PROBE_SKY 3u            /* in: rd[3n]           out: 3n */
 #define DR_PROBE_MIE_THETA 4u      /* in: u1[n]            out: n (theta / pi) */
+#define DR_PROBE_MIE_EXACT_DIR 5u  /* in: u1[n]            out: 2n (ct, st) of the exact sampler */
 int dr_probe_sampler(dr_ctx *ctx, uint32_t what, const float *in, uint32_t n, float *out);
 /* Fraction of nsamp delta-tracked segments along each ray that escape. */
 int dr_probe_transmittance(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,

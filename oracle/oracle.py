@@ -32,7 +32,8 @@ class OrcParams(C.Structure):
         ("sky_cfg", (C.c_float * 9) * 3), ("sky_rad", C.c_float * 3),
         ("mie_pdf", C.c_void_p), ("mie_cdf", C.c_void_p), ("mie_n", C.c_uint32),
         ("viewi", C.c_float * 16), ("proji", C.c_float * 16), ("w", C.c_uint32), ("h", C.c_uint32),
-        ("depth", C.c_float),
+        ("depth", C.c_float), ("depth_map", C.c_void_p), ("depthcomp", C.c_uint32),
+        ("phase_mode", C.c_uint32), ("mie_exact", C.c_void_p),
     ]
 
 
@@ -82,6 +83,11 @@ class Port:
         L.orc_render_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                          C.c_uint64, C.c_uint64, vp, vp, C.POINTER(OrcCounters), C.c_int]
         L.orc_render_tile_mt.restype = C.c_int
+        L.orc_mie_exact_table.argtypes = [vp, u32, vp]
+        L.orc_mie_exact_dirs.argtypes = [vp, u32, vp, u32, vp, vp]
+        L.orc_shadow_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
+                                         C.c_uint64, C.c_uint64, vp, C.POINTER(OrcCounters), C.c_int]
+        L.orc_shadow_tile_mt.restype = C.c_int
         L.orc_render_path.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, C.c_uint64, C.c_uint64,
                                       vp, vp, C.POINTER(OrcCounters)]
         L.orc_transmittance_mc.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), vp, vp, C.c_uint64, C.c_uint64]
@@ -150,7 +156,32 @@ class Port:
         P.proji[:] = [float(v) for v in cfg["proji"]]
         P.w, P.h = cfg["w"], cfg["h"]
         P.depth = float(np.finfo(np.float32).max)
+        if cfg.get("depth") is not None:
+            dm = np.ascontiguousarray(cfg["depth"], np.float32).reshape(-1)
+            assert dm.size == cfg["w"] * cfg["h"]
+            keep.append(dm)
+            P.depth_map = dm.ctypes.data
+            P.depthcomp = 1 if cfg.get("depthcomp") else 0
+        if cfg.get("phase_mode", 0) == 1:
+            tab = Port().mie_exact_table(pdf)
+            keep.append(tab)
+            P.phase_mode, P.mie_exact = 1, tab.ctypes.data
         return P
+
+    def mie_exact_table(self, pdf: np.ndarray) -> np.ndarray:
+        """Exact-mode sampler table from the RGB pdf (n x 3): 8 n + 4 floats."""
+        pdf = np.ascontiguousarray(pdf, np.float32)
+        out = np.zeros(8 * len(pdf) + 4, np.float32)
+        self.L.orc_mie_exact_table(_p(pdf), len(pdf), _p(out))
+        return out
+
+    def mie_exact_dirs(self, tab: np.ndarray, n: int, u1: np.ndarray):
+        """(ct, st) of exact-mode samples for the uniforms u1."""
+        u1 = np.ascontiguousarray(u1, np.float32)
+        ct = np.zeros(len(u1), np.float32)
+        st = np.zeros(len(u1), np.float32)
+        self.L.orc_mie_exact_dirs(_p(tab), n, _p(u1), len(u1), _p(ct), _p(st))
+        return ct, st
 
     def render_tile(self, S, P, x0, y0, tw, th, spp, seed, sample_base=0, threads=0):
         sun = np.zeros((th, tw, 4), np.float32)
@@ -160,6 +191,14 @@ class Port:
         self.L.orc_render_tile_mt(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base, _p(sun), _p(sky),
                                   C.byref(cnt), nt)
         return sun, sky, cnt.as_dict()
+
+    def shadow_tile(self, S, P, x0, y0, tw, th, spp, seed, sample_base=0, threads=0):
+        out = np.zeros((th, tw, 4), np.float32)
+        cnt = OrcCounters()
+        nt = threads if threads > 0 else (os.cpu_count() or 1)
+        self.L.orc_shadow_tile_mt(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base, _p(out),
+                                  C.byref(cnt), nt)
+        return out, cnt.as_dict()
 
     def render_path(self, S, P, px, py, seed, sample):
         a = np.zeros(4, np.float32)
@@ -187,8 +226,10 @@ class Reference:
         L.ref_solar_elevation.argtypes = [vp]
         L.ref_solar_elevation.restype = f32
         L.ref_render.argtypes = [vp, vp, vp, vp, vp, f32, f64, f64, u32, f32, f32, u32, u32, u32, u32, u32, u32, u32,
-                                 vp, vp]
+                                 vp, vp, vp, u32]
         L.ref_render.restype = C.c_int
+        L.ref_shadow.argtypes = [vp, vp, vp, vp, vp, f32, u32, f32, f32, u32, u32, u32, u32, u32, u32, u32, vp, vp]
+        L.ref_shadow.restype = C.c_int
         L.ref_sample_voxel_space.argtypes = [vp, vp, vp, u32]
         L.ref_sample_voxel_space.restype = f32
         L.ref_mie_table_size.restype = u32
@@ -286,10 +327,27 @@ class _RefScene:
         sc = np.ascontiguousarray(cfg["sun_color"], np.float32)
         sun = np.zeros((th, tw, 4), np.float32)
         sky = np.zeros((th, tw, 4), np.float32)
+        depth = None if cfg.get("depth") is None else np.ascontiguousarray(cfg["depth"], np.float32).reshape(-1)
         rc = self.ref.L.ref_render(self.h, _p(viewi), _p(proji), _p(sd), _p(sc), float(cfg["sun_angle"]),
                                    float(cfg["turbidity"]), float(cfg["ground_albedo"]), int(cfg["scattevs"]),
                                    float(cfg["sigma_s"]), float(cfg["sigma_a"]), int(cfg["w"]), int(cfg["h"]),
-                                   x0, y0, tw, th, spp, _p(sun), _p(sky))
+                                   x0, y0, tw, th, spp, _p(sun), _p(sky), None if depth is None else _p(depth),
+                                   1 if cfg.get("depthcomp") else 0)
         if rc != 0:
             raise RuntimeError("ref_render failed")
         return sun, sky
+
+    def shadow(self, cfg: dict, x0, y0, tw, th, spp):
+        """RenderKernel::Shadow over one tile; returns the phb[0] float4 tile (sums over spp)."""
+        viewi = np.ascontiguousarray(cfg["viewi"], np.float32)
+        proji = np.ascontiguousarray(cfg["proji"], np.float32)
+        sd = np.ascontiguousarray(cfg["sun_dir"], np.float32)
+        sc = np.ascontiguousarray(cfg["sun_color"], np.float32)
+        out = np.zeros((th, tw, 4), np.float32)
+        depth = None if cfg.get("depth") is None else np.ascontiguousarray(cfg["depth"], np.float32).reshape(-1)
+        rc = self.ref.L.ref_shadow(self.h, _p(viewi), _p(proji), _p(sd), _p(sc), float(cfg["sun_angle"]),
+                                   int(cfg["scattevs"]), float(cfg["sigma_s"]), float(cfg["sigma_a"]), int(cfg["w"]),
+                                   int(cfg["h"]), x0, y0, tw, th, spp, None if depth is None else _p(depth), _p(out))
+        if rc != 0:
+            raise RuntimeError("ref_shadow failed")
+        return out

@@ -53,7 +53,12 @@ typedef struct {
     /* camera: rows r[0..3] of the inverse view / projection matrices */
     float viewi[16], proji[16];
     uint32_t w, h;
-    float depth;           /* compositing depth (FLT_MAX when unused) */
+    float depth;           /* compositing depth of every camera ray (FLT_MAX when unused) */
+    /* per-pixel depth texture, w*h row-major, or NULL (src/kernel.cpp:548-554, 579-585) */
+    const float *depth_map;
+    uint32_t depthcomp;    /* KERNEL_DEPTHCOMP: camera rays stop at depth_map */
+    uint32_t phase_mode;   /* 0 = the reference's sampler, 1 = exact inverse CDF */
+    const float *mie_exact;/* exact-mode table (orc_mie_exact_table), 8 n + 4 floats */
 } orc_params;
 
 typedef struct {
@@ -89,6 +94,11 @@ float orc_mie_eval(const orc_params *P, float ct);
 float orc_mie_sample_theta_scan(const orc_params *P, float u1);   /* reference linear scan */
 float orc_mie_sample_theta_bisect(const orc_params *P, float u1); /* same bin by bisection */
 void orc_mie_sample(const orc_params *P, const float iv[3], float u1, float u2, float out[3]);
+/* exact-mode sampler: table from the red pdf column, direction of a sample */
+void orc_mie_exact_table(const float *pdf_rgb, uint32_t n, float *out);
+void orc_mie_exact_dir(const float *tab, uint32_t n, float u1, float *ct, float *st);
+void orc_mie_exact_dirs(const float *tab, uint32_t n, const float *u1, uint32_t count, float *ct, float *st);
+void orc_mie_sample_exact(const orc_params *P, const float iv[3], float u1, float u2, float out[3]);
 void orc_sun_eval(const orc_params *P, const float rd[3], float out[3]);
 float orc_sun_pdf(const orc_params *P, const float v[3]);
 void orc_sun_sample(const orc_params *P, float u1, float u2, float out[3]);
@@ -113,6 +123,15 @@ int orc_render_tile(const orc_scene *S, const orc_params *P, uint32_t x0, uint32
                     uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
                     orc_counters *cnt);
 /* A single path sample, for per-path comparisons. */
+/* One tile of RenderKernel::Shadow (src/kernel.cpp:569-607): per pixel, the
+ * sum over spp sun-direction samples of the shadow-segment result divided by
+ * the sun colour, from the point at the pixel's depth along the camera ray.
+ * Sample s of pixel p draws from PCG32 stream (seed, p, sample_base + s). */
+int orc_shadow_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                       uint32_t spp, uint64_t seed, uint64_t sample_base, float *out, orc_counters *cnt,
+                       int nthreads);
+void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
+                     uint64_t sample, float out[4], orc_counters *cnt);
 void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
                      uint64_t sample, float out_sun[4], float out_sky[4], orc_counters *cnt);
 

@@ -81,8 +81,12 @@ static int track_depth(const orc_scene *S, const orc_params *P, const float ro[3
             const float q = orc_rng_uniform(g);
             rm = rm && (rho / smax < q);
             if (!rm) {
+                /* src/kernel.cpp:214-217, 370-384: the lane's mask mm = td < depth
+                 * is re-evaluated on the next leaf step; alpha is taken from rm
+                 * first (1: collided), then rm |= !mm makes a collision at or
+                 * beyond the depth no scattering event (2). */
                 *td_out = td;
-                return 0;
+                return td < depth ? 0 : 2;
             }
             sr = sr - orc_log(orc_rng_uniform(g)) / denom;
         }
@@ -93,7 +97,7 @@ static int track_depth(const orc_scene *S, const orc_params *P, const float ro[3
 
 int orc_track(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], void *rng, float *td,
               orc_counters *cnt) {
-    return track_depth(S, P, ro, rd, (orc_rng *)rng, FLT_MAX, td, cnt);
+    return track_depth(S, P, ro, rd, (orc_rng *)rng, FLT_MAX, td, cnt) != 0;
 }
 
 void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
@@ -107,12 +111,14 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
     orc_rng_seed(&g, seed, (uint64_t)py * P->w + px, sample);
     if (cnt) cnt->paths++;
     const float f = P->sigma_s / (P->sigma_a + P->sigma_s);
+    const float depth0 = (P->depth_map && P->depthcomp) ? P->depth_map[(size_t)py * P->w + px] : P->depth;
     float T[3] = {1.0f, 1.0f, 1.0f};
     uint32_t r = 0;
     for (;;) {
         float td;
-        int esc = track_depth(S, P, ro, rd, &g, r == 0 ? P->depth : FLT_MAX, &td, cnt);
-        if (r == 0) out_sun[3] = out_sky[3] = esc ? 0.0f : 1.0f;
+        int esc = track_depth(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, cnt);
+        if (r == 0) out_sun[3] = out_sky[3] = esc == 1 ? 0.0f : 1.0f;
+        if (esc == 2) break;
         if (esc) {
             if (r > 0) {
                 float sun[3], sky[3];
@@ -128,7 +134,8 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
         if (r >= P->scattevs) break;
         float srd[3], lrd[3], p1[3], p3[3], rc[3];
         const float u1 = orc_rng_uniform(&g), u2 = orc_rng_uniform(&g);
-        orc_mie_sample(P, rd, u1, u2, srd);
+        if (P->phase_mode == 1) orc_mie_sample_exact(P, rd, u1, u2, srd);
+        else orc_mie_sample(P, rd, u1, u2, srd);
         const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
         orc_sun_sample(P, u3, u4, lrd);
         orc_mie_eval_rgb(P, dot3(srd, rd), p1);
@@ -152,6 +159,46 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
     }
 }
 
+/* RenderKernel::Shadow for one (pixel, sample), src/kernel.cpp:569-607.  The
+ * camera ray is cut at the pixel's depth when that lies before the far clip
+ * plane (clip_end = -z/w of (0,0,1,1) * projInv); from there one shadow segment
+ * runs along a sun-cone sample with r = scattevs (SampleVolume: escape gives
+ * sun(lrd), a collision 0).  A pixel without geometry in front of the far plane
+ * traces nothing and gets sun(lrd), as its mask lane keeps "not scattering".
+ * The result is divided by float4::load(&color), whose w is 0: alpha becomes
+ * 1/0 = +inf per sample (scattevs > 0: the r > 0 branch sets alpha 1 on every
+ * lane), rgb = sun(lrd) / colour. */
+void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
+                     uint64_t sample, float out[4], orc_counters *cnt) {
+    for (int k = 0; k < 4; ++k) out[k] = 0.0f;
+    float ro[3], rd[3];
+    int inf;
+    orc_camera_ray(P, px, py, ro, rd, &inf);
+    if (!inf) return;
+    if (cnt) cnt->paths++;
+    const float zz = P->proji[8 + 2] + P->proji[12 + 2], zw = P->proji[8 + 3] + P->proji[12 + 3];
+    const float clip_end = -zz / zw;
+    const float depth = P->depth_map ? P->depth_map[(size_t)py * P->w + px] : FLT_MAX;
+    const int active = depth < clip_end;
+    orc_rng g;
+    orc_rng_seed(&g, seed, (uint64_t)py * P->w + px, sample);
+    const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
+    float lrd[3];
+    orc_sun_sample(P, u3, u4, lrd);
+    int esc = 1;
+    if (active) {
+        float ro1[3], td;
+        for (int k = 0; k < 3; ++k) ro1[k] = ro[k] + rd[k] * depth;
+        esc = track_depth(S, P, ro1, lrd, &g, FLT_MAX, &td, cnt);
+    }
+    float lc[3] = {0.0f, 0.0f, 0.0f};
+    if (P->scattevs > 0 && esc) orc_sun_eval(P, lrd, lc);
+    const float color_w = 0.0f;
+    const float a = (P->scattevs > 0 || !esc) ? 1.0f : 0.0f;
+    for (int k = 0; k < 3; ++k) out[k] = lc[k] / P->sun_color[k];
+    out[3] = a / color_w;
+}
+
 typedef struct {
     const orc_scene *S;
     const orc_params *P;
@@ -160,6 +207,7 @@ typedef struct {
     float *sun, *sky;
     orc_counters cnt;
     int next_row_mod, nthreads, tid;
+    int shadow;
 } tile_job;
 
 static void *tile_worker(void *arg) {
@@ -176,7 +224,12 @@ static void *tile_worker(void *arg) {
                 orc_camera_ray(J->P, J->x0 + i, J->y0 + j, ro, rd, &inf);
                 if (!inf) break;
                 any = 1;
-                orc_render_path(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, a, b, &J->cnt);
+                if (J->shadow) {
+                    orc_shadow_path(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, a, &J->cnt);
+                    for (int k = 0; k < 4; ++k) b[k] = 0.0f;
+                } else {
+                    orc_render_path(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, a, b, &J->cnt);
+                }
                 for (int k = 0; k < 4; ++k) {
                     acc_sun[k] += a[k];
                     acc_sky[k] += b[k];
@@ -184,18 +237,18 @@ static void *tile_worker(void *arg) {
             }
             if (any) {
                 memcpy(&J->sun[4 * ((size_t)j * J->tw + i)], acc_sun, 16);
-                memcpy(&J->sky[4 * ((size_t)j * J->tw + i)], acc_sky, 16);
+                if (J->sky) memcpy(&J->sky[4 * ((size_t)j * J->tw + i)], acc_sky, 16);
             }
         }
     }
     return 0;
 }
 
-int orc_render_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
-                       uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
-                       orc_counters *cnt, int nthreads) {
+static int tile_run(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                    uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
+                    orc_counters *cnt, int nthreads, int shadow) {
     memset(out_sun, 0, sizeof(float) * 4 * (size_t)tw * th);
-    memset(out_sky, 0, sizeof(float) * 4 * (size_t)tw * th);
+    if (out_sky) memset(out_sky, 0, sizeof(float) * 4 * (size_t)tw * th);
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
     tile_job jobs[256];
@@ -205,7 +258,7 @@ int orc_render_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uin
         memset(J, 0, sizeof(*J));
         J->S = S; J->P = P; J->x0 = x0; J->y0 = y0; J->tw = tw; J->th = th; J->spp = spp;
         J->rows = 2 * (th / 2); J->seed = seed; J->base = sample_base; J->sun = out_sun; J->sky = out_sky;
-        J->nthreads = nthreads; J->tid = t;
+        J->nthreads = nthreads; J->tid = t; J->shadow = shadow;
     }
     for (int t = 1; t < nthreads; ++t) pthread_create(&th_ids[t], 0, tile_worker, &jobs[t]);
     tile_worker(&jobs[0]);
@@ -220,6 +273,18 @@ int orc_render_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uin
         }
     }
     return 0;
+}
+
+int orc_render_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                       uint32_t spp, uint64_t seed, uint64_t sample_base, float *out_sun, float *out_sky,
+                       orc_counters *cnt, int nthreads) {
+    return tile_run(S, P, x0, y0, tw, th, spp, seed, sample_base, out_sun, out_sky, cnt, nthreads, 0);
+}
+
+int orc_shadow_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                       uint32_t spp, uint64_t seed, uint64_t sample_base, float *out, orc_counters *cnt,
+                       int nthreads) {
+    return tile_run(S, P, x0, y0, tw, th, spp, seed, sample_base, out, 0, cnt, nthreads, 1);
 }
 
 int orc_render_tile(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,

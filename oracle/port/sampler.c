@@ -16,6 +16,7 @@
 #include "orc_math.h"
 #include <math.h>
 #include <float.h>
+#include <stdlib.h>
 
 static inline float sse_max(float a, float b) { return a > b ? a : b; } /* _mm_max_ps(a,b) */
 static inline float sse_min(float a, float b) { return a < b ? a : b; } /* _mm_min_ps(a,b) */
@@ -147,6 +148,114 @@ void orc_mie_sample(const orc_params *P, const float iv[3], float u1, float u2, 
     orc_sincos(th, &s_, &c_);
     float ct = -c_; /* -cos_ps(): sign flip of the __m128 */
     float st = sqrtf(sse_max(1.0f - ct * ct, 0.0f));
+    compose_dir(b1, b2, iv, st, ct, ph, out);
+}
+
+/* ---- exact-mode Mie sampler (DR_PHASE_MIE_EXACT) ---------------------------
+ * Target density over phi = acos(-ct) in [0, pi] (phi = 0 is backscatter):
+ * f(phi) sin(phi), with f the red channel of the table interpolated linearly in
+ * phi exactly as MiePhase::Evaluate interpolates it (src/KernelSampler.cpp:
+ * 214-231: knots at phi_k = k pi / n, the last bin extrapolating the line
+ * through the last two entries).  Bin k carries f = f0 + beta (phi - phi_k) and
+ * mass M_k = H_k(pi/n), where H_k(x) = int_0^x (f0 + beta s) sin(phi_k + s) ds
+ *   = S [(f0 + beta x) sin x - beta (1 - cos x)]
+ *   + C [f0 (1 - cos x) + beta (sin x - x cos x)],   S, C = sin, cos(phi_k).
+ * The sampler inverts the CDF exactly: the bin by bisection on the
+ * cumulative masses, then x in [0, pi/n] by safeguarded Newton on H_k.
+ * Table (float): per bin (cdf_k, f0, beta, M_k), (S, C, pi/n, 0); then (1, 0, 0, 0). */
+void orc_mie_exact_table(const float *pdf_rgb, uint32_t n, float *out) {
+    const double dphi = 3.14159265358979323846 / (double)n;
+    double *mass = (double *)malloc(sizeof(double) * n);
+    double total = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        double fa, fb;
+        if (k + 1 < n) {
+            fa = pdf_rgb[3 * k];
+            fb = pdf_rgb[3 * (k + 1)];
+        } else {
+            fa = pdf_rgb[3 * (n - 1)];
+            fb = 2.0 * pdf_rgb[3 * (n - 1)] - pdf_rgb[3 * (n - 2)];
+        }
+        if (fa < 0.0) fa = 0.0;
+        if (fb < 0.0) fb = 0.0;
+        const double beta = (fb - fa) / dphi, phi = dphi * (double)k, x = dphi;
+        const double S = sin(phi), C = cos(phi);
+        const double m = S * ((fa + beta * x) * sin(x) - beta * (1.0 - cos(x))) +
+                         C * (fa * (1.0 - cos(x)) + beta * (sin(x) - x * cos(x)));
+        mass[k] = m > 0.0 ? m : 0.0;
+        float *o = out + 8 * (size_t)k;
+        o[1] = (float)fa;
+        o[2] = (float)beta;
+        o[3] = (float)mass[k];
+        o[4] = (float)S;
+        o[5] = (float)C;
+        o[6] = (float)dphi;
+        o[7] = 0.0f;
+        total += mass[k];
+    }
+    double acc = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        out[8 * (size_t)k] = (float)(acc / total);
+        acc += mass[k];
+    }
+    float *e = out + 8 * (size_t)n;
+    e[0] = 1.0f;
+    e[1] = e[2] = e[3] = 0.0f;
+    free(mass);
+}
+
+/* sin x, 1 - cos x and sin x - x cos x by their Taylor series (x <= pi/4) */
+static inline void local_trig(float x, float *sx, float *omc, float *sxc) {
+    const float x2 = x * x;
+    *sx = x * (1.0f - (x2 / 6.0f) * (1.0f - (x2 / 20.0f) * (1.0f - (x2 / 42.0f) * (1.0f - x2 / 72.0f))));
+    *omc = (x2 / 2.0f) * (1.0f - (x2 / 12.0f) * (1.0f - (x2 / 30.0f) * (1.0f - (x2 / 56.0f) * (1.0f - x2 / 90.0f))));
+    *sxc = ((x2 * x) / 3.0f) * (1.0f - (x2 / 10.0f) * (1.0f - (x2 / 28.0f) * (1.0f - x2 / 54.0f)));
+}
+
+/* ct = -cos(phi) and st = sin(phi) of the exact-mode sample for u1. */
+void orc_mie_exact_dir(const float *tab, uint32_t n, float u1, float *ct, float *st) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (tab[8 * (size_t)mid] <= u1) lo = mid;
+        else hi = mid - 1;
+    }
+    const float *b = tab + 8 * (size_t)lo;
+    const float c0 = b[0], c1 = tab[8 * (size_t)(lo + 1)];
+    const float f0 = b[1], beta = b[2], mk = b[3], S = b[4], C = b[5], dx = b[6];
+    const float d = c1 - c0;
+    const float up = d > 0.0f ? (u1 - c0) / d : 0.5f;
+    const float m = up * mk;
+    float xl = 0.0f, xh = dx, x = up * dx;
+    for (int it = 0; it < 8; ++it) {
+        float sx, omc, sxc;
+        local_trig(x, &sx, &omc, &sxc);
+        const float fx = f0 + beta * x;
+        const float h = (S * (fx * sx - beta * omc) + C * (f0 * omc + beta * sxc)) - m;
+        const float hp = fx * (S * (1.0f - omc) + C * sx);
+        if (h > 0.0f) xh = x;
+        else xl = x;
+        float xn = hp > 0.0f ? x - h / hp : 0.5f * (xl + xh);
+        if (!(xn > xl && xn < xh)) xn = 0.5f * (xl + xh);
+        x = xn;
+    }
+    float sx, omc, sxc;
+    local_trig(x, &sx, &omc, &sxc);
+    const float cx = 1.0f - omc;
+    *ct = 0.0f - (C * cx - S * sx);
+    *st = sse_max(S * cx + C * sx, 0.0f);
+}
+
+void orc_mie_exact_dirs(const float *tab, uint32_t n, const float *u1, uint32_t count, float *ct, float *st) {
+    for (uint32_t i = 0; i < count; ++i) orc_mie_exact_dir(tab, n, u1[i], &ct[i], &st[i]);
+}
+
+void orc_mie_sample_exact(const orc_params *P, const float iv[3], float u1, float u2, float out[3]) {
+    float ct, st;
+    orc_mie_exact_dir(P->mie_exact, P->mie_n, u1, &ct, &st);
+    const float ph = (2.0f * ORC_PI) * u2;
+    float b1[3], b2[3];
+    sampling_basis(iv, b1, b2);
     compose_dir(b1, b2, iv, st, ct, ph, out);
 }
 

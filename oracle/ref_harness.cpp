@@ -20,6 +20,7 @@
 #include "ArHosekSkyModel.h"
 
 #include <cstring>
+#include <vector>
 #include <cstdio>
 #include <cstdarg>
 #include <cmath>
@@ -126,10 +127,11 @@ extern "C" float ref_solar_elevation(const float sun_dir[3]) {
  * (7, 0.15) of src/kernel.cpp:525.  Outputs are the two tile buffers phb[0]
  * (sun) and phb[1] (sky) as float4 per pixel, row-major in the tile; pixels the
  * reference leaves unwritten (outside the frame, odd last row/column) are 0. */
-extern "C" int ref_render(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
-                          const float sun_color[3], float sun_angle, double turbidity, double albedo,
-                          unsigned scattevs, float sigma_s, float sigma_a, unsigned w, unsigned h, unsigned x0,
-                          unsigned y0, unsigned tw, unsigned th, unsigned spp, float *out_sun, float *out_sky) {
+static int ref_run(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
+                   const float sun_color[3], float sun_angle, double turbidity, double albedo, unsigned scattevs,
+                   float sigma_s, float sigma_a, unsigned w, unsigned h, unsigned x0, unsigned y0, unsigned tw,
+                   unsigned th, unsigned spp, const float *depth, unsigned flags, int shadow, float *out_sun,
+                   float *out_sky) {
     Scene *s = (Scene *)p;
     KernelSampler::BaseLight::DeleteAll();
     dfloat3 D(sun_dir[0], sun_dir[1], sun_dir[2]);
@@ -141,19 +143,44 @@ extern "C" int ref_render(void *p, const float viewi[16], const float proji[16],
         vi.r[r] = dfloat4(viewi[4 * r + 0], viewi[4 * r + 1], viewi[4 * r + 2], viewi[4 * r + 3]);
         pi.r[r] = dfloat4(proji[4 * r + 0], proji[4 * r + 1], proji[4 * r + 2], proji[4 * r + 3]);
     }
+    std::vector<float> dcopy;
+    if (depth) dcopy.assign(depth, depth + (size_t)w * h);
     RenderKernel k;
-    if (!k.Initialize(s, 0, &vi, &pi, &KernelSampler::MiePhase::gmie, &KernelSampler::NullEnv::nenv, 0, scattevs,
-                      sigma_s, sigma_a, tw, th, w, h, 0))
+    if (!k.Initialize(s, 0, &vi, &pi, &KernelSampler::MiePhase::gmie, &KernelSampler::NullEnv::nenv,
+                      depth ? dcopy.data() : 0, scattevs, sigma_s, sigma_a, tw, th, w, h, flags))
         return -1;
     arhosekskymodelstate_free(k.pskyms);
     float se = ref_solar_elevation(sun_dir);
     k.pskyms = arhosek_rgb_skymodelstate_alloc_init(turbidity, albedo, se);
     std::memset(k.phb[0], 0, (size_t)tw * th * 16);
     std::memset(k.phb[1], 0, (size_t)tw * th * 16);
-    k.Render(x0, y0, tw, th, spp);
+    if (shadow)
+        k.Shadow(x0, y0, tw, th, spp);
+    else
+        k.Render(x0, y0, tw, th, spp);
     std::memcpy(out_sun, k.phb[0], (size_t)tw * th * 16);
-    std::memcpy(out_sky, k.phb[1], (size_t)tw * th * 16);
+    if (out_sky) std::memcpy(out_sky, k.phb[1], (size_t)tw * th * 16);
     k.Destroy();
     KernelSampler::BaseLight::DeleteAll();
     return 0;
+}
+
+/* RenderKernel::Render over one tile (src/kernel.cpp:536-567); depth (w*h or
+ * NULL) and flags (KERNEL_DEPTHCOMP) as RenderKernel::Initialize takes them. */
+extern "C" int ref_render(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
+                          const float sun_color[3], float sun_angle, double turbidity, double albedo,
+                          unsigned scattevs, float sigma_s, float sigma_a, unsigned w, unsigned h, unsigned x0,
+                          unsigned y0, unsigned tw, unsigned th, unsigned spp, float *out_sun, float *out_sky,
+                          const float *depth, unsigned flags) {
+    return ref_run(p, viewi, proji, sun_dir, sun_color, sun_angle, turbidity, albedo, scattevs, sigma_s, sigma_a, w,
+                   h, x0, y0, tw, th, spp, depth, flags, 0, out_sun, out_sky);
+}
+
+/* RenderKernel::Shadow over one tile (src/kernel.cpp:569-607): phb[0] only. */
+extern "C" int ref_shadow(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
+                          const float sun_color[3], float sun_angle, unsigned scattevs, float sigma_s, float sigma_a,
+                          unsigned w, unsigned h, unsigned x0, unsigned y0, unsigned tw, unsigned th, unsigned spp,
+                          const float *depth, float *out) {
+    return ref_run(p, viewi, proji, sun_dir, sun_color, sun_angle, 3.0, 0.3, scattevs, sigma_s, sigma_a, w, h, x0,
+                   y0, tw, th, spp, depth, 0, 1, out, 0);
 }

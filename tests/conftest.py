@@ -78,7 +78,24 @@ def settings_from_cfg(cfg: dict):
         sun_color=cfg["sun_color"], sun_angle=cfg["sun_angle"],
         sky=SkyState(np.asarray(cfg["sky_configs"]), np.asarray(cfg["sky_radiances"])),
         phase=PhaseTable(cfg["mie_pdf"], cfg["mie_cdf"]), viewi=cfg["viewi"], proji=cfg["proji"], w=cfg["w"],
-        h=cfg["h"])
+        h=cfg["h"], depth=cfg.get("depth"), depthcomp=bool(cfg.get("depthcomp", False)),
+        phase_mode=int(cfg.get("phase_mode", 0)))
+
+
+def depth_texture(w: int, h: int) -> np.ndarray:
+    """Depth texture for the shadow-pass and compositing checks: every third pixel
+    has no geometry before the far plane (1e30), the others sit 2.3-2.7 units
+    along the camera ray (inside the config-0 cloud, 2.5 units from the camera)."""
+    j, i = np.mgrid[0:h, 0:w]
+    d = (2.3 + 0.4 * ((i * 7 + j * 3) % 11) / 10.0).astype(np.float32)
+    d[(i + j) % 3 == 0] = np.float32(1e30)
+    return d
+
+
+def clip_end(proji) -> np.float32:
+    """Far clip distance of RenderKernel::Shadow: -z/w of (0,0,1,1) * projInv."""
+    q = np.asarray(proji, np.float32).reshape(4, 4)
+    return np.float32(-np.float32(q[2, 2] + q[3, 2]) / np.float32(q[2, 3] + q[3, 3]))
 
 
 @pytest.fixture(scope="session")

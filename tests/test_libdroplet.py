@@ -146,3 +146,33 @@ def test_addon_flow_renders_tiles(lib):
             a, b = r.render_tile(16, 16, 32, 32, 8)
             ref += a + b
     assert np.allclose(acc, ref.reshape(-1, 4), rtol=1e-3, atol=1e-5 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
+def test_addon_shadow_pass(lib):
+    """libdroplet.Shadow as RenderShadow (addon/__init__.py:126-152) drives it:
+    QueryResult(0) holds the shadow sums of the tile, equal to the renderer's."""
+    from conftest import depth_texture, golden_octree, settings_from_cfg
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree
+
+    scene = fake_scene()
+    scene.droplet_depth = depth_texture(64, 64)
+    lib.BeginRender(scene, NS(), 32, 32, 64, 64, 1)
+    wait_ready(lib)
+    lib.Shadow(8, 8, 32, 32, 100)
+    while True:
+        qr = lib.QueryResult(0)
+        if qr is not None:
+            break
+    got = np.asarray(qr, np.float64)
+    assert got.shape == (32 * 32, 4)
+    nodes, bricks, mlevel = golden_octree()
+    cfg = c0_cfg(64, 64)
+    cfg["depth"] = depth_texture(64, 64)
+    with Renderer(0) as r:
+        r.upload(Octree(nodes, bricks, mlevel))
+        r.set_params(settings_from_cfg(cfg))
+        ref, _ = r.render_shadow_tile(8, 8, 32, 32, 100)
+    assert np.array_equal(got[:, :3], ref.reshape(-1, 4)[:, :3])
+    assert (got[:, :3] < 100).any() and np.isposinf(got[:, 3]).all()
