@@ -9,148 +9,28 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "../../include/droplet_b200.h"
+#include "dr_host.h"
 #include "dr_internal.h"
 #include "dr_kernels.h"
 
 namespace dr {
-
-static thread_local std::string g_error;
-
-void set_error(int code, const std::string &msg) {
-    (void)code;
-    g_error = msg;
-}
 
 int build_octree(const int32_t *org, const float *vals, uint32_t n_blocks, float s, uint32_t maxdepth, int nthreads,
                  dr_octree *out);
 int sky_cook(const double *const rgb[3], const double *const rad[3], double turbidity, double albedo,
              double elevation, double configs[3][9], double radiances[3]);
 
-// Exact-mode phase sampler table (DR_PHASE_MIE_EXACT).  Target density over
-// phi = acos(-ct): f(phi) sin(phi), f the red pdf column interpolated linearly
-// in phi as MiePhase::Evaluate does (src/KernelSampler.cpp:214-231; knots at
-// k pi / n, the last bin extrapolating the last two entries, clamped at 0).
-// Per bin k, in FP64: f0 = f(phi_k), beta = slope, mass
-//   M_k = S[(f0 + beta d) sin d - beta (1 - cos d)] + C[f0 (1 - cos d) + beta (sin d - d cos d)]
-// (the integral of f sin over the bin, d = pi/n, S, C = sin, cos phi_k).
-// Layout (float): per bin (cdf_k, f0, beta, M_k), (S, C, d, 0); then (1, 0, 0, 0).
-static void mie_exact_table(const float *pdf_rgb, uint32_t n, float *out) {
-    const double d = 3.14159265358979323846 / (double)n;
-    std::vector<double> mass(n);
-    double total = 0.0;
-    for (uint32_t k = 0; k < n; ++k) {
-        double fa = k + 1 < n ? (double)pdf_rgb[3 * k] : (double)pdf_rgb[3 * (n - 1)];
-        double fb = k + 1 < n ? (double)pdf_rgb[3 * (k + 1)]
-                              : 2.0 * (double)pdf_rgb[3 * (n - 1)] - (double)pdf_rgb[3 * (n - 2)];
-        fa = fa < 0.0 ? 0.0 : fa;
-        fb = fb < 0.0 ? 0.0 : fb;
-        const double beta = (fb - fa) / d, phi = d * (double)k;
-        const double S = std::sin(phi), C = std::cos(phi);
-        const double m = S * ((fa + beta * d) * std::sin(d) - beta * (1.0 - std::cos(d))) +
-                         C * (fa * (1.0 - std::cos(d)) + beta * (std::sin(d) - d * std::cos(d)));
-        mass[k] = m > 0.0 ? m : 0.0;
-        float *o = out + 8 * (size_t)k;
-        o[1] = (float)fa;
-        o[2] = (float)beta;
-        o[3] = (float)mass[k];
-        o[4] = (float)S;
-        o[5] = (float)C;
-        o[6] = (float)d;
-        o[7] = 0.0f;
-        total += mass[k];
-    }
-    double acc = 0.0;
-    for (uint32_t k = 0; k < n; ++k) {
-        out[8 * (size_t)k] = (float)(acc / total);
-        acc += mass[k];
-    }
-    float *e = out + 8 * (size_t)n;
-    e[0] = 1.0f;
-    e[1] = e[2] = e[3] = 0.0f;
-}
-
-static int cuda_fail(cudaError_t e, const char *what) {
-    g_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-    return e == cudaErrorMemoryAllocation ? DR_ERR_NOMEM : DR_ERR_CUDA;
-}
-
-#define DR_CUDA(call, what)                                  \
-    do {                                                     \
-        cudaError_t e_ = (call);                             \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what);   \
-    } while (0)
-
-template <typename T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    cudaError_t reserve(size_t count) {
-        if (count <= n && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        cudaError_t e = cudaMalloc(&p, sizeof(T) * (count ? count : 1));
-        if (e == cudaSuccess) n = count;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
-
 }  // namespace dr
 
 using namespace dr;
 
-struct dr_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;
-    bool has_scene = false, has_params = false;
-    DevScene scene{};
-    DevParams params{};
-    DevBuf<uint4> child;
-    DevBuf<float4> leaf;
-    DevBuf<float> bricks;
-    DevBuf<unsigned char> mie_pack;
-    DevBuf<float> depth;
-    DevBuf<DevCounters> counters;
-    DevBuf<float4> tile_sun, tile_sky;
-    DevBuf<unsigned char> scratch;
-    DevBuf<WorkQueue> work;
-    DevBuf<uint32_t> macro, cells;
-    bool use_grid = true;
-    Tuning tuning{0u, 128u, 0u, 8u, 0u};
-    std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)
-};
 
-namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
-
-int need(bool ok, int code, const char *msg) {
-    if (!ok) set_error(code, msg);
-    return ok ? DR_OK : code;
-}
-
-}  // namespace
 
 extern "C" {
 
 int dr_version(void) { return 100; }
 
-const char *dr_last_error(void) { return g_error.c_str(); }
+const char *dr_last_error(void) { return last_error(); }
 
 int dr_device_count(int *count) {
     if (!count) return need(false, DR_ERR_INVALID, "dr_device_count: null output");
@@ -202,9 +82,7 @@ int dr_destroy(dr_ctx *c) {
         DeviceGuard g(c->device);
         std::lock_guard<std::mutex> lk(c->mu);
         if (c->stream) cudaStreamSynchronize(c->stream);
-        c->child.release();
-        c->leaf.release();
-        c->bricks.release();
+        c->bufs.release();
         c->mie_pack.release();
         c->depth.release();
         c->counters.release();
@@ -212,8 +90,6 @@ int dr_destroy(dr_ctx *c) {
         c->tile_sky.release();
         c->scratch.release();
         c->work.release();
-        c->macro.release();
-        c->cells.release();
         if (c->stream) cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -239,184 +115,25 @@ int dr_sky_cook(const double *const dataset_rgb[3], const double *const dataset_
 }
 
 int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
-    if (!c || !s || !s->nodes || !s->bricks) return need(false, DR_ERR_INVALID, "dr_upload_scene: null argument");
-    if (s->lvoxc != kLvox) return need(false, DR_ERR_INVALID, "dr_upload_scene: bricks must be 8^3");
-    if (s->n_nodes < 2 || s->n_nodes >= kLeafBit)
-        return need(false, DR_ERR_INVALID, "dr_upload_scene: need 2 <= n_nodes < 2^31");
-    const dr_node *N = s->nodes;
-    auto is_leaf = [&](uint32_t i) { return N[i].volx[0] != DR_NONE || N[i].volx[1] != DR_NONE; };
-    if (is_leaf(0)) return need(false, DR_ERR_INVALID, "dr_upload_scene: the root must be an internal node");
-    std::vector<uint32_t> child((size_t)s->n_nodes * 8);
-    std::vector<float4> leaf((size_t)s->n_nodes * 2);
-    for (uint32_t i = 0; i < s->n_nodes; ++i) {
-        const dr_node &o = N[i];
-        if (o.volx[0] != DR_NONE)
-            return need(false, DR_ERR_INVALID, "dr_upload_scene: surface (SDF) leaves are not supported");
-        if (is_leaf(i)) {
-            if (o.volx[1] >= s->n_leaves)
-                return need(false, DR_ERR_INVALID, "dr_upload_scene: brick index out of range");
-            if (!(o.ce[3] > 0.0f) || !std::isfinite(o.ce[3]) || !(o.qval[1] >= 0.0f) || !std::isfinite(o.qval[1]))
-                return need(false, DR_ERR_INVALID, "dr_upload_scene: leaf with bad extent or majorant");
-            uint32_t bits;
-            std::memcpy(&bits, &o.volx[1], 4);
-            float fb;
-            std::memcpy(&fb, &bits, 4);
-            leaf[2 * (size_t)i] = make_float4(o.ce[0], o.ce[1], o.ce[2], o.ce[3]);
-            leaf[2 * (size_t)i + 1] = make_float4(o.qval[1], fb, 0.0f, 0.0f);
-        } else {
-            leaf[2 * (size_t)i] = make_float4(o.ce[0], o.ce[1], o.ce[2], o.ce[3]);
-            leaf[2 * (size_t)i + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t ch = o.chn[k];
-            if (ch == 0) {
-                child[8 * (size_t)i + k] = 0;
-                continue;
-            }
-            if (ch >= s->n_nodes || ch == i)
-                return need(false, DR_ERR_INVALID, "dr_upload_scene: child index out of range");
-            child[8 * (size_t)i + k] = is_leaf(ch) ? (ch | kLeafBit) : ch;
-        }
-    }
-    // Leaf grid for the cell-walk traversal: valid when the tree is a tree (each
-    // node reached once from the root) and every leaf sits at the same depth.
-    std::vector<uint32_t> macro, cells;
-    uint32_t levels = 0, n = 0, mdim = 0;
-    {
-        struct Item { uint32_t node, depth, x, y, z; };
-        std::vector<Item> stack{{0u, 0u, 0u, 0u, 0u}};
-        std::vector<uint8_t> seen(s->n_nodes, 0);
-        std::vector<Item> leaves;
-        bool ok = true;
-        int leaf_depth = -1;
-        while (!stack.empty() && ok) {
-            Item it = stack.back();
-            stack.pop_back();
-            if (seen[it.node] || it.depth > 11) { ok = false; break; }
-            seen[it.node] = 1;
-            if (is_leaf(it.node)) {
-                if (leaf_depth < 0) leaf_depth = (int)it.depth;
-                if ((int)it.depth != leaf_depth) ok = false;
-                leaves.push_back(it);
-                continue;
-            }
-            for (uint32_t k = 0; k < 8; ++k) {
-                const uint32_t ch = N[it.node].chn[k];
-                if (ch) stack.push_back({ch, it.depth + 1, 2 * it.x + (k & 1), 2 * it.y + ((k >> 1) & 1), 2 * it.z + (k >> 2)});
-            }
-        }
-        if (ok && leaf_depth >= 1) {
-            levels = (uint32_t)leaf_depth;
-            n = 1u << levels;
-            mdim = n >= 8 ? n / 8 : 1;
-            macro.assign((size_t)mdim * mdim * mdim, kNone);
-            for (const Item &lf : leaves) {
-                const size_t m = ((size_t)(lf.z >> 3) * mdim + (lf.y >> 3)) * mdim + (lf.x >> 3);
-                if (macro[m] == kNone) {
-                    macro[m] = (uint32_t)(cells.size() / 512);
-                    cells.resize(cells.size() + 512, kNone);
-                }
-                cells[(size_t)macro[m] * 512 + (lf.z & 7) * 64 + (lf.y & 7) * 8 + (lf.x & 7)] = lf.node;
-            }
-        } else {
-            macro.assign(1, kNone);
-        }
-        if (cells.empty()) cells.assign(512, kNone);
-    }
+    if (!c) return need(false, DR_ERR_INVALID, "dr_upload_scene: null argument");
+    HostScene h;
+    int rc = prepare_scene(s, h);
+    if (rc != DR_OK) return rc;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
-    const size_t nb = (size_t)s->n_leaves * kBrick;
-    DR_CUDA(cudaStreamSynchronize(c->stream), "dr_upload_scene: sync");
-    DR_CUDA(c->macro.reserve(macro.size()), "dr_upload_scene: alloc grid");
-    DR_CUDA(c->cells.reserve(cells.size()), "dr_upload_scene: alloc grid");
-    DR_CUDA(cudaMemcpyAsync(c->macro.p, macro.data(), macro.size() * 4, cudaMemcpyHostToDevice, c->stream),
-            "dr_upload_scene: copy grid");
-    DR_CUDA(cudaMemcpyAsync(c->cells.p, cells.data(), cells.size() * 4, cudaMemcpyHostToDevice, c->stream),
-            "dr_upload_scene: copy grid");
-    DR_CUDA(c->child.reserve((size_t)s->n_nodes * 2), "dr_upload_scene: alloc nodes");
-    DR_CUDA(c->leaf.reserve((size_t)s->n_nodes * 2), "dr_upload_scene: alloc leaves");
-    DR_CUDA(c->bricks.reserve(nb + 1), "dr_upload_scene: alloc bricks");
-    DR_CUDA(cudaMemcpyAsync(c->child.p, child.data(), child.size() * 4, cudaMemcpyHostToDevice, c->stream),
-            "dr_upload_scene: copy nodes");
-    DR_CUDA(cudaMemcpyAsync(c->leaf.p, leaf.data(), leaf.size() * sizeof(float4), cudaMemcpyHostToDevice, c->stream),
-            "dr_upload_scene: copy leaves");
-    if (nb)
-        DR_CUDA(cudaMemcpyAsync(c->bricks.p, s->bricks, nb * 4, cudaMemcpyHostToDevice, c->stream),
-                "dr_upload_scene: copy bricks");
-    DR_CUDA(cudaStreamSynchronize(c->stream), "dr_upload_scene: sync");
-    c->scene.child = c->child.p;
-    c->scene.leaf = c->leaf.p;
-    c->scene.bricks = c->bricks.p;
-    for (int k = 0; k < 4; ++k) c->scene.root_ce[k] = N[0].ce[k];
-    c->scene.n_nodes = s->n_nodes;
-    c->scene.n_leaves = s->n_leaves;
-    c->scene.macro = c->macro.p;
-    c->scene.cells = c->cells.p;
-    c->scene.levels = c->use_grid ? levels : 0u;
-    c->scene.n = n;
-    c->scene.mdim = mdim;
-    c->leaf_flag.assign(s->n_nodes, 0);
-    for (uint32_t i = 0; i < s->n_nodes; ++i) c->leaf_flag[i] = is_leaf(i) ? 1 : 0;
+    rc = upload_scene(h, c->bufs, c->use_grid, c->stream, c->scene);
+    if (rc != DR_OK) return rc;
+    c->leaf_flag = std::move(h.leaf_flag);
     c->has_scene = true;
     return DR_OK;
 }
 
 int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     if (!c || !p) return need(false, DR_ERR_INVALID, "dr_set_params: null argument");
-    if (!p->mie_pdf || !p->mie_cdf || p->mie_n < 4 || p->mie_n > kMieMax || (p->mie_n % 4))
-        return need(false, DR_ERR_INVALID, "dr_set_params: phase tables need 4 <= mie_n <= 4096, mie_n % 4 == 0");
-    if (p->phase_mode != DR_PHASE_MIE_REFERENCE && p->phase_mode != DR_PHASE_MIE_EXACT)
-        return need(false, DR_ERR_INVALID, "dr_set_params: unknown phase mode");
-    if (p->phase_mode == DR_PHASE_MIE_EXACT && p->mie_n > 512)
-        return need(false, DR_ERR_INVALID, "dr_set_params: the exact phase sampler takes mie_n <= 512");
-    for (uint32_t i = 0; i < p->mie_n; ++i)
-        if (!(p->mie_pdf[3 * i] >= 0.0f) || !std::isfinite(p->mie_pdf[3 * i]))
-            return need(false, DR_ERR_INVALID, "dr_set_params: phase pdf must be finite and >= 0");
-    if (p->w == 0 || p->h == 0) return need(false, DR_ERR_INVALID, "dr_set_params: empty image");
-    if (p->scattevs > 100000u) return need(false, DR_ERR_INVALID, "dr_set_params: scattevs above 100000");
-    if (!(p->sigma_s >= 0.0f) || !(p->sigma_a >= 0.0f) || !(p->sigma_s + p->sigma_a > 0.0f))
-        return need(false, DR_ERR_INVALID, "dr_set_params: cross sections must be >= 0 with a positive sum");
-    DevParams d{};
-    d.sigma_s = p->sigma_s;
-    d.sigma_a = p->sigma_a;
-    d.sigma_e = p->sigma_a + p->sigma_s;                 // msigmae = msigmaa + msigmas
-    d.albedo = p->sigma_s / (p->sigma_a + p->sigma_s);
-    d.scattevs = p->scattevs;
-    for (int k = 0; k < 3; ++k) {
-        d.sun_dir[k] = p->sun_dir[k];
-        d.sun_color[k] = p->sun_color[k];
-    }
-    d.sun_cos = std::cos(p->sun_angle);                  // SunLight ctor: cosf(angle)
-    const float ctm = d.sun_cos;
-    d.sun_pdf = 1.0f / ((2.0f * 3.14159265358979f) * (1.0f - ctm * ctm));  // SunLight::Pdf
-    for (int i = 0; i < 3; ++i) {
-        for (int j = 0; j < 9; ++j) d.sky_cfg[i][j] = (float)p->sky_configs[i][j];
-        d.sky_rad[i] = (float)p->sky_radiances[i];
-    }
-    d.mie_n = p->mie_n;
-    d.phase_mode = p->phase_mode;
-    std::memcpy(d.viewi, p->viewi, sizeof(d.viewi));
-    std::memcpy(d.proji, p->proji, sizeof(d.proji));
-    d.w = p->w;
-    d.h = p->h;
-    d.depthcomp = (p->flags & DR_KERNEL_DEPTHCOMP) ? 1u : 0u;
-    {
-        // RenderKernel::Shadow: zfar = (0,0,1,1) * projInv, clip_end = -zfar.z / zfar.w
-        const float zz = p->proji[8 + 2] + p->proji[12 + 2], zw = p->proji[8 + 3] + p->proji[12 + 3];
-        d.clip_end = -zz / zw;
-    }
-    const size_t n_ex = p->phase_mode == DR_PHASE_MIE_EXACT ? 8 * (size_t)p->mie_n + 4 : 0;
-    std::vector<unsigned char> pack((size_t)p->mie_n * 20 + 4 * n_ex);
-    for (uint32_t i = 0; i < p->mie_n; ++i) {
-        float4 v = make_float4(p->mie_pdf[3 * i], p->mie_pdf[3 * i + 1], p->mie_pdf[3 * i + 2], 0.0f);
-        std::memcpy(&pack[16 * (size_t)i], &v, 16);
-        std::memcpy(&pack[16 * (size_t)p->mie_n + 4 * (size_t)i], &p->mie_cdf[3 * i], 4);
-    }
-    if (n_ex) {
-        std::vector<float> ex(n_ex);
-        mie_exact_table(p->mie_pdf, p->mie_n, ex.data());
-        std::memcpy(&pack[20 * (size_t)p->mie_n], ex.data(), 4 * n_ex);
-    }
+    DevParams d;
+    std::vector<unsigned char> pack;
+    int rc = prepare_params(p, d, pack);
+    if (rc != DR_OK) return rc;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     DR_CUDA(cudaStreamSynchronize(c->stream), "dr_set_params: sync");
@@ -427,40 +144,25 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
         DR_CUDA(cudaMemcpy(c->depth.p, p->depth, sizeof(float) * p->w * p->h, cudaMemcpyHostToDevice),
                 "dr_set_params: copy depth");
         d.depth = c->depth.p;
-    } else {
-        d.depth = nullptr;
     }
-    d.mie_pdf = nullptr;
-    d.mie_cdf = nullptr;
-    d.mie_exact = nullptr;
     c->params = d;
     c->has_params = true;
     return DR_OK;
 }
 
 static int tile_args(const dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
-                     uint64_t base, TileArgs &A) {
+                     uint64_t base, uint32_t tile, TileArgs &A) {
     if (!c->has_scene || !c->has_params)
         return need(false, DR_ERR_STATE, "render: upload a scene and set parameters first");
-    if (tw == 0 || th == 0) return need(false, DR_ERR_INVALID, "render: empty tile");
-    A.x0 = x0;
-    A.y0 = y0;
-    A.tw = tw;
-    A.th = th;
-    A.cols = 2 * (tw / 2);
-    A.rows = 2 * (th / 2);
-    A.spp = spp;
-    A.seed = seed;
-    A.sample_base = base;
-    A.n_paths = (uint64_t)A.cols * A.rows * spp;
-    return DR_OK;
+    return make_tile_args(x0, y0, tw, th, spp, seed, base, tile, A);
 }
 
 int dr_render_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                          uint64_t sample_base, float *sun_dev, float *sky_dev, void *stream) {
     if (!c || !sun_dev || !sky_dev) return need(false, DR_ERR_INVALID, "dr_render_tile_async: null argument");
     TileArgs A;
-    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, A);
+    const uint32_t tile = c->tuning.kernel == DR_KERNEL_PER_PATH ? 0u : c->tuning.tile;
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, tile, A);
     if (rc != DR_OK) return rc;
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
@@ -483,7 +185,7 @@ int dr_shadow_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint3
                          uint64_t sample_base, float *out_dev, void *stream) {
     if (!c || !out_dev) return need(false, DR_ERR_INVALID, "dr_shadow_tile_async: null argument");
     TileArgs A;
-    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, A);
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, 0u, A);
     if (rc != DR_OK) return rc;
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
@@ -509,14 +211,15 @@ int dr_shadow_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
 
 int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
     if (!c || !t) return need(false, DR_ERR_INVALID, "dr_set_tuning: null argument");
-    if (t->kernel > DR_KERNEL_PER_PATH || t->event_batch > 32 || t->blocks_per_sm > 64 || t->traversal > 1)
+    if (!valid_tuning(t))
         return need(false, DR_ERR_INVALID,
-                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1");
+                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1, tile <= 64");
     c->tuning.kernel = t->kernel;
     c->tuning.block = kPersistentBlock;
     c->tuning.blocks_per_sm = t->blocks_per_sm;
     c->tuning.event_batch = t->event_batch;
     c->tuning.traversal = t->traversal;
+    c->tuning.tile = t->tile;
     return DR_OK;
 }
 
@@ -526,6 +229,7 @@ int dr_get_tuning(dr_ctx *c, dr_tuning *t) {
     t->blocks_per_sm = c->tuning.blocks_per_sm;
     t->event_batch = c->tuning.event_batch;
     t->traversal = c->tuning.traversal;
+    t->tile = c->tuning.tile;
     return DR_OK;
 }
 

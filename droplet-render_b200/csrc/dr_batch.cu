@@ -1,0 +1,280 @@
+// Batched rendering: many scenes and views in one persistent launch, replayed
+// from a CUDA graph (declared in include/droplet_b200.h, dr_batch_*).
+//
+// The reference renders one tile of one view per RenderKernel::Render call
+// (src/kernel.cpp:536-567).  A batch uploads every scene once, lays the paths
+// of all views out as one index space (view-major; inside a view, pixels in
+// the tuned order with consecutive samples), and captures
+//   memset(outputs) -> persistent kernel over all views -> step counter += 1
+// as a graph.  Launch k of a batch renders samples [k spp, (k+1) spp) of every
+// view, the same streams dr_render_tile draws with sample_base = k spp.
+#include <cstring>
+#include <memory>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/droplet_b200.h"
+#include "dr_host.h"
+#include "dr_kernels.h"
+
+using namespace dr;
+
+struct dr_batch {
+    dr_ctx *ctx = nullptr;
+    cudaStream_t stream = nullptr;  // capture stream
+    std::vector<std::unique_ptr<SceneBufs>> scene_bufs;
+    std::vector<std::unique_ptr<DevBuf<float>>> depth_bufs;
+    DevBuf<DevScene> scenes;
+    DevBuf<BatchView> views;
+    DevBuf<uint64_t> begins;
+    DevBuf<float4> out;
+    DevBuf<unsigned char> mie_pack;
+    DevBuf<WorkQueue> work;
+    DevBuf<unsigned long long> step;
+    std::vector<BatchView> host_views;
+    std::vector<size_t> out_off;  // float4 offset of view v's sun tile; its sky tile follows
+    size_t out_n = 0;             // float4 count of all outputs
+    DevParams p0{};
+    Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u};
+    uint64_t n_paths = 0, launches = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void drop_graph(dr_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// Lays the view's paths out for the current tile order and (re)captures the graph.
+int build_graph(dr_batch *b) {
+    drop_graph(b);
+    uint64_t begin = 0;
+    std::vector<uint64_t> begins(b->host_views.size());
+    for (size_t v = 0; v < b->host_views.size(); ++v) {
+        BatchView &V = b->host_views[v];
+        TileArgs A;
+        int rc = make_tile_args(V.A.x0, V.A.y0, V.A.tw, V.A.th, V.A.spp, V.A.seed, 0, b->tuning.tile, A);
+        if (rc != DR_OK) return rc;
+        V.A = A;
+        V.begin = begin;
+        begins[v] = begin;
+        begin += A.n_paths;
+    }
+    b->n_paths = begin;
+    DR_CUDA(cudaMemcpy(b->views.p, b->host_views.data(), sizeof(BatchView) * b->host_views.size(),
+                       cudaMemcpyHostToDevice),
+            "dr_batch: copy views");
+    DR_CUDA(cudaMemcpy(b->begins.p, begins.data(), sizeof(uint64_t) * begins.size(), cudaMemcpyHostToDevice),
+            "dr_batch: copy views");
+    BatchArgs B;
+    B.views = b->views.p;
+    B.scenes = b->scenes.p;
+    B.begins = b->begins.p;
+    B.n_views = (uint32_t)b->host_views.size();
+    B.n_paths = b->n_paths;
+    B.step = b->step.p;
+    DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");
+    cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
+    if (e == cudaSuccess)
+        e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning,
+                                b->ctx->device, b->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(e, "dr_batch: capture");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "dr_batch: end capture");
+    b->graph = g;
+    DR_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "dr_batch: instantiate graph");
+    return DR_OK;
+}
+
+void release(dr_batch *b) {
+    drop_graph(b);
+    for (auto &s : b->scene_bufs) s->release();
+    for (auto &d : b->depth_bufs) d->release();
+    b->scenes.release();
+    b->views.release();
+    b->begins.release();
+    b->out.release();
+    b->mie_pack.release();
+    b->work.release();
+    b->step.release();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    b->stream = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, const dr_batch_view *views,
+                    uint32_t n_views, dr_batch **out) {
+    if (out) *out = nullptr;
+    if (!c || !scenes || !views || !out || n_scenes == 0 || n_views == 0)
+        return need(false, DR_ERR_INVALID, "dr_batch_create: null argument or empty batch");
+    // Validate and convert everything on the host first.
+    std::vector<HostScene> hs(n_scenes);
+    for (uint32_t i = 0; i < n_scenes; ++i) {
+        int rc = prepare_scene(&scenes[i], hs[i]);
+        if (rc != DR_OK) return rc;
+    }
+    std::vector<BatchView> hv(n_views);
+    std::vector<unsigned char> pack0;
+    for (uint32_t v = 0; v < n_views; ++v) {
+        const dr_batch_view &bv = views[v];
+        if (bv.scene >= n_scenes) return need(false, DR_ERR_INVALID, "dr_batch_create: view scene index out of range");
+        if (!bv.params) return need(false, DR_ERR_INVALID, "dr_batch_create: view without parameters");
+        std::vector<unsigned char> pack;
+        int rc = prepare_params(bv.params, hv[v].P, pack);
+        if (rc != DR_OK) return rc;
+        if (v == 0) pack0 = pack;
+        else if (pack != pack0)
+            return need(false, DR_ERR_INVALID, "dr_batch_create: every view must use the same phase tables and mode");
+        TileArgs A;
+        rc = make_tile_args(bv.x0, bv.y0, bv.tw, bv.th, bv.spp, bv.seed, 0, 0, A);
+        if (rc != DR_OK) return rc;
+        hv[v].A = A;
+        hv[v].scene = bv.scene;
+    }
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    std::unique_ptr<dr_batch> b(new dr_batch());
+    b->ctx = c;
+    b->tuning = c->tuning;
+    b->tuning.kernel = DR_KERNEL_PERSISTENT;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "dr_batch_create: stream");
+    int rc = DR_OK;
+    auto fail = [&](int code) {
+        release(b.get());
+        return code;
+    };
+    std::vector<DevScene> ds(n_scenes);
+    for (uint32_t i = 0; i < n_scenes; ++i) {
+        b->scene_bufs.emplace_back(new SceneBufs());
+        rc = upload_scene(hs[i], *b->scene_bufs.back(), c->use_grid, b->stream, ds[i]);
+        if (rc != DR_OK) return fail(rc);
+    }
+    size_t total = 0;
+    b->out_off.resize(n_views);
+    for (uint32_t v = 0; v < n_views; ++v) {
+        b->out_off[v] = total;
+        total += 2 * (size_t)hv[v].A.tw * hv[v].A.th;
+    }
+    b->out_n = total;
+#define BATCH_CUDA(call, what)                        \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return fail(cuda_fail(e_, what)); \
+    } while (0)
+    BATCH_CUDA(b->out.reserve(total), "dr_batch_create: alloc outputs");
+    for (uint32_t v = 0; v < n_views; ++v) {
+        hv[v].sun = b->out.p + b->out_off[v];
+        hv[v].sky = hv[v].sun + (size_t)hv[v].A.tw * hv[v].A.th;
+        const dr_render_params *p = views[v].params;
+        if (p->depth) {
+            b->depth_bufs.emplace_back(new DevBuf<float>());
+            DevBuf<float> &d = *b->depth_bufs.back();
+            BATCH_CUDA(d.reserve((size_t)p->w * p->h), "dr_batch_create: alloc depth");
+            BATCH_CUDA(cudaMemcpy(d.p, p->depth, sizeof(float) * p->w * p->h, cudaMemcpyHostToDevice),
+                       "dr_batch_create: copy depth");
+            hv[v].P.depth = d.p;
+        }
+    }
+    BATCH_CUDA(b->scenes.reserve(n_scenes), "dr_batch_create: alloc scenes");
+    BATCH_CUDA(cudaMemcpy(b->scenes.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice),
+               "dr_batch_create: copy scenes");
+    BATCH_CUDA(b->views.reserve(n_views), "dr_batch_create: alloc views");
+    BATCH_CUDA(b->begins.reserve(n_views), "dr_batch_create: alloc views");
+    BATCH_CUDA(b->mie_pack.reserve(pack0.size()), "dr_batch_create: alloc tables");
+    BATCH_CUDA(cudaMemcpy(b->mie_pack.p, pack0.data(), pack0.size(), cudaMemcpyHostToDevice),
+               "dr_batch_create: copy tables");
+    BATCH_CUDA(b->work.reserve(1), "dr_batch_create: alloc queue");
+    BATCH_CUDA(b->step.reserve(1), "dr_batch_create: alloc step");
+    BATCH_CUDA(cudaMemset(b->step.p, 0, sizeof(unsigned long long)), "dr_batch_create: clear step");
+#undef BATCH_CUDA
+    b->p0 = hv[0].P;
+    b->host_views = std::move(hv);
+    rc = build_graph(b.get());
+    if (rc != DR_OK) return fail(rc);
+    *out = b.release();
+    return DR_OK;
+}
+
+int dr_batch_destroy(dr_batch *b) {
+    if (!b) return DR_OK;
+    {
+        DeviceGuard g(b->ctx->device);
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        release(b);
+    }
+    delete b;
+    return DR_OK;
+}
+
+int dr_batch_set_tuning(dr_batch *b, const dr_tuning *t) {
+    if (!b || !valid_tuning(t)) return need(false, DR_ERR_INVALID, "dr_batch_set_tuning: bad argument");
+    if (t->kernel != DR_KERNEL_PERSISTENT)
+        return need(false, DR_ERR_INVALID, "dr_batch_set_tuning: a batch runs the persistent kernel");
+    DeviceGuard g(b->ctx->device);
+    DR_CUDA(cudaStreamSynchronize(b->stream), "dr_batch_set_tuning: sync");
+    b->tuning.kernel = DR_KERNEL_PERSISTENT;
+    b->tuning.blocks_per_sm = t->blocks_per_sm;
+    b->tuning.event_batch = t->event_batch;
+    b->tuning.traversal = t->traversal;
+    b->tuning.tile = t->tile;
+    return build_graph(b);
+}
+
+int dr_batch_get_tuning(dr_batch *b, dr_tuning *t) {
+    if (!b || !t) return need(false, DR_ERR_INVALID, "dr_batch_get_tuning: null argument");
+    t->kernel = DR_KERNEL_PERSISTENT;
+    t->blocks_per_sm = b->tuning.blocks_per_sm;
+    t->event_batch = b->tuning.event_batch;
+    t->traversal = b->tuning.traversal;
+    t->tile = b->tuning.tile;
+    return DR_OK;
+}
+
+int dr_batch_launch(dr_batch *b, void *stream) {
+    if (!b || !b->exec) return need(false, DR_ERR_INVALID, "dr_batch_launch: no batch");
+    DeviceGuard g(b->ctx->device);
+    DR_CUDA(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->ctx->stream), "dr_batch_launch");
+    ++b->launches;
+    return DR_OK;
+}
+
+int dr_batch_output(dr_batch *b, uint32_t view, float **sun_dev, float **sky_dev) {
+    if (!b || view >= b->host_views.size() || !sun_dev || !sky_dev)
+        return need(false, DR_ERR_INVALID, "dr_batch_output: bad argument");
+    *sun_dev = (float *)b->host_views[view].sun;
+    *sky_dev = (float *)b->host_views[view].sky;
+    return DR_OK;
+}
+
+int dr_batch_read(dr_batch *b, uint32_t view, float *sun_out, float *sky_out) {
+    if (!b || view >= b->host_views.size() || !sun_out || !sky_out)
+        return need(false, DR_ERR_INVALID, "dr_batch_read: bad argument");
+    DeviceGuard g(b->ctx->device);
+    const BatchView &V = b->host_views[view];
+    const size_t n = (size_t)V.A.tw * V.A.th;
+    DR_CUDA(cudaDeviceSynchronize(), "dr_batch_read: sync");
+    DR_CUDA(cudaMemcpy(sun_out, V.sun, n * sizeof(float4), cudaMemcpyDeviceToHost), "dr_batch_read: copy");
+    DR_CUDA(cudaMemcpy(sky_out, V.sky, n * sizeof(float4), cudaMemcpyDeviceToHost), "dr_batch_read: copy");
+    return DR_OK;
+}
+
+int dr_batch_info(dr_batch *b, uint64_t *n_paths, uint64_t *launches) {
+    if (!b) return need(false, DR_ERR_INVALID, "dr_batch_info: null batch");
+    if (n_paths) *n_paths = b->n_paths;
+    if (launches) *launches = b->launches;
+    return DR_OK;
+}
+
+}  // extern "C"

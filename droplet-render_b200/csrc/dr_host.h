@@ -1,0 +1,120 @@
+// Host-side helpers shared by the C-ABI entry points (dr_api.cu, dr_batch.cu):
+// error reporting, device buffers, and the validation + conversion of scenes
+// and render settings into their device layouts.
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/droplet_b200.h"
+#include "dr_internal.h"
+
+namespace dr {
+
+void set_error(int code, const std::string &msg);
+const char *last_error();
+int cuda_fail(cudaError_t e, const char *what);
+// Returns DR_OK when ok, else records msg and returns code.
+int need(bool ok, int code, const char *msg);
+
+#define DR_CUDA(call, what)                                  \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what);   \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t reserve(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, sizeof(T) * (count ? count : 1));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// A validated scene in its device layout, still on the host.
+struct HostScene {
+    std::vector<uint32_t> child;   // 8 per node (see DevScene)
+    std::vector<float4> leaf;      // 2 per node
+    std::vector<uint32_t> macro, cells;
+    std::vector<uint8_t> leaf_flag;
+    uint32_t levels = 0, n = 0, mdim = 0;
+    uint32_t n_nodes = 0, n_leaves = 0;
+    float root_ce[4] = {0, 0, 0, 0};
+    const float *bricks = nullptr;  // the caller's brick pool (n_leaves * 512 floats)
+};
+
+// Device buffers of one uploaded scene.
+struct SceneBufs {
+    DevBuf<uint4> child;
+    DevBuf<float4> leaf;
+    DevBuf<float> bricks;
+    DevBuf<uint32_t> macro, cells;
+    void release() {
+        child.release();
+        leaf.release();
+        bricks.release();
+        macro.release();
+        cells.release();
+    }
+};
+
+// Checks a scene descriptor (src/scene.h:21-31 records) and builds the device
+// layout: remapped child entries, leaf records, and the leaf grid of the cell walk.
+int prepare_scene(const dr_scene_desc *s, HostScene &out);
+// Copies a prepared scene into bufs (synchronously on st) and fills S.
+int upload_scene(const HostScene &h, SceneBufs &bufs, bool use_grid, cudaStream_t st, DevScene &S);
+// Checks render settings and converts them (the depth pointer is left null);
+// pack receives the phase tables as staged in shared memory.
+int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned char> &pack);
+// Shared-memory pack size of the phase tables for d.
+size_t mie_pack_bytes(const DevParams &d);
+// Tile arguments of a render call (tile > 0: square pixel order of the persistent kernel).
+int make_tile_args(uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed, uint64_t base,
+                   uint32_t tile, TileArgs &A);
+bool valid_tuning(const dr_tuning *t);
+
+}  // namespace dr
+
+// The context behind the C ABI's opaque dr_ctx handle.
+struct dr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    bool has_scene = false, has_params = false;
+    dr::DevScene scene{};
+    dr::DevParams params{};
+    dr::SceneBufs bufs;
+    dr::DevBuf<unsigned char> mie_pack;
+    dr::DevBuf<float> depth;
+    dr::DevBuf<dr::DevCounters> counters;
+    dr::DevBuf<float4> tile_sun, tile_sky;
+    dr::DevBuf<unsigned char> scratch;
+    dr::DevBuf<dr::WorkQueue> work;
+    bool use_grid = true;
+    dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u};
+    std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)
+};

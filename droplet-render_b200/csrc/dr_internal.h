@@ -64,8 +64,10 @@ struct TileArgs {
     uint32_t x0, y0, tw, th;
     uint32_t cols, rows;      // rendered extent: even parts of tw, th
     uint32_t spp;
+    uint32_t tile;            // persistent kernel: pixel order in tile x tile squares (0 = row-major)
+    uint32_t tiles_x;         // squares per row when tile > 0
     uint64_t seed, sample_base;
-    uint64_t n_paths;         // cols * rows * spp
+    uint64_t n_paths;         // path indices: cols * rows * spp (row-major) or squares * tile^2 * spp
 };
 
 struct DevCounters {
@@ -79,6 +81,29 @@ struct Tuning {
     uint32_t blocks_per_sm; // 0 = as many as fit
     uint32_t event_batch;   // lanes of a warp that must be waiting before events run
     uint32_t traversal;     // 0 = octree stack traversal, 1 = leaf-grid cell walk
+    uint32_t tile;          // pixel order of the persistent kernel: 0 = row-major, else square side
+};
+
+// One view of a batched launch: its parameters, tile and output, the scene it
+// renders and the first global path index it owns.
+struct BatchView {
+    DevParams P;
+    TileArgs A;
+    float4 *sun, *sky;
+    uint32_t scene;
+    uint32_t pad;
+    uint64_t begin;
+};
+
+// A batched launch: every view's paths form one index space [0, n_paths) in
+// view order; begins[v] = views[v].begin (binary-searched per fetched path).
+struct BatchArgs {
+    const BatchView *views;
+    const DevScene *scenes;
+    const uint64_t *begins;
+    uint32_t n_views;
+    uint64_t n_paths;
+    const unsigned long long *step;  // launches so far: view samples start at sample_base + step * spp
 };
 
 // Work queue of the persistent kernel: next path index to hand out.

@@ -423,15 +423,28 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
 }
 
 // Starts path number p; returns false when p lies outside the frame (no work).
+// Path index p -> (pixel, sample): samples of a pixel are consecutive; pixels
+// run row-major, or square by square (tile x tile, row-major inside) when
+// A.tile > 0, where indices of pixels past the tile's edge carry no work.
 template <bool WALK>
 __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const DevScene &S, const DevParams &P,
-                                           const TileArgs &A, Count &cnt, uint32_t &paths, uint32_t &state,
-                                           Trav *slow) {
+                                           const TileArgs &A, uint64_t shift, Count &cnt, uint32_t &paths,
+                                           uint32_t &state, Trav *slow) {
     const uint64_t pl = p / A.spp;
     const uint32_t s = (uint32_t)(p - pl * A.spp);
     const uint32_t pix = (uint32_t)pl;
-    L.px = A.x0 + pix % A.cols;
-    L.py = A.y0 + pix / A.cols;
+    uint32_t ix, iy;
+    if (A.tile) {
+        const uint32_t t2 = A.tile * A.tile, sq = pix / t2, r = pix - sq * t2;
+        ix = (sq % A.tiles_x) * A.tile + r % A.tile;
+        iy = (sq / A.tiles_x) * A.tile + r / A.tile;
+        if (ix >= A.cols || iy >= A.rows) return false;
+    } else {
+        ix = pix % A.cols;
+        iy = pix / A.cols;
+    }
+    L.px = A.x0 + ix;
+    L.py = A.y0 + iy;
     if (!camera_ray(P, L.px, L.py, L.ro, L.rd)) return false;
     ++paths;
     L.T[0] = L.T[1] = L.T[2] = 1.0f;
@@ -443,25 +456,78 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     begin_segment(L, S, cnt, state, slow);
     // A camera ray that misses the root box draws no random number: its
     // sample is exactly zero.  Seed the stream only for rays that enter.
-    if (L.wmode != 0u) L.g = rng_seed(A.seed, (uint64_t)L.py * P.w + L.px, A.sample_base + s);
+    if (L.wmode != 0u) L.g = rng_seed(A.seed, (uint64_t)L.py * P.w + L.px, A.sample_base + shift + s);
     return true;
 }
 
-template <int MINB, bool WALK>
+// One loop iteration of a lane that holds a path (see render_persistent_kernel).
+template <bool WALK>
+__device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
+                                          const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
+                                          Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow) {
+    if (events) {
+        if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
+        return;
+    }
+    if (state == kTrav) {
+        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt);
+        if (r == 1u) {
+            state = kStep;
+        } else if (r == 2u) {
+            L.esc = kTrackEscaped;
+            state = kEvent;
+        }
+    }
+    if (state == kStep) {
+        const uint32_t rs = track_step(L, cnt);
+        if (rs == 1) state = kTrav;
+        else if (rs == 2) state = kEvent;
+    }
+}
+
+// View owning global path index p: the last v with begins[v] <= p.
+__device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
+    uint32_t lo = 0, hi = B.n_views - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&B.begins[mid]) <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// BATCH: the paths of many views (each with its own scene, parameters, tile
+// and output) share one work queue; a lane looks its view up when it fetches
+// a path and reads that view's records from global memory (L1-resident).
+template <int MINB, bool WALK, bool BATCH>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
                                                                             float4 *sky_out, DevCounters *C,
-                                                                            WorkQueue *Q, uint32_t event_batch) {
+                                                                            WorkQueue *Q, uint32_t event_batch,
+                                                                            BatchArgs B) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
-    const MieSmem M = mie_view(P, smem);
+    uint32_t mb;
+    MieSmem M;
+    uint64_t n_total, shift = 0;
+    if constexpr (BATCH) {
+        mb = mie_bytes(B.views[0].P);
+        M = mie_view(B.views[0].P, smem);
+        n_total = B.n_paths;
+        shift = *B.step;
+    } else {
+        mb = mie_bytes(P);
+        M = mie_view(P, smem);
+        n_total = A.n_paths;
+    }
+    const bool staged = stage_mie(mie_pack, mb, smem, &mbar);
     Count cnt;
     cnt.zero();
     uint32_t paths = 0;
     uint32_t nstack[kMaxDepth];
-    Trav slow[WALK ? 1 : 1];
+    Trav slow[1];
     PathLane<WALK> L;
+    uint32_t view = 0;
     uint32_t state = staged ? kFetch : kDone;
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
     const uint32_t lane = threadIdx.x & 31u;
@@ -476,34 +542,38 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
             base = __shfl_sync(FULL, base, leader);
             if (state == kFetch) {
                 const uint64_t p = base + __popc(want & lt_mask);
-                if (p >= A.n_paths) state = kDone;
-                else if (!start_path(L, p, S, P, A, cnt, paths, state, slow)) state = kFetch;
+                if (p >= n_total) {
+                    state = kDone;
+                } else {
+                    bool ok;
+                    if constexpr (BATCH) {
+                        view = find_view(B, p);
+                        const BatchView &V = B.views[view];
+                        ok = start_path(L, p - V.begin, B.scenes[V.scene], V.P, V.A, shift * V.A.spp, cnt, paths,
+                                        state, slow);
+                    } else {
+                        ok = start_path(L, p, S, P, A, 0ull, cnt, paths, state, slow);
+                    }
+                    if (!ok) state = kFetch;
+                }
             }
         }
         if (__all_sync(FULL, state == kDone)) break;
         const uint32_t ev = __ballot_sync(FULL, state == kEvent);
         const uint32_t busy = __ballot_sync(FULL, state == kTrav || state == kStep);
-        if (ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0)) {
-            if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
-            continue;
-        }
-        if (state == kTrav) {
-            const uint32_t r = trav_step(L, S, P, nstack, slow, cnt);
-            if (r == 1u) {
-                state = kStep;
-            } else if (r == 2u) {
-                L.esc = kTrackEscaped;
-                state = kEvent;
-            }
-        }
-        if (state == kStep) {
-            const uint32_t rs = track_step(L, cnt);
-            if (rs == 1) state = kTrav;
-            else if (rs == 2) state = kEvent;
+        const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
+        if constexpr (BATCH) {
+            const BatchView &V = B.views[view];
+            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow);
+        } else {
+            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow);
         }
     }
     warp_sum_counts(cnt, C, paths);
 }
+
+// Advances the launch counter of a batch (the last node of its graph).
+__global__ void batch_step_kernel(unsigned long long *step) { *step += 1ull; }
 
 // ---- parity probes ------------------------------------------------------------
 __global__ void probe_leaf_kernel(DevScene S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
@@ -712,47 +782,88 @@ cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const Tile
 }
 
 // Variants of the persistent kernel compiled for 4, 5, 6 and 8 resident
-// blocks per SM (fewer registers, some spilled to L1-resident local memory).
+// blocks per SM (fewer registers, some spilled to L1-resident local memory),
+// each with the stack traversal or the cell walk, single frame or batch.
 using PersistentFn = void (*)(DevScene, DevParams, TileArgs, const void *, float4 *, float4 *, DevCounters *,
-                              WorkQueue *, uint32_t);
-static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal) {
+                              WorkQueue *, uint32_t, BatchArgs);
+template <bool BATCH>
+static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
     if (traversal == 1u) {
-        if (minb >= 8) return render_persistent_kernel<8, true>;
-        if (minb >= 6) return render_persistent_kernel<6, true>;
-        if (minb >= 5) return render_persistent_kernel<5, true>;
-        return render_persistent_kernel<4, true>;
+        if (minb >= 8) return render_persistent_kernel<8, true, BATCH>;
+        if (minb >= 6) return render_persistent_kernel<6, true, BATCH>;
+        if (minb >= 5) return render_persistent_kernel<5, true, BATCH>;
+        return render_persistent_kernel<4, true, BATCH>;
     }
-    if (minb >= 8) return render_persistent_kernel<8, false>;
-    if (minb >= 6) return render_persistent_kernel<6, false>;
-    if (minb >= 5) return render_persistent_kernel<5, false>;
-    return render_persistent_kernel<4, false>;
+    if (minb >= 8) return render_persistent_kernel<8, false, BATCH>;
+    if (minb >= 6) return render_persistent_kernel<6, false, BATCH>;
+    if (minb >= 5) return render_persistent_kernel<5, false, BATCH>;
+    return render_persistent_kernel<4, false, BATCH>;
+}
+
+static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch) {
+    return batch ? persistent_variant_of<true>(minb, traversal) : persistent_variant_of<false>(minb, traversal);
 }
 
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persistent_variant(variant, traversal), kPersistentBlock,
-                                                      smem_bytes) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persistent_variant(variant, traversal, false),
+                                                      kPersistentBlock, smem_bytes) != cudaSuccess)
         return 1;
     return nb > 0 ? nb : 1;
+}
+
+// Grid of the persistent kernel: SMs x resident blocks (the tuned count, capped
+// by what fits).
+static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, bool batch, PersistentFn &fn,
+                                   int &blocks, uint32_t &event_batch) {
+    int sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
+    fn = persistent_variant(variant, tune.traversal, batch);
+    int maxb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, kPersistentBlock, smem) != cudaSuccess || maxb < 1)
+        maxb = 1;
+    const int bps = tune.blocks_per_sm && (int)tune.blocks_per_sm < maxb ? (int)tune.blocks_per_sm : maxb;
+    blocks = sms * bps;
+    event_batch = tune.event_batch ? (tune.event_batch > 32 ? 32u : tune.event_batch) : 8u;
+    return cudaSuccess;
 }
 
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
                                      const Tuning &tune, int device, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
-    int sms = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
     const size_t smem = mie_smem(P);
-    const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
-    const int maxb = persistent_max_blocks_per_sm(variant, tune.traversal, smem);
-    const int bps = tune.blocks_per_sm && (int)tune.blocks_per_sm < maxb ? (int)tune.blocks_per_sm : maxb;
+    PersistentFn fn;
+    int blocks;
+    uint32_t batch;
+    cudaError_t e = persistent_grid(tune, device, smem, false, fn, blocks, batch);
+    if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
-    const uint32_t batch = tune.event_batch ? (tune.event_batch > 32 ? 32u : tune.event_batch) : 8u;
-    persistent_variant(variant, tune.traversal)<<<sms * bps, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q,
-                                                                          batch);
+    fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q, batch, BatchArgs{});
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, int device,
+                                cudaStream_t st) {
+    const size_t smem = mie_smem(P0);
+    PersistentFn fn;
+    int blocks;
+    uint32_t batch;
+    cudaError_t e = persistent_grid(tune, device, smem, true, fn, blocks, batch);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
+    if (e != cudaSuccess) return e;
+    if (B.n_paths) {
+        fn<<<blocks, kPersistentBlock, smem, st>>>(DevScene{}, DevParams{}, TileArgs{}, mie_pack, nullptr, nullptr, C,
+                                                   Q, batch, B);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    batch_step_kernel<<<1, 1, 0, st>>>(step);
     return cudaGetLastError();
 }
 

@@ -16,6 +16,12 @@ cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const Tile
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
                                      const Tuning &tune, int device, cudaStream_t st);
+// Batched persistent launch over all views of B (P0: the first view's parameters,
+// which fix the shared phase tables), then one increment of *step; Q->next is
+// cleared on st first.  The three launches are what a batch's graph captures.
+cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, int device,
+                                cudaStream_t st);
 // Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,

@@ -108,7 +108,12 @@ class DrCounters(C.Structure):
 
 class DrTuning(C.Structure):
     _fields_ = [("kernel", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("event_batch", C.c_uint32),
-                ("traversal", C.c_uint32)]
+                ("traversal", C.c_uint32), ("tile", C.c_uint32)]
+
+
+class DrBatchView(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("params", C.c_void_p), ("x0", C.c_uint32), ("y0", C.c_uint32),
+                ("tw", C.c_uint32), ("th", C.c_uint32), ("spp", C.c_uint32), ("seed", C.c_uint64)]
 
 
 # name -> (restype, argtypes); every symbol the header declares
@@ -149,6 +154,15 @@ SIGNATURES = {
          C.c_void_p],
     ),
     "dr_synchronize": (C.c_int, [C.c_void_p]),
+    "dr_batch_create": (
+        C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "dr_batch_destroy": (C.c_int, [C.c_void_p]),
+    "dr_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
+    "dr_batch_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
+    "dr_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dr_batch_output": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "dr_batch_read": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "dr_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "dr_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
     "dr_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
     "dr_get_counters": (C.c_int, [C.c_void_p, C.POINTER(DrCounters)]),

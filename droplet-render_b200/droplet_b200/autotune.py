@@ -1,18 +1,19 @@
-"""Launch-shape autotuner for the persistent path kernel.
+"""Launch-shape autotuner for the persistent path kernel (single frames and batches).
 
-The persistent kernel has four knobs (`dr_tuning`):
+The persistent kernel has five knobs (`dr_tuning`):
 * the compiled variant, i.e. resident blocks per SM. 4/5/6/8 trade registers for
   occupancy; the smaller register budgets spill a little to L1-resident local memory.
 * the event batch: how many lanes of a warp must be waiting on a segment end before
   the warp shades them.
-* the kernel family (persistent, or one thread per path).
 * the traversal: octree descent with a node stack, or the cell walk over the leaf
   grid (faster where leaves are dense along rays, slower through wide empty regions).
+* the tile: pixels handed out row-major or square by square (ray coherence).
+* the kernel family (persistent, or one thread per path; single frames only).
 
-`tune` renders a representative region with every candidate, times each with CUDA
-events on a dedicated stream, and keeps the fastest. Results are cached per (GPU
-name, workload key) in a small JSON file, so a later run with the same key skips
-the search.
+`tune` searches in two stages: occupancy x event batch first, then traversal x tile
+around the best; each candidate is timed with CUDA events on a dedicated stream.
+Results are cached per (GPU name, workload key) in a small JSON file, so a later run
+with the same key skips the search.
 """
 from __future__ import annotations
 
@@ -22,12 +23,15 @@ import time
 
 from . import _native as N
 
-DEFAULT_CANDIDATES = [
-    (0, bps, batch, trav)
-    for trav in (0, 1)
-    for bps in (4, 5, 6, 8)
-    for batch in (4, 8, 16, 24)
-] + [(1, 0, 0, 0)]
+STAGE1 = [(0, bps, batch, 0, 0) for bps in (4, 5, 6, 8) for batch in (8, 16, 24)]
+PER_PATH = (1, 0, 0, 0, 0)
+
+
+def stage2(best):
+    k, bps, batch, _, _ = best
+    out = [(k, bps, batch, trav, tile) for trav in (0, 1) for tile in (0, 8, 16)]
+    out += [(k, bps, b2, 0, 0) for b2 in (12, 20, 28, 32) if b2 != batch]
+    return out
 
 
 def _cache_path() -> str:
@@ -67,33 +71,88 @@ def time_region(renderer, region, spp: int, seed: int, repeats: int, stream, sun
     return a.elapsed_time(b) / repeats
 
 
-def tune(renderer, region, spp: int, key: str, candidates=None, repeats: int = 2, seed: int = 7,
-         use_cache: bool = True):
-    """Picks the fastest (kernel, blocks_per_sm, event_batch, traversal) for the region and
-    leaves it set on the renderer.  Returns (best, table of (candidate, ms))."""
+def time_batch(batch, repeats: int, stream) -> float:
+    """Milliseconds per graph launch of a batch with its current tuning."""
     import torch
 
-    gpu = torch.cuda.get_device_name(renderer.device)
+    batch.launch(stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(repeats):
+        batch.launch(stream.cuda_stream)
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / repeats
+
+
+def search(target, timer, per_path: bool = True):
+    """Two-stage search over target.set_tuning(*candidate); returns (best, table)."""
+    table = []
+    seen = set()
+
+    def run(cands):
+        for c in cands:
+            if c in seen:
+                continue
+            seen.add(c)
+            target.set_tuning(*c)
+            table.append((list(c), timer()))
+
+    run(STAGE1 + ([PER_PATH] if per_path else []))
+    best = tuple(min(table, key=lambda r: r[1])[0])
+    if best[0] == 0:
+        run(stage2(best))
+    table.sort(key=lambda r: r[1])
+    return tuple(table[0][0]), table
+
+
+def _cached(key, target, use_cache):
+    import torch
+
+    gpu = torch.cuda.get_device_name(getattr(target, "device", 0))
     ckey = f"{gpu}|{key}"
     cache = _load_cache() if use_cache else {}
     if use_cache and ckey in cache:
         best = tuple(cache[ckey]["best"])
-        renderer.set_tuning(*best)
-        return best, cache[ckey]["table"]
+        target.set_tuning(*best)
+        return ckey, cache, (best, cache[ckey]["table"])
+    return ckey, cache, None
+
+
+def tune(renderer, region, spp: int, key: str, repeats: int = 2, seed: int = 7, use_cache: bool = True):
+    """Picks the fastest launch shape for rendering `region` at `spp` and leaves it
+    set on the renderer.  Returns (best, table of (candidate, ms))."""
+    import torch
+
+    ckey, cache, hit = _cached(key, renderer, use_cache)
+    if hit:
+        return hit
     x0, y0, w, h = region
     sun = torch.empty((h, w, 4), dtype=torch.float32, device=f"cuda:{renderer.device}")
     sky = torch.empty_like(sun)
     stream = torch.cuda.Stream(device=renderer.device)
-    saved = renderer.get_tuning()
-    table = []
     t0 = time.time()
-    for cand in candidates or DEFAULT_CANDIDATES:
-        renderer.set_tuning(*cand)
-        ms = time_region(renderer, region, spp, seed, repeats, stream, sun, sky)
-        table.append((list(cand), ms))
-    table.sort(key=lambda r: r[1])
-    best = tuple(table[0][0]) if table else saved
+    best, table = search(renderer, lambda: time_region(renderer, region, spp, seed, repeats, stream, sun, sky))
     renderer.set_tuning(*best)
+    if use_cache:
+        cache[ckey] = {"best": list(best), "table": table, "seconds": time.time() - t0}
+        _store_cache(cache)
+    return best, table
+
+
+def tune_batch(batch, key: str, repeats: int = 2, use_cache: bool = True):
+    """tune() for a Batch: times whole graph launches of `batch` (normally a
+    reduced probe batch of the same scenes and views) and leaves the best set."""
+    import torch
+
+    ckey, cache, hit = _cached(key, batch.renderer, use_cache)
+    if hit:
+        batch.set_tuning(*hit[0])
+        return hit
+    stream = torch.cuda.Stream(device=batch.renderer.device)
+    t0 = time.time()
+    best, table = search(batch, lambda: time_batch(batch, repeats, stream), per_path=False)
+    batch.set_tuning(*best)
     if use_cache:
         cache[ckey] = {"best": list(best), "table": table, "seconds": time.time() - t0}
         _store_cache(cache)

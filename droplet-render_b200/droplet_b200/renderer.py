@@ -158,14 +158,15 @@ class Renderer:
     def synchronize(self):
         N.check(N.lib().dr_synchronize(self._ctx))
 
-    def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0):
-        t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal))
+    def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
+                   tile: int = 0):
+        t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal), int(tile))
         N.check(N.lib().dr_set_tuning(self._ctx, C.byref(t)))
 
     def get_tuning(self):
         t = N.DrTuning()
         N.check(N.lib().dr_get_tuning(self._ctx, C.byref(t)))
-        return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal))
+        return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal), int(t.tile))
 
     def counters(self) -> dict:
         c = N.DrCounters()
@@ -221,3 +222,83 @@ class Renderer:
         N.check(N.lib().dr_probe_transmittance(self._ctx, ro.ctypes.data, rd.ctypes.data, len(ro), int(nsamp),
                                                int(seed), out.ctypes.data))
         return out
+
+
+@dataclass
+class BatchView:
+    """One view of a batch: scene index, settings, region, samples per launch, seed."""
+    scene: int
+    settings: RenderSettings
+    spp: int
+    seed: int = 0
+    region: tuple | None = None   # (x0, y0, tw, th); None = the whole image
+
+
+class Batch:
+    """Many scenes and views rendered by one persistent launch replayed from a CUDA
+    graph (dr_batch_*).  Launch k renders samples [k spp, (k+1) spp) of each view,
+    the streams Renderer.render_tile draws with sample_base = k spp."""
+
+    def __init__(self, renderer: "Renderer", scenes: list, views: list):
+        descs = (N.DrSceneDesc * len(scenes))()
+        self._keep = []
+        for i, oc in enumerate(scenes):
+            nodes = np.ascontiguousarray(oc.nodes)
+            bricks = np.ascontiguousarray(oc.bricks, np.float32)
+            self._keep += [nodes, bricks]
+            descs[i] = N.DrSceneDesc(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+        bv = (N.DrBatchView * len(views))()
+        params = []
+        self.views = list(views)
+        for i, v in enumerate(views):
+            p = v.settings.to_c()
+            params.append(p)
+            x0, y0, tw, th = v.region if v.region is not None else (0, 0, v.settings.w, v.settings.h)
+            bv[i] = N.DrBatchView(int(v.scene), C.cast(C.pointer(p), C.c_void_p), x0, y0, tw, th, int(v.spp),
+                                  int(v.seed))
+        self.regions = [v.region if v.region is not None else (0, 0, v.settings.w, v.settings.h) for v in views]
+        self._h = C.c_void_p()
+        self.renderer = renderer
+        N.check(N.lib().dr_batch_create(renderer.handle, descs, len(scenes), bv, len(views), C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            N.lib().dr_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
+                   tile: int = 0):
+        t = N.DrTuning(0, int(blocks_per_sm), int(event_batch), int(traversal), int(tile))
+        N.check(N.lib().dr_batch_set_tuning(self._h, C.byref(t)))
+
+    def get_tuning(self):
+        t = N.DrTuning()
+        N.check(N.lib().dr_batch_get_tuning(self._h, C.byref(t)))
+        return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal), int(t.tile))
+
+    def launch(self, stream_ptr: int = 0):
+        N.check(N.lib().dr_batch_launch(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def output_ptrs(self, view: int):
+        a, b = C.c_void_p(), C.c_void_p()
+        N.check(N.lib().dr_batch_output(self._h, int(view), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def read(self, view: int):
+        """(sun, sky) sums of the last launch for one view, shape (th, tw, 4)."""
+        _, _, tw, th = self.regions[view]
+        sun = np.zeros((th, tw, 4), np.float32)
+        sky = np.zeros((th, tw, 4), np.float32)
+        N.check(N.lib().dr_batch_read(self._h, int(view), sun.ctypes.data, sky.ctypes.data))
+        return sun, sky
+
+    def info(self):
+        n, k = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().dr_batch_info(self._h, C.byref(n), C.byref(k)))
+        return int(n.value), int(k.value)

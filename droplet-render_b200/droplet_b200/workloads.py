@@ -119,14 +119,43 @@ MEDIA = {
     "c0": {"sigma_t": 20.0, "albedo": 0.99, "scattevs": 8},
     "c1": {"sigma_t": 60.0, "albedo": 0.999, "scattevs": 64},
 }
+# The batched workload's fields take their own sigma_t; albedo as config 0 and
+# the reference UI's default of 500 scattering events.
+C2_ALBEDO, C2_SCATTEVS = 0.99, 500
 
 
 def medium(name: str):
     """(sigma_s, sigma_a, scattevs) in binary32 for a named configuration."""
     m = MEDIA[name]
-    st = np.float32(m["sigma_t"])
-    ss = np.float32(m["sigma_t"] * m["albedo"])
-    return float(ss), float(np.float32(st - ss)), int(m["scattevs"])
+    return medium_of(m["sigma_t"], m["albedo"], m["scattevs"])
+
+
+def medium_of(sigma_t: float, albedo: float, scattevs: int):
+    st = np.float32(sigma_t)
+    ss = np.float32(sigma_t * albedo)
+    return float(ss), float(np.float32(st - ss)), int(scattevs)
+
+
+def c2_batch(seed: int = 2026):
+    """The batched workload (8 fields x 8 views), drawn with default_rng(seed).
+
+    Fields: the config-0 puff recipe at seeds 10-17, grid edge from
+    {64, 128, 256, 512}, sigma_t uniform in [10, 80].  Views: 8 per field at
+    uniform random azimuths (camera 2.5 units from the centre, 10 degrees up,
+    40 degree field of view), square images with an even side uniform in
+    [128, 1024], spp from {16, 64, 256}, and the sun (azimuth 30) at a whole
+    degree of elevation uniform in [5, 80] (the sky states are cooked per
+    degree).  Returns (fields, views) as lists of dicts."""
+    rng = np.random.default_rng(seed)
+    fields = [{"seed": 10 + i, "n": int(rng.choice([64, 128, 256, 512])),
+               "sigma_t": float(rng.uniform(10.0, 80.0))} for i in range(8)]
+    views = []
+    for f in range(8):
+        for _ in range(8):
+            views.append({"field": f, "azimuth": float(rng.uniform(0.0, 360.0)),
+                          "side": 2 * int(rng.integers(64, 513)), "spp": int(rng.choice([16, 64, 256])),
+                          "sun_elevation": int(rng.integers(5, 81))})
+    return fields, views
 
 
 def eval_blocks_numpy(recipe: FieldRecipe, block_origins: np.ndarray, chunk: int = 2048) -> np.ndarray:

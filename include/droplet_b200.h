@@ -171,11 +171,44 @@ typedef struct {
     uint32_t blocks_per_sm;  /* persistent kernel: resident blocks per SM, 0 = as many as fit */
     uint32_t event_batch;    /* persistent kernel: waiting lanes before a warp shades (1..32, 0 = 8) */
     uint32_t traversal;      /* persistent kernel: DR_TRAVERSAL_* */
+    uint32_t tile;           /* persistent kernel: pixel order in tile x tile squares, 0 = row-major (<= 64) */
 } dr_tuning;
 #define DR_TRAVERSAL_STACK 0u  /* octree descent with a node stack (the reference's order) */
 #define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */
 int dr_set_tuning(dr_ctx *ctx, const dr_tuning *tuning);
 int dr_get_tuning(dr_ctx *ctx, dr_tuning *tuning);
+
+/* ---- batched rendering (no reference counterpart: the reference renders one
+ * tile of one view per RenderKernel::Render call, src/kernel.cpp:536-567) ----
+ * A batch holds several scenes and views and renders every view's spp new
+ * samples in ONE persistent launch replayed from a CUDA graph.  Launch k of a
+ * batch renders, for each view, the samples dr_render_tile would render with
+ * sample_base = k * spp; outputs hold the sums of the last launch. */
+typedef struct dr_batch dr_batch;
+typedef struct {
+    uint32_t scene;                  /* index into the scenes given to dr_batch_create */
+    const dr_render_params *params;  /* settings of this view; phase tables and mode equal across views */
+    uint32_t x0, y0, tw, th;         /* region of the view's image */
+    uint32_t spp;                    /* samples per pixel per launch */
+    uint64_t seed;                   /* path streams (seed, pixel, sample) as in dr_render_tile */
+} dr_batch_view;
+/* Uploads every scene, copies every view's settings (and depth texture) and
+ * captures the launch graph with the context's tuning (kernel forced to
+ * DR_KERNEL_PERSISTENT).  Counters accumulate into the context's. */
+int dr_batch_create(dr_ctx *ctx, const dr_scene_desc *scenes, uint32_t n_scenes, const dr_batch_view *views,
+                    uint32_t n_views, dr_batch **out);
+int dr_batch_destroy(dr_batch *batch);
+/* Re-lays the views out and recaptures the graph for another launch shape. */
+int dr_batch_set_tuning(dr_batch *batch, const dr_tuning *tuning);
+int dr_batch_get_tuning(dr_batch *batch, dr_tuning *tuning);
+/* Enqueues one graph launch on stream (NULL = the context stream). */
+int dr_batch_launch(dr_batch *batch, void *stream);
+/* Device pointers of a view's output tiles (tw*th float4 each; sums of the last launch). */
+int dr_batch_output(dr_batch *batch, uint32_t view, float **sun_dev, float **sky_dev);
+/* Waits for the device and copies a view's output tiles to the host. */
+int dr_batch_read(dr_batch *batch, uint32_t view, float *sun_out, float *sky_out);
+/* Path indices per launch (tile padding included) and launches so far. */
+int dr_batch_info(dr_batch *batch, uint64_t *n_paths, uint64_t *launches);
 
 /* ---- counters ------------------------------------------------------------ */
 int dr_get_counters(dr_ctx *ctx, dr_counters *out);

@@ -8,6 +8,11 @@ Fixtures (all produced by the reference, none hand-written):
   mie_reference_table.npz  miepdf / miecdf of src/KernelSampler.cpp:8-141
   sky_states.json          arhosek_rgb_skymodelstate_alloc_init results for the
                            configurations' (turbidity, albedo, elevation)
+  sky_states_by_degree.json the same for turbidity 3, ground albedo 0.3 and a
+                           sun at every whole degree of elevation 5..80
+                           (azimuth 30): the batched workload's suns
+                           (`python tests/golden/make_golden.py sky` writes
+                           this file alone)
   c0_octree.npz            the config-0 scene (64^3 puff, seed 1) as built by the
                            C restatement of the scene build (oracle/port), which
                            the product builder must reproduce bit for bit
@@ -49,8 +54,24 @@ def c0_config(ref: Reference, w: int, h: int, pdf, cdf) -> dict:
                 sky_configs=cfgs, sky_radiances=rads, mie_pdf=pdf, mie_cdf=cdf, viewi=viewi, proji=proji, w=w, h=h)
 
 
+def sky_by_degree(ref: Reference):
+    states = []
+    for deg in range(5, 81):
+        sd = cam.sun_direction(float(deg), W.SUN["azimuth"])
+        E = ref.solar_elevation(sd)
+        c, r = ref.sky_state(W.SKY["turbidity"], W.SKY["albedo"], E)
+        states.append({"degree": deg, "turbidity": W.SKY["turbidity"], "albedo": W.SKY["albedo"], "elevation": E,
+                       "configs": c.tolist(), "radiances": r.tolist()})
+    with open(os.path.join(HERE, "sky_states_by_degree.json"), "w") as f:
+        json.dump(states, f)
+
+
 def main():
     ref, port = Reference(), Port()
+    if sys.argv[1:] == ["sky"]:
+        sky_by_degree(ref)
+        return
+    sky_by_degree(ref)
     pdf, cdf = ref.mie_tables()
     np.savez(os.path.join(HERE, "mie_reference_table.npz"), pdf=pdf, cdf=cdf)
 
