@@ -89,8 +89,141 @@ def crop_box(n=CPU_CROP):
     return (W_IMG - n) // 2, (H_IMG - n) // 2, n, n
 
 
+def batched_workload(pdf, cdf):
+    """Scenes and per-view settings of the batched workload (workloads.c2_batch)."""
+    from droplet_b200.renderer import PhaseTable, RenderSettings
+    from droplet_b200.scene import build_octree
+    from droplet_b200.sky import SkyState
+
+    with open(os.path.join(GOLDEN, "sky_states_by_degree.json")) as f:
+        sky = {s["degree"]: s for s in json.load(f)}
+    fields, views = W.c2_batch()
+    scenes = []
+    for fd in fields:
+        rec = W.config0_recipe(fd["n"], fd["seed"])
+        org, vals = W.sparse_field_fast(rec)
+        scenes.append(build_octree(org, vals, rec.voxel_size, 12))
+    settings = []
+    for v in views:
+        fd, side = fields[v["field"]], v["side"]
+        eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], v["azimuth"], W.CAMERA["elevation"])
+        viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], side, side)
+        ss, sa, ev = W.medium_of(fd["sigma_t"], W.C2_ALBEDO, W.C2_SCATTEVS)
+        st = sky[v["sun_elevation"]]
+        settings.append(RenderSettings(
+            sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=cam.sun_direction(v["sun_elevation"], W.SUN["azimuth"]),
+            sun_color=np.asarray(W.SUN["color"], np.float32), sun_angle=W.SUN["angle"],
+            sky=SkyState(np.asarray(st["configs"]), np.asarray(st["radiances"])), phase=PhaseTable(pdf, cdf),
+            viewi=viewi, proji=proji, w=side, h=side))
+    return fields, views, scenes, settings
+
+
+def measure_batched(r, pdf, cdf, steps: int, warmup: int):
+    """The batched workload (8 fields x 64 views, one persistent launch per step
+    replayed from a CUDA graph) against the plain single-frame path on the same
+    views: one launch per view (device time), and the addon's call pattern,
+    64x64 tiles through the blocking host API (wall time)."""
+    import torch
+
+    from droplet_b200 import autotune
+    from droplet_b200.renderer import Batch, BatchView
+
+    t = time.time()
+    fields, views, scenes, settings = batched_workload(pdf, cdf)
+    t_build = time.time() - t
+    saved = r.get_tuning()
+    bviews = [BatchView(v["field"], settings[i], v["spp"], 100 + i) for i, v in enumerate(views)]
+    b = Batch(r, scenes, bviews)
+    # the autotuner times a probe batch: every view, centre crop of at most 128^2, 4 spp
+    probe = []
+    for i, v in enumerate(views):
+        c = min(v["side"], 128)
+        o = (v["side"] - c) // 2
+        probe.append(BatchView(v["field"], settings[i], 4, 100 + i, (o, o, c, c)))
+    pb = Batch(r, scenes, probe)
+    t = time.time()
+    best, table = autotune.tune_batch(pb, "c2-probe", use_cache=False)
+    t_tune = time.time() - t
+    pb.close()
+    b.set_tuning(*best)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(max(1, warmup)):
+        b.launch(stream.cuda_stream)
+    stream.synchronize()
+    r.reset_counters()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            b.launch(stream.cuda_stream)
+            ev[k][1].record(stream)
+    stream.synchronize()
+    ms = [a.elapsed_time(e) for a, e in ev]
+    verts = r.counters()["vertices"] / steps
+    n_paths, _ = b.info()
+    batched = verts / (np.mean(ms) / 1e3)
+    # plain, one launch per view (same samples as the batch's first launch)
+    r.set_tuning(*best)
+    cur, plain_ms, plain_v = -1, 0.0, 0
+    side_max = max(v["side"] for v in views)
+    sun = torch.empty((side_max, side_max, 4), device="cuda")
+    sky = torch.empty_like(sun)
+    for i, v in enumerate(views):
+        if v["field"] != cur:
+            r.upload(scenes[v["field"]])
+            cur = v["field"]
+        r.set_params(settings[i])
+        r.reset_counters()
+        flush.fill_(1.0)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r.render_tile_async(0, 0, v["side"], v["side"], v["spp"], 100 + i, 0, sun.data_ptr(), sky.data_ptr(),
+                            stream.cuda_stream)
+        e.record(stream)
+        e.synchronize()
+        plain_ms += a.elapsed_time(e)
+        plain_v += r.counters()["vertices"]
+    plain = plain_v / (plain_ms / 1e3)
+    # the addon's pattern: 64x64 tiles, one blocking dr_render_tile each (host buffers)
+    cur, t_tiles, tiles_v, n_tiles = -1, 0.0, 0, 0
+    for i, v in enumerate(views):
+        if v["field"] != cur:
+            r.upload(scenes[v["field"]])
+            cur = v["field"]
+        r.set_params(settings[i])
+        r.reset_counters()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for y in range(0, v["side"], 64):
+            for x in range(0, v["side"], 64):
+                r.render_tile(x, y, min(64, v["side"] - x), min(64, v["side"] - y), v["spp"], seed=100 + i,
+                              sample_base=0)
+                n_tiles += 1
+        t_tiles += time.perf_counter() - t
+        tiles_v += r.counters()["vertices"]
+    tiles = tiles_v / t_tiles
+    b.close()
+    r.set_tuning(*saved)
+    return {
+        "workload": "8 fields (config-0 puffs, seeds 10-17, {64..512}^3, sigma_t U[10,80]) x 8 views "
+                    "(side U[128,1024], spp {16,64,256}, sun U[5,80] deg, 500 events), default_rng(2026)",
+        "value": batched, "unit": "vertices/s", "ms_per_launch": float(np.mean(ms)), "launch_ms": ms,
+        "vertices_per_launch": verts, "path_indices_per_launch": n_paths,
+        "plain_per_view": {"value": plain, "ms": plain_ms, "launches": len(views)},
+        "plain_addon_tiles_64": {"value": tiles, "seconds": t_tiles, "calls": n_tiles},
+        "speedup_vs_plain_per_view": batched / plain, "speedup_vs_addon_tiles": batched / tiles,
+        "tuning": {"choice": list(best), "seconds": round(t_tune, 2), "probe": "centre <=128^2 crops, 4 spp",
+                   "top": [[c, round(m, 3)] for c, m in table[:6]]},
+        "graph": "memset outputs -> persistent kernel over all views -> step counter", "build_s": round(t_build, 1),
+        "l2": "flushed before each timed launch (256 MB write)",
+    }
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms by one
+    nvidia-smi process in loop mode, kept for the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -99,27 +232,44 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.rows = []
-        self.stop = threading.Event()
+        self.proc = None
         self.th = threading.Thread(target=self.run, daemon=True)
+        self.recording = False
 
     def run(self):
-        while not self.stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
+        try:
+            for line in self.proc.stdout:
+                if self.recording:
                     self.rows.append([x.strip() for x in line.split(",")])
-            except Exception:
-                pass
-            self.stop.wait(0.2)
+        except Exception:
+            pass
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
 
     def __enter__(self):
-        self.th.start()
+        self.recording = True
         return self
 
     def __exit__(self, *a):
-        self.stop.set()
-        self.th.join(timeout=10)
+        time.sleep(0.15)
+        self.recording = False
+
+    def close(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.proc = None
 
     def summary(self):
         if not self.rows:
@@ -184,6 +334,58 @@ def port_vertices(nodes, bricks, cfg, threads: int) -> int:
     x0, y0, tw, th = crop_box()
     _, _, cnt = port.render_tile(S, P, x0, y0, tw, th, SPP, seed=99, threads=threads)
     return cnt["vertices"]
+
+
+def seconds_to_rmse(r, stream, region, ms_per_frame: float, target: float = 0.01, ref_spp: int = 4096,
+                    chunk: int = 256):
+    """Seconds of plain rendering to reach `target` relative RMSE against the
+    converged image.  The converged image is the mean of two independent
+    ref_spp renders A and B (fresh seeds); the reference's own noise is removed
+    with MSE(A, B) / 4.  A 64-spp frame (the step's workload) gives the error
+    at 64 spp; MSE falls as 1/spp, so n* = 64 (rmse_64 / target)^2 spp, and
+    a render at n* spp (fresh seed) checks the prediction."""
+    import torch
+
+    x0, y0, tw, th = region
+
+    def render(spp, seed):
+        out = torch.zeros((th, tw, 4), dtype=torch.float64, device="cuda")
+        sun = torch.empty((th, tw, 4), dtype=torch.float32, device="cuda")
+        sky = torch.empty_like(sun)
+        done = 0
+        with torch.cuda.stream(stream):
+            while done < spp:
+                n = min(chunk, spp - done)
+                r.render_tile_async(x0, y0, tw, th, n, seed, done, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
+                out += (sun + sky).double()
+                done += n
+        stream.synchronize()
+        return (out[..., :3] / spp).reshape(-1)
+
+    t = time.time()
+    A, B = render(ref_spp, 7001), render(ref_spp, 7002)
+    X64 = render(SPP, 7003)
+    # pixels whose sums hold a NaN (the reference estimator's 0/0 cases, e.g. a
+    # direction with rd.y == 0 in the sky term) are left out, and counted
+    ok = torch.isfinite(A) & torch.isfinite(B) & torch.isfinite(X64)
+    R = 0.5 * (A + B)
+    noise = float(((A - B)[ok] ** 2).mean()) / 4.0
+    scale = float((R[ok] ** 2).mean())
+
+    def rel(X, m):
+        return float(np.sqrt(max(float(((X - R)[m] ** 2).mean()) - noise, 0.0) / scale))
+
+    e64 = rel(X64, ok)
+    n_star = int(np.ceil(SPP * (e64 / target) ** 2))
+    check = None
+    if n_star <= 4 * ref_spp:
+        Xn = render(n_star, 7004)
+        check = rel(Xn, ok & torch.isfinite(Xn))
+    return {"target": target, "rmse_at_64spp": e64, "spp_needed": n_star, "check_rmse_at_spp_needed": check,
+            "seconds": n_star / SPP * ms_per_frame / 1e3,
+            "reference_image": f"mean of 2 x {ref_spp} spp GPU renders, its noise removed (MSE(A,B)/4)",
+            "reference_noise_rel": float(np.sqrt(noise / scale)), "wall_s": round(time.time() - t, 1),
+            "non_finite_values_excluded": int((~ok).sum())}
 
 
 def run_reference(args):
@@ -274,7 +476,9 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks, torch.cuda.stream(stream):
+    clocks = ClockSampler(local).start()
+    time.sleep(0.3)  # the sampler's first lines
+    with clocks, torch.cuda.stream(stream):
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
@@ -283,6 +487,7 @@ def run_b200(args):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    clocks.close()
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
     t_local = sum(kernel_ms) / 1e3
     cnt = r.counters()
@@ -298,10 +503,11 @@ def run_b200(args):
     value = verts / t_max
 
     # end to end through the public blocking API with host buffers (params upload
-    # from host + render + copy of both tile buffers back), timed on the host
-    h_sun = np.zeros((H_IMG, W_IMG, 4), np.float32)
-    h2d = 0
-    settings_c = settings.to_c()
+    # from host + render + copy of both tile buffers back into the caller's
+    # frame buffers, allocated once as a renderer keeps its framebuffer), timed
+    # on the host
+    frame = (np.zeros((TH, TW, 4), np.float32), np.zeros((TH, TW, 4), np.float32))
+    r.render_tile(X0, Y0, TW, TH, 1, seed=seed, sample_base=0, out=frame)  # touches the pages once
     h2d = int(pdf.nbytes / 3 * 4 + cdf.nbytes / 3 + 16 * 4 * 2 + 64)
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
@@ -310,7 +516,7 @@ def run_b200(args):
     t0 = time.perf_counter()
     for k in range(e2e_steps):
         r.set_params(settings)
-        a, b = r.render_tile(X0, Y0, TW, TH, SPP, seed=seed, sample_base=(args.warmup + k) * SPP)
+        r.render_tile(X0, Y0, TW, TH, SPP, seed=seed, sample_base=(args.warmup + k) * SPP, out=frame)
     t_e2e = (time.perf_counter() - t0)
     if world > 1:
         t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
@@ -319,15 +525,28 @@ def run_b200(args):
     e2e_value = (verts / args.steps) * e2e_steps / t_e2e  # same work per frame
     d2h = 2 * TH * TW * 16
 
+    # Algorithmic bytes per vertex B_v = 64 node visits + 32 density lookups +
+    # 24 Mie evaluations, counted on a calibration frame (16 spp, fixed seed)
+    # with the octree stack traversal, whose node visits are the reference's.
+    saved = r.get_tuning()
+    r.set_tuning(0, saved[1], saved[2], 0, saved[4])
+    r.reset_counters()
+    with torch.cuda.stream(stream):
+        r.render_tile_async(X0, Y0, TW, TH, 16, 4242, 0, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    cal = r.counters()
+    r.set_tuning(*saved)
+    b_v = (64.0 * cal["node_visits"] + 32.0 * cal["density_lookups"] + 24.0 * cal["mie_evals"]) / cal["vertices"]
     peak, peak_kind = measured_peak()
-    bytes_per_step = (64.0 * cnt["node_visits"] + 32.0 * cnt["density_lookups"] + 24.0 * cnt["mie_evals"]) / args.steps
+    bytes_per_step = b_v * cnt["vertices"] / args.steps
     avg_s = t_local / args.steps
     achieved = bytes_per_step / avg_s / 1e9
     traffic = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
                 "traffic": (traffic["dram_bytes_per_vertex"] * cnt["vertices"] / args.steps) if traffic else None,
-                "algorithmic_bytes_per_vertex": bytes_per_step / (cnt["vertices"] / args.steps)}
+                "algorithmic_bytes_per_vertex": b_v,
+                "calibration": "B_v from a 16-spp frame (seed 4242) with the octree stack traversal"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -346,6 +565,20 @@ def run_b200(args):
         except Exception as e:  # the reference oracle needs oracle/_ref
             cpu = {"value": None, "unit": "vertices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    rmse = None
+    if rank == 0 and world == 1 and not args.no_rmse:
+        rmse = seconds_to_rmse(r, stream, (X0, Y0, TW, TH), t_local / args.steps * 1e3)
+        rmse["seconds_e2e"] = rmse["spp_needed"] / SPP * (verts / args.steps) / e2e_value
+        if cpu and cpu.get("value"):
+            rmse["seconds_cpu_reference"] = rmse["spp_needed"] / SPP * (verts / args.steps) / cpu["value"]
+        log(f"s to 1% rmse: {rmse['seconds']:.2f} (spp {rmse['spp_needed']}, check {rmse['check_rmse_at_spp_needed']})")
+
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = measure_batched(r, pdf, cdf, steps=2, warmup=1)
+        log(f"batched: {batched['value'] / 1e9:.3f} G vertices/s, plain per view "
+            f"{batched['plain_per_view']['value'] / 1e9:.3f}, addon tiles {batched['plain_addon_tiles_64']['value'] / 1e9:.3f}")
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": world, "steps": args.steps,
@@ -362,6 +595,8 @@ def run_b200(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
+            "seconds_to_1pct_rmse": rmse,
+            "batched": batched,
             "counters_per_step": {k: v / args.steps for k, v in cnt.items()},
             "kernel_ms": kernel_ms,
         }
@@ -381,7 +616,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--crop", type=int, default=0, help="render only an NxN centre crop per step (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
-    ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal (no tuning)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload measurement")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the seconds-to-1%%-RMSE measurement")
+    ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal,tile (no tuning)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -90,6 +90,16 @@ int dr_destroy(dr_ctx *c) {
         c->tile_sky.release();
         c->scratch.release();
         c->work.release();
+        c->band_work.release();
+        for (int k = 0; k < 2; ++k)
+            if (c->band_stream[k]) cudaStreamSynchronize(c->band_stream[k]), cudaStreamDestroy(c->band_stream[k]);
+        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
+        if (c->ev_clear) cudaEventDestroy(c->ev_clear);
+        for (int k = 0; k < dr_ctx::kBands; ++k) {
+            if (c->band_done[k]) cudaEventDestroy(c->band_done[k]);
+            if (c->copy_done[k]) cudaEventDestroy(c->copy_done[k]);
+        }
+        if (c->pinned) cudaFreeHost(c->pinned);
         if (c->stream) cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -233,22 +243,106 @@ int dr_get_tuning(dr_ctx *c, dr_tuning *t) {
     return DR_OK;
 }
 
+// Pipeline objects of dr_render_tile, created on first use.
+static int ensure_pipeline(dr_ctx *c, size_t n) {
+    if (!c->copy_stream) {
+        DR_CUDA(cudaStreamCreateWithFlags(&c->band_stream[0], cudaStreamNonBlocking), "render: streams");
+        DR_CUDA(cudaStreamCreateWithFlags(&c->band_stream[1], cudaStreamNonBlocking), "render: streams");
+        DR_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "render: streams");
+        DR_CUDA(cudaEventCreateWithFlags(&c->ev_clear, cudaEventDisableTiming), "render: events");
+        for (int k = 0; k < dr_ctx::kBands; ++k) {
+            DR_CUDA(cudaEventCreateWithFlags(&c->band_done[k], cudaEventDisableTiming), "render: events");
+            DR_CUDA(cudaEventCreateWithFlags(&c->copy_done[k], cudaEventDisableTiming), "render: events");
+        }
+        DR_CUDA(c->band_work.reserve(dr_ctx::kBands), "render: queues");
+    }
+    if (c->pinned_n < n) {
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->pinned = nullptr;
+        c->pinned_n = 0;
+        DR_CUDA(cudaHostAlloc((void **)&c->pinned, 2 * n * sizeof(float4), cudaHostAllocDefault),
+                "render: pinned staging");
+        c->pinned_n = n;
+    }
+    return DR_OK;
+}
+
+// Blocking render into host buffers.  The tile's rows are cut into up to
+// kBands even bands; band k renders on stream k % 2 (so a band starts while the
+// previous one drains), is copied to pinned staging on the copy stream when it
+// is done, and the host moves it to the caller's buffers while later bands
+// still render.  Paths depend only on (pixel, sample): banding does not change
+// the result.
 int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                    uint64_t sample_base, float *sun_out, float *sky_out) {
     if (!c || !sun_out || !sky_out) return need(false, DR_ERR_INVALID, "dr_render_tile: null argument");
+    if (!c->has_scene || !c->has_params)
+        return need(false, DR_ERR_STATE, "render: upload a scene and set parameters first");
+    if (tw == 0 || th == 0) return need(false, DR_ERR_INVALID, "render: empty tile");
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t n = (size_t)tw * th;
     DR_CUDA(c->tile_sun.reserve(n), "render: alloc tile");
     DR_CUDA(c->tile_sky.reserve(n), "render: alloc tile");
-    int rc = dr_render_tile_async(c, x0, y0, tw, th, spp, seed, sample_base, (float *)c->tile_sun.p,
-                                  (float *)c->tile_sky.p, nullptr);
+    int rc = ensure_pipeline(c, n);
     if (rc != DR_OK) return rc;
-    DR_CUDA(cudaMemcpyAsync(sun_out, c->tile_sun.p, n * sizeof(float4), cudaMemcpyDeviceToHost, c->stream),
-            "render: copy out");
-    DR_CUDA(cudaMemcpyAsync(sky_out, c->tile_sky.p, n * sizeof(float4), cudaMemcpyDeviceToHost, c->stream),
-            "render: copy out");
-    DR_CUDA(cudaStreamSynchronize(c->stream), "render: sync");
+    const uint32_t rows = 2 * (th / 2);
+    const uint32_t nb = rows >= 512 ? 8u : rows >= 128 ? 4u : 1u;
+    uint32_t hb = (rows + nb - 1) / nb;
+    hb += hb & 1u;
+    DR_CUDA(cudaMemsetAsync(c->tile_sun.p, 0, n * sizeof(float4), c->stream), "render: clear");
+    DR_CUDA(cudaMemsetAsync(c->tile_sky.p, 0, n * sizeof(float4), c->stream), "render: clear");
+    DR_CUDA(cudaEventRecord(c->ev_clear, c->stream), "render: record");
+    DR_CUDA(cudaStreamWaitEvent(c->band_stream[0], c->ev_clear, 0), "render: wait");
+    DR_CUDA(cudaStreamWaitEvent(c->band_stream[1], c->ev_clear, 0), "render: wait");
+    const uint32_t tile = c->tuning.kernel == DR_KERNEL_PER_PATH ? 0u : c->tuning.tile;
+    std::vector<std::pair<size_t, size_t>> spans;  // (float4 offset, float4 count) per band
+    cudaError_t err = cudaSuccess;
+    for (uint32_t k = 0, r0 = 0; r0 < rows && err == cudaSuccess; ++k, r0 += hb) {
+        const uint32_t rk = rows - r0 < hb ? rows - r0 : hb;
+        TileArgs A;
+        rc = make_tile_args(x0, y0 + r0, tw, rk, spp, seed, sample_base, tile, A);
+        if (rc != DR_OK) break;
+        const size_t off = (size_t)r0 * tw, cnt = (size_t)rk * tw;
+        float4 *sd = c->tile_sun.p + off, *kd = c->tile_sky.p + off;
+        cudaStream_t bs = c->band_stream[k & 1];
+        if (c->tuning.kernel == DR_KERNEL_PER_PATH)
+            err = launch_render_tile(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->counters.p, bs);
+        else
+            err = launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->counters.p,
+                                           c->band_work.p + k, c->tuning, c->device, bs);
+        if (err == cudaSuccess) err = cudaEventRecord(c->band_done[k], bs);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(c->copy_stream, c->band_done[k], 0);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(c->pinned + 4 * off, sd, cnt * sizeof(float4), cudaMemcpyDeviceToHost,
+                                  c->copy_stream);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(c->pinned + 4 * (c->pinned_n + off), kd, cnt * sizeof(float4),
+                                  cudaMemcpyDeviceToHost, c->copy_stream);
+        if (err == cudaSuccess) err = cudaEventRecord(c->copy_done[k], c->copy_stream);
+        spans.emplace_back(off, cnt);
+    }
+    for (size_t k = 0; k < spans.size(); ++k) {
+        const cudaError_t e = cudaEventSynchronize(c->copy_done[k]);
+        if (e != cudaSuccess && err == cudaSuccess) err = e;
+        if (err != cudaSuccess) break;
+        std::memcpy(sun_out + 4 * spans[k].first, c->pinned + 4 * spans[k].first, spans[k].second * sizeof(float4));
+        std::memcpy(sky_out + 4 * spans[k].first, c->pinned + 4 * (c->pinned_n + spans[k].first),
+                    spans[k].second * sizeof(float4));
+    }
+    // keep the context stream ordered after the bands and the copies
+    if (err == cudaSuccess) err = cudaStreamSynchronize(c->copy_stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(c->band_stream[0]);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(c->band_stream[1]);
+    if (err != cudaSuccess) {
+        cudaDeviceSynchronize();
+        return cuda_fail(err, "render");
+    }
+    if (rc != DR_OK) return rc;
+    if (rows < th) {  // odd tile: the last row is not rendered (2x2 pixel blocks)
+        std::memset(sun_out + 4 * (size_t)rows * tw, 0, (size_t)tw * sizeof(float4));
+        std::memset(sky_out + 4 * (size_t)rows * tw, 0, (size_t)tw * sizeof(float4));
+    }
     return DR_OK;
 }
 

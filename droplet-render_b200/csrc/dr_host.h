@@ -117,4 +117,15 @@ struct dr_ctx {
     bool use_grid = true;
     dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u};
     std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)
+    // host-buffer render pipeline (dr_render_tile): row bands rendered on two
+    // streams, each copied to pinned staging as soon as it is done
+    static constexpr int kBands = 8;
+    cudaStream_t band_stream[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_clear = nullptr;
+    cudaEvent_t band_done[kBands] = {};
+    cudaEvent_t copy_done[kBands] = {};
+    dr::DevBuf<dr::WorkQueue> band_work;
+    float *pinned = nullptr;  // 2 * pinned_n float4: sun then sky
+    size_t pinned_n = 0;
 };

@@ -121,12 +121,20 @@ class Renderer:
         N.check(N.lib().dr_set_params(self._ctx, C.byref(p)))
         self.settings = s
 
-    def render_tile(self, x0: int, y0: int, tw: int, th: int, spp: int, seed: int = 0, sample_base: int | None = None):
+    def render_tile(self, x0: int, y0: int, tw: int, th: int, spp: int, seed: int = 0, sample_base: int | None = None,
+                    out: tuple | None = None):
         """Sums over `spp` samples: (sun, sky) arrays of shape (th, tw, 4).  Without an
-        explicit sample_base each call continues the stream (new, independent samples)."""
+        explicit sample_base each call continues the stream (new, independent samples).
+        `out` = (sun, sky) reuses caller-owned C-contiguous float32 arrays."""
         base = self.sample_base if sample_base is None else int(sample_base)
-        sun = np.zeros((th, tw, 4), np.float32)
-        sky = np.zeros((th, tw, 4), np.float32)
+        if out is not None:
+            sun, sky = out
+            for a in (sun, sky):
+                if a.dtype != np.float32 or a.shape != (th, tw, 4) or not a.flags.c_contiguous:
+                    raise ValueError("out arrays must be C-contiguous float32 of shape (th, tw, 4)")
+        else:
+            sun = np.zeros((th, tw, 4), np.float32)
+            sky = np.zeros((th, tw, 4), np.float32)
         N.check(N.lib().dr_render_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, sun.ctypes.data,
                                        sky.ctypes.data))
         if sample_base is None:
