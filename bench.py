@@ -336,6 +336,154 @@ def port_vertices(nodes, bricks, cfg, threads: int) -> int:
     return cnt["vertices"]
 
 
+def c3_views(pdf, cdf, cfgs, rads, n_views: int = 16, side: int = 256):
+    """The inverse-rendering workload's views: the config-0 camera and sun at
+    n_views evenly spaced azimuths."""
+    from droplet_b200.renderer import PhaseTable, RenderSettings
+    from droplet_b200.sky import SkyState
+
+    ss, sa, ev = W.medium("c0")
+    out = []
+    for k in range(n_views):
+        eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], 360.0 * k / n_views, W.CAMERA["elevation"])
+        viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], side, side)
+        out.append(RenderSettings(
+            sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"]),
+            sun_color=np.asarray(W.SUN["color"], np.float32), sun_angle=W.SUN["angle"], sky=SkyState(cfgs, rads),
+            phase=PhaseTable(pdf, cdf), viewi=viewi, proji=proji, w=side, h=side, finite_paths=True))
+    return out
+
+
+def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd_groups: int = 8,
+                    fd_spp: int = 32, fd_eps: float = 1e-3):
+    """Inverse rendering (config 3): target = the config-0 puff at 128^3, seed 5,
+    16 views of 256^2 at 256 spp; parameters = the brick samples of a uniform
+    0.3 grid (128^3) and the albedo; L2 image loss; 32 spp per gradient step.
+    Times the forward (render of the 16 views) and the adjoint (backward) with
+    CUDA events; checks the gradient against central finite differences with
+    common random numbers (eps 1e-3, majorants held fixed) on 256 random
+    voxels (default_rng(5)): per seed group, the directional derivative along
+    random signs on those voxels."""
+    import torch
+
+    from droplet_b200 import adjoint as AD
+    from droplet_b200.scene import build_from_dense, build_octree
+
+    t = time.time()
+    rec = W.config0_recipe(128, 5)
+    org, vals = W.sparse_field_fast(rec)
+    target_oc = build_octree(org, vals, rec.voxel_size, 12)
+    guess_oc = build_from_dense(np.full((128, 128, 128), 0.3, np.float32), 1.0 / 128, 12)
+    views = c3_views(pdf, cdf, cfgs, rads)
+    saved = r.get_tuning()
+    r.upload(target_oc)
+    with torch.no_grad():
+        tb = torch.tensor(target_oc.bricks, device="cuda")
+        tsun, tsky = AD.render(tb, torch.tensor(0.99, device="cuda"), r,
+                               [AD.DiffView(v, 256, 500 + k) for k, v in enumerate(views)])
+        target = (tsun + tsky)[..., :3].clone()
+    r.upload(guess_oc)
+    b = torch.tensor(guess_oc.bricks, device="cuda", requires_grad=True)
+    alb = torch.tensor(0.99, device="cuda", requires_grad=True)
+    t_setup = time.time() - t
+    fw, bw = [], []
+    stream = torch.cuda.current_stream()
+    for it in range(warmup + steps):
+        dv = [AD.DiffView(v, 32, 1000 + 97 * it + k) for k, v in enumerate(views)]
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        sun, sky = AD.render(b, alb, r, dv, majorant_scale=1.05)
+        loss = (((sun + sky)[..., :3] - target) ** 2).sum()
+        e1.record(stream)
+        b.grad = None
+        alb.grad = None
+        loss.backward()
+        e2.record(stream)
+        e2.synchronize()
+        if it >= warmup:
+            fw.append(e0.elapsed_time(e1))
+            bw.append(e1.elapsed_time(e2))
+    grad = b.grad.detach().clone()
+    galb = float(alb.grad)
+    # finite differences with common random numbers (eps 1e-3) on 256 voxels
+    nl = guess_oc.n_leaves
+    rng = np.random.default_rng(5)
+    pick = torch.as_tensor(rng.choice(nl * 512, 256, replace=False), device="cuda")
+    signs = torch.as_tensor(rng.choice([-1.0, 1.0], 256).astype(np.float32), device="cuda")
+    u = torch.zeros(nl * 512, device="cuda")
+    u[pick] = signs
+    u = u.reshape(nl, 512)
+    eps = fd_eps
+    base = b.detach().clone()
+    r.set_bricks_dev(base.data_ptr(), nl, 1.05)  # majorants with headroom, then held fixed
+    img = torch.empty((256, 256, 4), device="cuda")
+    img2 = torch.empty_like(img)
+
+    def loss_at(bricks, albedo, seed):
+        r.set_bricks_dev(bricks.data_ptr(), nl, 0.0)
+        tot = 0.0
+        for k, v in enumerate(views):
+            r.set_params(AD._with_albedo(v, albedo))
+            r.render_tile_async(0, 0, 256, 256, fd_spp, seed + k, 0, img.data_ptr(), img2.data_ptr())
+            r.synchronize()
+            x = (img.double() + img2.double())[..., :3] / fd_spp
+            tot += float((delta[k].double() * x).sum())
+        return tot
+
+    def adjoint_at(albedo, seed):
+        r.set_bricks_dev(base.data_ptr(), nl, 0.0)
+        g = torch.zeros_like(base)
+        ga = torch.zeros(1, dtype=torch.float64, device="cuda")
+        for k, v in enumerate(views):
+            r.set_params(AD._with_albedo(v, albedo))
+            d4 = torch.zeros((256, 256, 4), device="cuda")
+            d4[..., :3] = delta[k] / fd_spp
+            r.adjoint_tile_async(0, 0, 256, 256, fd_spp, seed + k, 0, d4.data_ptr(), d4.data_ptr(), g.data_ptr(),
+                                 ga.data_ptr())
+            r.synchronize()
+        return g, float(ga.item())
+
+    # linearised loss: delta = dL/dI at the base point, so both estimators
+    # target the same derivative of the expected image
+    a0 = 0.99
+    with torch.no_grad():
+        dv = [AD.DiffView(v, fd_spp, 50000 + k) for k, v in enumerate(views)]
+        sun, sky = AD.render(base, torch.tensor(a0, device="cuda"), r, dv, majorant_scale=0.0)
+        delta = 2 * ((sun + sky)[..., :3] - target)
+    fd, ad, fa, aa = [], [], [], []
+    t = time.time()
+    # the one-thread-per-path kernel sums each pixel's 32-sample groups in a
+    # fixed order: the two renders of a difference share their rounding
+    r.set_tuning(1, 0, 0, 0, 0)
+    ea = 1e-3
+    for gi in range(fd_groups):
+        seed = 70000 + 1000 * gi
+        fd.append((loss_at(base + eps * u, a0, seed) - loss_at(base - eps * u, a0, seed)) / (2 * eps))
+        fa.append((loss_at(base, a0 + ea, seed) - loss_at(base, a0 - ea, seed)) / (2 * ea))
+        g, ga = adjoint_at(a0, seed)
+        ad.append(float((g * u).sum()))
+        aa.append(ga)
+    fd, ad, fa, aa = np.array(fd), np.array(ad), np.array(fa), np.array(aa)
+    diff = fd - ad
+    r.set_tuning(*saved)
+    return {
+        "workload": "config-0 puff 128^3 seed 5 target, 16 views 256^2 (target 256 spp), uniform 0.3 guess "
+                    f"({guess_oc.n_leaves} leaves x 512 samples), L2 loss, 32 spp per gradient step",
+        "forward_ms": float(np.mean(fw)), "adjoint_ms": float(np.mean(bw)),
+        "adjoint_over_forward": float(np.mean(bw) / np.mean(fw)),
+        "grad_norm": float(grad.norm()), "grad_albedo": galb,
+        "fd_check": {"eps": eps, "voxels": 256, "groups": fd_groups, "spp_per_view": fd_spp,
+                     "directional_fd": fd.tolist(), "directional_adjoint": ad.tolist(),
+                     "mean_fd": float(fd.mean()), "mean_adjoint": float(ad.mean()),
+                     "rel_diff_of_means": float(abs(fd.mean() - ad.mean()) / max(abs(ad.mean()), 1e-30)),
+                     "se_of_diff": float(diff.std(ddof=1) / np.sqrt(len(diff))),
+                     "albedo": {"eps": ea, "fd": fa.tolist(), "adjoint": aa.tolist(),
+                                "max_rel_diff": float(np.max(np.abs(fa - aa) / np.maximum(np.abs(fa), 1e-30)))},
+                     "seconds": round(time.time() - t, 1)},
+        "setup_s": round(t_setup, 1),
+    }
+
+
 def seconds_to_rmse(r, stream, region, ms_per_frame: float, target: float = 0.01, ref_spp: int = 4096,
                     chunk: int = 256):
     """Seconds of plain rendering to reach `target` relative RMSE against the
@@ -573,6 +721,14 @@ def run_b200(args):
             rmse["seconds_cpu_reference"] = rmse["spp_needed"] / SPP * (verts / args.steps) / cpu["value"]
         log(f"s to 1% rmse: {rmse['seconds']:.2f} (spp {rmse['spp_needed']}, check {rmse['check_rmse_at_spp_needed']})")
 
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = measure_adjoint(r, pdf, cdf, cfgs, rads, fd_groups=args.fd_groups, fd_spp=args.fd_spp,
+                                  fd_eps=args.fd_eps)
+        log(f"adjoint: forward {adjoint['forward_ms']:.1f} ms, adjoint {adjoint['adjoint_ms']:.1f} ms, "
+            f"ratio {adjoint['adjoint_over_forward']:.2f}, fd {adjoint['fd_check']['mean_fd']:.4g} "
+            f"vs {adjoint['fd_check']['mean_adjoint']:.4g}")
+
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = measure_batched(r, pdf, cdf, steps=2, warmup=1)
@@ -597,6 +753,7 @@ def run_b200(args):
             "clocks": clocks.summary(),
             "seconds_to_1pct_rmse": rmse,
             "batched": batched,
+            "adjoint": adjoint,
             "counters_per_step": {k: v / args.steps for k, v in cnt.items()},
             "kernel_ms": kernel_ms,
         }
@@ -618,6 +775,10 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload measurement")
     ap.add_argument("--no-rmse", action="store_true", help="skip the seconds-to-1%%-RMSE measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the inverse-rendering (adjoint) measurement")
+    ap.add_argument("--fd-groups", type=int, default=8, help="seed groups of the finite-difference check")
+    ap.add_argument("--fd-spp", type=int, default=32, help="spp per view of the finite-difference check")
+    ap.add_argument("--fd-eps", type=float, default=1e-3, help="brick-sample step of the finite-difference check")
     ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal,tile (no tuning)")
     args = ap.parse_args()
     if args.impl == "reference":

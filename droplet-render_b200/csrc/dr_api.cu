@@ -1,4 +1,5 @@
 // C ABI of droplet_b200 (declared in include/droplet_b200.h).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -90,6 +91,9 @@ int dr_destroy(dr_ctx *c) {
         c->tile_sky.release();
         c->scratch.release();
         c->work.release();
+        c->leaf_nodes.release();
+        c->grad_copies.release();
+        c->albedo_slots.release();
         c->band_work.release();
         for (int k = 0; k < 2; ++k)
             if (c->band_stream[k]) cudaStreamSynchronize(c->band_stream[k]), cudaStreamDestroy(c->band_stream[k]);
@@ -133,6 +137,14 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
     std::lock_guard<std::mutex> lk(c->mu);
     rc = upload_scene(h, c->bufs, c->use_grid, c->stream, c->scene);
     if (rc != DR_OK) return rc;
+    std::vector<uint32_t> ln;
+    for (uint32_t i = 0; i < h.n_nodes; ++i)
+        if (h.leaf_flag[i]) ln.push_back(i);
+    DR_CUDA(c->leaf_nodes.reserve(ln.size()), "dr_upload_scene: alloc leaf list");
+    if (!ln.empty())
+        DR_CUDA(cudaMemcpy(c->leaf_nodes.p, ln.data(), ln.size() * 4, cudaMemcpyHostToDevice),
+                "dr_upload_scene: copy leaf list");
+    c->n_leaf_nodes = (uint32_t)ln.size();
     c->leaf_flag = std::move(h.leaf_flag);
     c->has_scene = true;
     return DR_OK;
@@ -527,6 +539,99 @@ int dr_transmittance_noalloc(dr_ctx *c, const float *ro_dev, const float *rd_dev
     DR_CUDA(launch_transmittance_noalloc(c->scene, c->params, scratch, ro_dev, rd_dev, n_rays, nsamp, seed, out_dev,
                                          st),
             "dr_transmittance_noalloc: launch");
+    return DR_OK;
+}
+
+
+// ---- differentiable rendering --------------------------------------------------
+int dr_set_bricks_dev(dr_ctx *c, const float *bricks_dev, uint32_t n_leaves, float majorant_scale, void *stream) {
+    if (!c || !bricks_dev) return need(false, DR_ERR_INVALID, "dr_set_bricks_dev: null argument");
+    if (!c->has_scene) return need(false, DR_ERR_STATE, "dr_set_bricks_dev: no scene");
+    if (n_leaves != c->scene.n_leaves)
+        return need(false, DR_ERR_INVALID, "dr_set_bricks_dev: brick count differs from the scene's");
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    DR_CUDA(cudaMemcpyAsync(c->bufs.bricks.p, bricks_dev, (size_t)n_leaves * kBrick * sizeof(float),
+                            cudaMemcpyDeviceToDevice, st),
+            "dr_set_bricks_dev: copy");
+    if (!(majorant_scale == 0.0f || majorant_scale >= 1.0f) || !std::isfinite(majorant_scale))
+        return need(false, DR_ERR_INVALID, "dr_set_bricks_dev: majorant_scale must be 0 or >= 1");
+    if (majorant_scale > 0.0f)
+        DR_CUDA(launch_leaf_majorants(c->bufs.leaf.p, c->leaf_nodes.p, c->n_leaf_nodes, c->bufs.bricks.p,
+                                      majorant_scale, st),
+                "dr_set_bricks_dev: majorants");
+    return DR_OK;
+}
+
+int dr_get_majorants(dr_ctx *c, float *out) {
+    if (!c || !out) return need(false, DR_ERR_INVALID, "dr_get_majorants: null argument");
+    if (!c->has_scene) return need(false, DR_ERR_STATE, "dr_get_majorants: no scene");
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    std::vector<float4> leaf((size_t)c->scene.n_nodes * 2);
+    DR_CUDA(cudaStreamSynchronize(c->stream), "dr_get_majorants: sync");
+    DR_CUDA(cudaMemcpy(leaf.data(), c->bufs.leaf.p, leaf.size() * sizeof(float4), cudaMemcpyDeviceToHost),
+            "dr_get_majorants: copy");
+    for (uint32_t i = 0; i < c->scene.n_nodes; ++i) out[i] = c->leaf_flag[i] ? leaf[2 * (size_t)i + 1].x : 0.0f;
+    return DR_OK;
+}
+
+int dr_adjoint_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
+                          uint64_t sample_base, const float *dsun_dev, const float *dsky_dev, float *grad_bricks_dev,
+                          double *grad_albedo_dev, void *stream) {
+    if (!c || !dsun_dev || !dsky_dev || !grad_bricks_dev || !grad_albedo_dev)
+        return need(false, DR_ERR_INVALID, "dr_adjoint_tile_async: null argument");
+    TileArgs A;
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, 0u, A);
+    if (rc != DR_OK) return rc;
+    if (!(c->params.albedo > 0.0f))
+        return need(false, DR_ERR_INVALID, "dr_adjoint_tile_async: the albedo gradient needs sigma_s > 0");
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    // spread copies of the gradient: up to 16, within 256 MB
+    const size_t gbytes = (size_t)c->scene.n_leaves * kBrick * sizeof(float);
+    uint32_t copies = (uint32_t)std::min<size_t>(16, (256u << 20) / (gbytes ? gbytes : 1));
+    if (copies > 1 && c->grad_copies.reserve((size_t)copies * c->scene.n_leaves * kBrick) != cudaSuccess) copies = 1;
+    if (!c->albedo_slots.p) {
+        DR_CUDA(c->albedo_slots.reserve(adjoint_slots()), "adjoint: alloc slots");
+        DR_CUDA(cudaMemset(c->albedo_slots.p, 0, sizeof(double) * adjoint_slots()), "adjoint: clear slots");
+    }
+    DR_CUDA(launch_adjoint_tile(c->scene, c->params, A, c->mie_pack.p, (const float4 *)dsun_dev,
+                                (const float4 *)dsky_dev, grad_bricks_dev, copies > 1 ? c->grad_copies.p : nullptr,
+                                copies, grad_albedo_dev, c->albedo_slots.p, c->counters.p, st),
+            "adjoint: launch");
+    return DR_OK;
+}
+
+int dr_adjoint_transmittance(dr_ctx *c, const float *ro, const float *rd, const float *weights, uint32_t n,
+                             uint64_t nsamp, uint64_t seed, float *grad_bricks, double *transmittance) {
+    if (!c || !ro || !rd || !weights || !grad_bricks || n == 0 || nsamp == 0)
+        return need(false, DR_ERR_INVALID, "dr_adjoint_transmittance: bad argument");
+    if (!c->has_scene || !c->has_params) return need(false, DR_ERR_STATE, "dr_adjoint_transmittance: no scene");
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const size_t ng = (size_t)c->scene.n_leaves * kBrick;
+    Scratch S;
+    size_t o_ro = S.add(12 * (size_t)n), o_rd = S.add(12 * (size_t)n), o_w = S.add(4 * (size_t)n),
+           o_e = S.add(8 * (size_t)n), o_g = S.add(4 * ng);
+    DR_CUDA(c->scratch.reserve(S.total), "adjoint: alloc");
+    unsigned char *b = c->scratch.p;
+    DR_CUDA(cudaMemcpy(b + o_ro, ro, 12 * (size_t)n, cudaMemcpyHostToDevice), "adjoint: copy");
+    DR_CUDA(cudaMemcpy(b + o_rd, rd, 12 * (size_t)n, cudaMemcpyHostToDevice), "adjoint: copy");
+    DR_CUDA(cudaMemcpy(b + o_w, weights, 4 * (size_t)n, cudaMemcpyHostToDevice), "adjoint: copy");
+    DR_CUDA(cudaMemset(b + o_e, 0, 8 * (size_t)n), "adjoint: clear");
+    DR_CUDA(cudaMemset(b + o_g, 0, 4 * ng), "adjoint: clear");
+    DR_CUDA(launch_adjoint_transmittance(c->scene, c->params, (const float *)(b + o_ro), (const float *)(b + o_rd),
+                                         (const float *)(b + o_w), n, nsamp, seed, (float *)(b + o_g),
+                                         (unsigned long long *)(b + o_e), c->stream),
+            "adjoint: launch");
+    DR_CUDA(cudaStreamSynchronize(c->stream), "adjoint: sync");
+    DR_CUDA(cudaMemcpy(grad_bricks, b + o_g, 4 * ng, cudaMemcpyDeviceToHost), "adjoint: copy out");
+    if (transmittance) {
+        std::vector<unsigned long long> esc(n);
+        DR_CUDA(cudaMemcpy(esc.data(), b + o_e, 8 * (size_t)n, cudaMemcpyDeviceToHost), "adjoint: copy out");
+        for (uint32_t i = 0; i < n; ++i) transmittance[i] = (double)esc[i] / (double)nsamp;
+    }
     return DR_OK;
 }
 

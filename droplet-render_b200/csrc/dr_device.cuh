@@ -523,6 +523,34 @@ __device__ __forceinline__ float sample_voxel_space(const float p[3], const floa
     return lerp_ref(v0, v1, nl[2]);
 }
 
+// Corner offsets (within the brick) and trilinear weights of the lookup above:
+// rho = sum_k w[k] * v[idx[k]] (lerp_ref(a, b, t) = (1 - t) a + t b), the
+// derivative of rho with respect to each brick sample.
+__device__ __forceinline__ void voxel_weights(const float p[3], const float4 ce, uint32_t idx[8], float w[8]) {
+    const float nm1 = (float)kLvox - 1.0f;
+    const float top = (float)(kLvox - 1);
+    const float cc[3] = {ce.x, ce.y, ce.z};
+    uint32_t ia[3], ib[3];
+    float nl[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float ni = ((-0.5f * ((cc[k] - ce.w) - p[k])) * nm1) / ce.w;
+        float nf = sse_max(floorf(ni), 0.0f);
+        float nc = sse_min(ceilf(ni), nm1);
+        nl[k] = ni - nf;
+        nc = sse_max(sse_min(nc, top), 0.0f);
+        nf = sse_max(sse_min(nf, top), 0.0f);
+        ia[k] = (uint32_t)nf;
+        ib[k] = (uint32_t)nc;
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t x = (c & 1) ? ib[0] : ia[0], y = (c & 2) ? ib[1] : ia[1], z = (c & 4) ? ib[2] : ia[2];
+        idx[c] = z * 64u + y * 8u + x;
+        w[c] = ((c & 1) ? nl[0] : 1.0f - nl[0]) * ((c & 2) ? nl[1] : 1.0f - nl[1]) * ((c & 4) ? nl[2] : 1.0f - nl[2]);
+    }
+}
+
 // ---- phase function: MiePhase, src/KernelSampler.cpp:214-285 --------------
 // Tables staged in shared memory: pdf as float4 (r, g, b, -), red CDF.
 struct MieSmem {
@@ -725,8 +753,30 @@ __device__ __forceinline__ bool camera_ray(const DevParams &P, uint32_t px, uint
 // so such a collision counts for coverage but does not scatter.  td receives
 // the distance of the collision (or of the last leaf exit).
 enum : uint32_t { kTrackCollided = 0, kTrackEscaped = 1, kTrackCut = 2 };
+
+// A tracking visitor sees every collision decision that involved a density
+// lookup: the leaf's brick and box, the position, rho, the majorant and
+// whether the collision was real (rho / smax >= q).  The forward renderer's
+// visitor does nothing; the adjoint's accumulates gradients.
+struct NoVisit {
+    __device__ __forceinline__ void operator()(const float *, const float4 &, const float *, float, float, bool) const {}
+};
+
+template <class Visit>
+__device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
+                                            Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
+                                            const Visit &visit);
+
 __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
                                           Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
+    const NoVisit nv;
+    return track_v(S, P.sigma_e, ro, rd, g, depth, td_out, nstack, cnt, nv);
+}
+
+template <class Visit>
+__device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
+                                            Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
+                                            const Visit &visit) {
     Trav T;
     trav_init(T, S, ro, rd, cnt);
     ++cnt.vertices;
@@ -754,7 +804,7 @@ __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P,
             td = __uint_as_float((__float_as_uint(td) & ~1u) | (__float_as_uint(tra) & 1u));
             s0 = __uint_as_float(__float_as_uint(tr0) & 1u);
         }
-        const float denom = P.sigma_e * smax;
+        const float denom = sigma_e * smax;
         float sr = -dlog(g.uniform()) / denom;
         for (;;) {
             const float sc = s0 + sr;
@@ -771,7 +821,12 @@ __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P,
                 ++cnt.density_lookups;
             }
             const float q = g.uniform();
+            const bool looked = rm;
             rm = rm && (rho / smax < q);
+            if (looked) {
+                const float rc[3] = {ro[0] + rd[0] * td, ro[1] + rd[1] * td, ro[2] + rd[2] * td};
+                visit(brick, ce, rc, rho, smax, !rm);
+            }
             if (!rm) {
                 td_out = td;
                 return td < depth ? kTrackCollided : kTrackCut;
@@ -786,6 +841,19 @@ __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P,
     }
     td_out = td;
     return kTrackEscaped;
+}
+
+// DR_KERNEL_FINITE_PATHS: a path sample whose sun or sky sum is not finite is
+// dropped (the reference's sky term is 0/0 for a direction with rd.y == 0:
+// rd.x / rd.y is infinite and is multiplied by 0, src/kernel.cpp:338-342).
+__device__ __forceinline__ void drop_nonfinite(const DevParams &P, float4 &sun, float4 &sky) {
+    if (!P.finite_paths) return;
+    const bool ok = isfinite(sun.x) && isfinite(sun.y) && isfinite(sun.z) && isfinite(sky.x) && isfinite(sky.y) &&
+                    isfinite(sky.z);
+    if (!ok) {
+        sun = make_float4(0.0f, 0.0f, 0.0f, sun.w);
+        sky = make_float4(0.0f, 0.0f, 0.0f, sky.w);
+    }
 }
 
 // ---- one camera path sample: SampleVolume recursion as a loop --------------
@@ -855,6 +923,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
             rd[k] = srd[k];
         }
     }
+    drop_nonfinite(P, sun_acc, sky_acc);
 }
 
 // ---- one shadow-pass sample: RenderKernel::Shadow (src/kernel.cpp:569-607) ----

@@ -244,6 +244,9 @@ int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned
     d.w = p->w;
     d.h = p->h;
     d.depthcomp = (p->flags & DR_KERNEL_DEPTHCOMP) ? 1u : 0u;
+    d.finite_paths = (p->flags & DR_KERNEL_FINITE_PATHS) ? 1u : 0u;
+    if (p->flags & ~(DR_KERNEL_DEPTHCOMP | DR_KERNEL_FINITE_PATHS))
+        return need(false, DR_ERR_INVALID, "dr_set_params: unknown flags");
     {
         // RenderKernel::Shadow: zfar = (0,0,1,1) * projInv, clip_end = -zfar.z / zfar.w
         const float zz = p->proji[8 + 2] + p->proji[12 + 2], zw = p->proji[8 + 3] + p->proji[12 + 3];

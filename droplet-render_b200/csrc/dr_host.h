@@ -114,6 +114,10 @@ struct dr_ctx {
     dr::DevBuf<float4> tile_sun, tile_sky;
     dr::DevBuf<unsigned char> scratch;
     dr::DevBuf<dr::WorkQueue> work;
+    dr::DevBuf<uint32_t> leaf_nodes;  // ids of the leaf nodes (majorant updates)
+    dr::DevBuf<float> grad_copies;    // adjoint: spread copies of the brick-pool gradient
+    dr::DevBuf<double> albedo_slots;  // adjoint: partial sums of the albedo gradient (kept zeroed)
+    uint32_t n_leaf_nodes = 0;
     bool use_grid = true;
     dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u};
     std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)

@@ -57,6 +57,7 @@ struct DevParams {
     uint32_t w, h;
     const float *depth;       // w*h or null
     uint32_t depthcomp;       // KERNEL_DEPTHCOMP: camera rays stop at depth
+    uint32_t finite_paths;    // a path whose contribution is not finite adds nothing
     float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
 };
 

@@ -259,7 +259,9 @@ __device__ __forceinline__ void begin_segment(PathLane<WALK> &L, const DevScene 
 }
 
 template <bool WALK>
-__device__ __forceinline__ void finish_path(PathLane<WALK> &L, const TileArgs &A, float4 *sun_out, float4 *sky_out) {
+__device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &P, const TileArgs &A, float4 *sun_out,
+                                            float4 *sky_out) {
+    drop_nonfinite(P, L.sun, L.sky);
     const bool any = (L.sun.x != 0.0f) | (L.sun.y != 0.0f) | (L.sun.z != 0.0f) | (L.sun.w != 0.0f) |
                      (L.sky.x != 0.0f) | (L.sky.y != 0.0f) | (L.sky.z != 0.0f) | (L.sky.w != 0.0f);
     if (any) {
@@ -388,12 +390,12 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
             L.sky.y = L.sky.y + L.T[1] * sky.y;
             L.sky.z = L.sky.z + L.T[2] * sky.z;
         }
-        finish_path(L, A, sun_out, sky_out);
+        finish_path(L, P, A, sun_out, sky_out);
         state = kFetch;
         return;
     }
     if (L.esc == kTrackCut || L.r >= P.scattevs) {
-        finish_path(L, A, sun_out, sky_out);
+        finish_path(L, P, A, sun_out, sky_out);
         state = kFetch;
         return;
     }
@@ -708,6 +710,307 @@ __global__ void probe_transmittance_kernel(DevScene S, DevParams P, const float 
     atomicAdd(&escapes[r], (unsigned long long)esc);
 }
 
+// ---- path-replay adjoint -------------------------------------------------------------
+// Gradient of a loss L(image) with respect to the brick samples and the
+// single-scatter albedo, given delta = dL/d(image sums) per pixel.  Delta
+// tracking decides each tentative collision with P(real) = rho/smax; with the
+// majorant held fixed the estimator's expectation depends on rho only through
+// these decisions, so (score-function form)
+//   dE[C]/dv = E[ sum_decisions C_after * dlog P(decision)/dv ],
+//   dlog P/dv = (drho/dv) / rho   (real),   -(drho/dv) / (smax - rho)   (null),
+// with drho/dv the trilinear weight of sample v.  C_after is the part of the
+// path's contribution that the decision can change: for a decision on the
+// camera or continuation segment r, everything the path adds from segment r
+// on (its total minus what it added before); on a shadow segment, that
+// segment's next-event contribution.  The albedo f enters each contribution as
+// f^m (m = scattering events before it): dC/df = sum m * c / f.
+// Each path is replayed from its random stream twice, as in path replay
+// backpropagation: pass 1 recomputes its total contribution, pass 2 replays the
+// same decisions and scatters gradients.  No per-path tape is stored; a shadow
+// segment is tracked once to learn whether it escapes and, if it did, again
+// from the saved stream state to scatter.
+
+struct ScatterVisit {
+    float w;  // dL/dC_after of the current segment
+    float *grad;
+    const float *bricks;
+    __device__ __forceinline__ void operator()(const float *brick, const float4 &ce, const float *rc, float rho,
+                                               float smax, bool real) const {
+        if (w == 0.0f) return;
+        float sc;
+        if (real) {
+            if (!(rho > 0.0f)) return;
+            sc = w / rho;
+        } else {
+            const float d = smax - rho;
+            if (!(d > 0.0f)) return;
+            sc = (0.0f - w) / d;
+        }
+        uint32_t idx[8];
+        float wt[8];
+        voxel_weights(rc, ce, idx, wt);
+        float *gb = grad + (brick - bricks);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (wt[c] != 0.0f) atomicAdd(gb + idx[c], sc * wt[c]);
+    }
+};
+
+// One copy of the tracking loop per visitor for the whole adjoint (each call
+// site inlining it would multiply the code the warps fetch).
+__device__ __noinline__ uint32_t track_plain(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
+                                             float depth, float &td, uint32_t *nstack, Count &cnt) {
+    const NoVisit nv;
+    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, nv);
+}
+
+__device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, const float *ro, const float *rd,
+                                               Rng &g, float depth, float &td, uint32_t *nstack, Count &cnt,
+                                               const ScatterVisit &sv) {
+    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, sv);
+}
+
+struct PathTotals {
+    float3 sun, sky;    // contribution of the path to the sun and sky sums
+    float3 asun, asky;  // sum over contributions of (scattering events before it) * contribution
+};
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float dot3f(const float3 a, const float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Pass 1 (SCATTER = false): fills tot.  Pass 2: scatters with tot known.
+template <bool SCATTER>
+__device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
+                                             uint32_t py, uint64_t seed, uint64_t sample, float3 dsun, float3 dsky,
+                                             PathTotals &tot, float *grad, uint32_t *nstack) {
+    float ro[3], rd[3];
+    if (!camera_ray(P, px, py, ro, rd)) return;
+    Count cnt;
+    cnt.zero();
+    Rng g = rng_seed(seed, (uint64_t)py * P.w + px, sample);
+    const float f = P.albedo;
+    float T0 = 1.0f, T1 = 1.0f, T2 = 1.0f;
+    const float depth0 = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
+    float3 acc_sun = f3(0.f, 0.f, 0.f), acc_sky = acc_sun, a_sun = acc_sun, a_sky = acc_sun;
+    ScatterVisit vis{0.0f, grad, S.bricks};
+    for (uint32_t r = 0;; ++r) {
+        float td;
+        uint32_t res;
+        if constexpr (SCATTER) {
+            vis.w = dot3f(dsun, f3(tot.sun.x - acc_sun.x, tot.sun.y - acc_sun.y, tot.sun.z - acc_sun.z)) +
+                    dot3f(dsky, f3(tot.sky.x - acc_sky.x, tot.sky.y - acc_sky.y, tot.sky.z - acc_sky.z));
+            res = track_scatter(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
+        } else {
+            res = track_plain(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+        }
+        if (res == kTrackCut) break;
+        if (res == kTrackEscaped) {
+            if (r > 0) {
+                const bool hit = sun_hit(P, rd);
+                const float3 cs = f3(T0 * (hit ? P.sun_color[0] : 0.0f), T1 * (hit ? P.sun_color[1] : 0.0f),
+                                     T2 * (hit ? P.sun_color[2] : 0.0f));
+                const float3 sk = sky_eval(P, rd);
+                const float3 ck = f3(T0 * sk.x, T1 * sk.y, T2 * sk.z);
+                const float m = (float)r;
+                acc_sun = f3(acc_sun.x + cs.x, acc_sun.y + cs.y, acc_sun.z + cs.z);
+                acc_sky = f3(acc_sky.x + ck.x, acc_sky.y + ck.y, acc_sky.z + ck.z);
+                a_sun = f3(a_sun.x + m * cs.x, a_sun.y + m * cs.y, a_sun.z + m * cs.z);
+                a_sky = f3(a_sky.x + m * ck.x, a_sky.y + m * ck.y, a_sky.z + m * ck.z);
+            }
+            break;
+        }
+        if (r >= P.scattevs) break;
+        float srd[3], lrd[3], rc[3];
+        const float u1 = g.uniform(), u2 = g.uniform();
+        mie_sample(M, rd, u1, u2, srd);
+        const float u3 = g.uniform(), u4 = g.uniform();
+        sun_sample(P, u3, u4, lrd);
+        const float3 p1 = mie_eval_rgb(M, dot3(srd, rd));
+        const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
+        const float3 p3 = mie_eval_rgb(M, dot3(lrd, rd));
+        const float q1 = sun_hit(P, srd) ? P.sun_pdf : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+        const Rng g0 = g;
+        float tds;
+        if (track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped) {
+            const bool hit = sun_hit(P, lrd);
+            const float3 cn = f3((T0 * ((p3.x / (p3.x + p2)) * f)) * (hit ? P.sun_color[0] : 0.0f),
+                                 (T1 * ((p3.y / (p3.y + p2)) * f)) * (hit ? P.sun_color[1] : 0.0f),
+                                 (T2 * ((p3.z / (p3.z + p2)) * f)) * (hit ? P.sun_color[2] : 0.0f));
+            if constexpr (SCATTER) {
+                ScatterVisit sv{dot3f(dsun, cn), grad, S.bricks};
+                if (sv.w != 0.0f) {
+                    Rng g1 = g0;  // the same draws again: ends in the state g already holds
+                    float t2;
+                    (void)track_scatter(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
+                }
+            }
+            const float m = (float)(r + 1);
+            acc_sun = f3(acc_sun.x + cn.x, acc_sun.y + cn.y, acc_sun.z + cn.z);
+            a_sun = f3(a_sun.x + m * cn.x, a_sun.y + m * cn.y, a_sun.z + m * cn.z);
+        }
+        T0 = T0 * ((p1.x / (p1.x + q1)) * f);
+        T1 = T1 * ((p1.y / (p1.y + q1)) * f);
+        T2 = T2 * ((p1.z / (p1.z + q1)) * f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ro[k] = rc[k];
+            rd[k] = srd[k];
+        }
+    }
+    if constexpr (!SCATTER) {
+        tot.sun = acc_sun;
+        tot.sky = acc_sky;
+        tot.asun = a_sun;
+        tot.asky = a_sky;
+    }
+}
+
+// Warp-wide sum of one float added to one of kSlots double accumulators
+// (slot = global warp index % kSlots; no block barrier, so a block's warps
+// retire independently); the slots are summed into the output afterwards.
+constexpr uint32_t kSlots = 1024;
+__device__ __forceinline__ void warp_add(float v, double *slots) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    if ((threadIdx.x & 31) == 0 && v != 0.0f) {
+        const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        atomicAdd(&slots[w % kSlots], (double)v);
+    }
+}
+
+__global__ void sum_slots_kernel(double *out, double *slots) {
+    __shared__ double part[32];
+    double v = 0.0;
+    for (uint32_t k = threadIdx.x; k < kSlots; k += blockDim.x) {
+        v += slots[k];
+        slots[k] = 0.0;
+    }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (uint32_t k = 0; k < blockDim.x / 32; ++k) s += part[k];
+        *out += s;
+    }
+}
+
+// One thread per (pixel, sample), the render kernel's layout; delta images in
+// tile layout (tw x th float4, rgb used).  Gradients go to copy
+// blockIdx.x % copies of the brick-pool gradient (grad + copy * stride): the
+// surface samples every path meets first are hit by all warps at once, and
+// spreading them over copies divides the conflicts on each address; the copies
+// are summed afterwards.
+__global__ void __launch_bounds__(kRenderBlock) adjoint_tile_kernel(DevScene S, DevParams P, TileArgs A,
+                                                                    const void *mie_pack, const float4 *dsun,
+                                                                    const float4 *dsky, float *grad,
+                                                                    uint32_t copies, size_t stride,
+                                                                    double *albedo_slots, DevCounters *C) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
+    uint32_t nstack[kMaxDepth];
+    const uint64_t gi = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
+    float galb = 0.0f;
+    grad += (size_t)(blockIdx.x % copies) * stride;
+    if (staged && gi < A.n_paths) {
+        const uint64_t pl = gi / A.spp;
+        const uint32_t s = (uint32_t)(gi - pl * A.spp);
+        const uint32_t pix = (uint32_t)pl;
+        const uint32_t i = pix % A.cols, j = pix / A.cols;
+        const size_t o = (size_t)j * A.tw + i;
+        const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
+        const float3 dsun3 = f3(ds.x, ds.y, ds.z), dsky3 = f3(dk.x, dk.y, dk.z);
+        if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
+            PathTotals tot{};
+            adjoint_pass<false>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, grad,
+                                nstack);
+            // a path whose contribution is not finite (the sky term's 0/0 for
+            // rd.y == 0) is left out of the gradient
+            const bool ok = isfinite(tot.sun.x) && isfinite(tot.sun.y) && isfinite(tot.sun.z) &&
+                            isfinite(tot.sky.x) && isfinite(tot.sky.y) && isfinite(tot.sky.z);
+            if (ok) {
+                adjoint_pass<true>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, grad,
+                                   nstack);
+                galb = (dot3f(dsun3, tot.asun) + dot3f(dsky3, tot.asky)) / P.albedo;
+            }
+        }
+    }
+    if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
+    warp_add(galb, albedo_slots);
+}
+
+// out[k] += sum over copies c of src[c * stride + k].
+__global__ void sum_copies_kernel(float *out, const float *src, uint32_t copies, size_t stride) {
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < stride; k += (size_t)gridDim.x * blockDim.x) {
+        float v = 0.0f;
+        for (uint32_t c = 0; c < copies; ++c) v += src[(size_t)c * stride + k];
+        out[k] += v;
+    }
+}
+
+// Gradient of sum_r w_r T_r (T_r: delta-tracking transmittance of ray r over
+// nsamp samples, streams (seed, r, s) as probe_transmittance_kernel) with
+// respect to the brick samples: an escaped sample replays its null decisions
+// with weight w_r / nsamp; a collided one contributes nothing.
+__global__ void adjoint_transmittance_kernel(DevScene S, DevParams P, const float *ro, const float *rd,
+                                             const float *wr, uint32_t n_rays, uint64_t nsamp, uint64_t seed,
+                                             float *grad, unsigned long long *escapes) {
+    const uint64_t chunks = (nsamp + 63) / 64;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= chunks * n_rays) return;
+    const uint32_t r = (uint32_t)(t / chunks);
+    const uint64_t c = t - (uint64_t)r * chunks;
+    const float o[3] = {ro[3 * r], ro[3 * r + 1], ro[3 * r + 2]}, d[3] = {rd[3 * r], rd[3 * r + 1], rd[3 * r + 2]};
+    Count cnt;
+    cnt.zero();
+    uint32_t nstack[kMaxDepth];
+    uint32_t esc = 0;
+    ScatterVisit sv{wr[r] / (float)nsamp, grad, S.bricks};
+    const uint64_t s1 = (c + 1) * 64 < nsamp ? (c + 1) * 64 : nsamp;
+    for (uint64_t s = c * 64; s < s1; ++s) {
+        Rng g = rng_seed(seed, r, s);
+        const Rng g0 = g;
+        float td;
+        if (track_plain(S, P.sigma_e, o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped) {
+            ++esc;
+            Rng g1 = g0;
+            (void)track_scatter(S, P.sigma_e, o, d, g1, 3.402823466e+38f, td, nstack, cnt, sv);
+        }
+    }
+    atomicAdd(&escapes[r], (unsigned long long)esc);
+}
+
+// Majorants after a brick update: max over the leaf's samples, floor 0.01
+// (src/scene.cpp:889-904), times scale (>= 1: headroom that lets samples grow
+// while the majorant stays fixed); a leaf whose majorant was 0 (never
+// resampled) keeps 0.
+__global__ void leaf_majorant_kernel(float4 *leaf, const uint32_t *leaf_nodes, uint32_t n_leafnodes,
+                                     const float *bricks, float scale) {
+    const uint32_t i = blockIdx.x;
+    if (i >= n_leafnodes) return;
+    const uint32_t node = leaf_nodes[i];
+    float4 meta = leaf[2 * (size_t)node + 1];
+    const float *b = bricks + (size_t)__float_as_uint(meta.y) * kBrick;
+    float m = 0.0f;
+    for (uint32_t k = threadIdx.x; k < kBrick; k += blockDim.x) m = fmaxf(m, b[k]);
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
+    __shared__ float wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t k = 1; k < (blockDim.x + 31) / 32; ++k) m = fmaxf(m, wm[k]);
+        wm[0] = fmaxf(m, wm[0]);
+        if (meta.x != 0.0f) meta.x = fmaxf(wm[0], 0.01f) * scale;
+        leaf[2 * (size_t)node + 1] = meta;
+    }
+}
+
 // ---- transmittance without allocation ----------------------------------------------
 // Scratch of the allocation-free entry point: one escape counter per ray in a
 // file-scope device array (512 KB on every GPU that loads the library, for the
@@ -901,6 +1204,54 @@ cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, co
     if (blocks == 0) return cudaSuccess;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
     probe_transmittance_kernel<<<(unsigned)blocks, 128, 0, st>>>(S, P, ro, rd, n_rays, nsamp, seed, escapes);
+    return cudaGetLastError();
+}
+
+
+uint32_t adjoint_slots() { return kSlots; }
+
+cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
+                                uint32_t copies, double *grad_albedo, double *slots, DevCounters *C,
+                                cudaStream_t st) {
+    if (A.n_paths == 0) return cudaSuccess;
+    const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
+    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    const size_t stride = (size_t)S.n_leaves * kBrick;
+    const bool spread = copies > 1 && copies_buf;
+    if (spread) {
+        cudaError_t e = cudaMemsetAsync(copies_buf, 0, sizeof(float) * stride * copies, st);
+        if (e != cudaSuccess) return e;
+    }
+    adjoint_tile_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(
+        S, P, A, mie_pack, dsun, dsky, spread ? copies_buf : grad, spread ? copies : 1u, stride, slots, C);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (spread) {
+        sum_copies_kernel<<<592, 256, 0, st>>>(grad, copies_buf, copies, stride);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    sum_slots_kernel<<<1, 256, 0, st>>>(grad_albedo, slots);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
+                                         const float *wr, uint32_t n_rays, uint64_t nsamp, uint64_t seed, float *grad,
+                                         unsigned long long *escapes, cudaStream_t st) {
+    const uint64_t threads = ((nsamp + 63) / 64) * n_rays;
+    const uint64_t blocks = (threads + 127) / 128;
+    if (blocks == 0) return cudaSuccess;
+    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    adjoint_transmittance_kernel<<<(unsigned)blocks, 128, 0, st>>>(S, P, ro, rd, wr, n_rays, nsamp, seed, grad,
+                                                                   escapes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_majorants(float4 *leaf, const uint32_t *leaf_nodes, uint32_t n_leafnodes, const float *bricks,
+                                  float scale, cudaStream_t st) {
+    if (n_leafnodes == 0) return cudaSuccess;
+    leaf_majorant_kernel<<<n_leafnodes, 128, 0, st>>>(leaf, leaf_nodes, n_leafnodes, bricks, scale);
     return cudaGetLastError();
 }
 

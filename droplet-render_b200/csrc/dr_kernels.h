@@ -37,6 +37,24 @@ cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, co
                                        uint32_t n_rays, uint64_t nsamp, uint64_t seed, unsigned long long *escapes,
                                        cudaStream_t st);
 
+// Path-replay adjoint of a tile (delta images in tile layout) and of a set of
+// transmittance rays; gradients accumulate into grad (brick-pool layout).
+// copies > 1: gradients are first spread over `copies` zeroed copies in
+// copies_buf (copies * n_leaves * 512 floats), then summed into grad.
+// The albedo gradient is gathered in adjoint_slots() zeroed doubles (slots),
+// then added to *grad_albedo (and the slots zeroed again).
+cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
+                                uint32_t copies, double *grad_albedo, double *slots, DevCounters *C,
+                                cudaStream_t st);
+uint32_t adjoint_slots();
+cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
+                                         const float *wr, uint32_t n_rays, uint64_t nsamp, uint64_t seed, float *grad,
+                                         unsigned long long *escapes, cudaStream_t st);
+// Leaf majorants of the listed leaf nodes recomputed from the brick pool.
+cudaError_t launch_leaf_majorants(float4 *leaf, const uint32_t *leaf_nodes, uint32_t n_leafnodes, const float *bricks,
+                                  float scale, cudaStream_t st);
+
 // Allocation-free transmittance: scratch in a file-scope device array.
 uint32_t noalloc_max_rays();
 cudaError_t noalloc_scratch(int device, unsigned long long **out);

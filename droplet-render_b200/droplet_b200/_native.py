@@ -25,6 +25,7 @@ DR_NONE = 0xFFFFFFFF
 DR_PHASE_MIE_REFERENCE = 0
 DR_PHASE_MIE_EXACT = 1
 DR_KERNEL_DEPTHCOMP = 0x1
+DR_KERNEL_FINITE_PATHS = 0x2
 
 DR_PROBE_MIE_EVAL_RGB = 0
 DR_PROBE_MIE_SAMPLE = 1
@@ -154,6 +155,17 @@ SIGNATURES = {
          C.c_void_p],
     ),
     "dr_synchronize": (C.c_int, [C.c_void_p]),
+    "dr_set_bricks_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]),
+    "dr_get_majorants": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dr_adjoint_tile_async": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
+         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
+    "dr_adjoint_transmittance": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p],
+    ),
     "dr_batch_create": (
         C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "dr_batch_destroy": (C.c_int, [C.c_void_p]),

@@ -50,6 +50,7 @@ class RenderSettings:
     h: int
     depth: np.ndarray | None = None   # depth texture: distance along each camera ray (shadow pass, compositing)
     depthcomp: bool = False           # KERNEL_DEPTHCOMP: camera rays stop at the depth texture
+    finite_paths: bool = False        # a path sample with a non-finite sum adds nothing (DR_KERNEL_FINITE_PATHS)
     phase_mode: int = N.DR_PHASE_MIE_REFERENCE
     _keep: list = field(default_factory=list, repr=False)
 
@@ -78,7 +79,7 @@ class RenderSettings:
             p.depth = d.ctypes.data
         else:
             p.depth = None
-        p.flags = N.DR_KERNEL_DEPTHCOMP if self.depthcomp else 0
+        p.flags = (N.DR_KERNEL_DEPTHCOMP if self.depthcomp else 0) | (N.DR_KERNEL_FINITE_PATHS if self.finite_paths else 0)
         return p
 
 
@@ -175,6 +176,34 @@ class Renderer:
         t = N.DrTuning()
         N.check(N.lib().dr_get_tuning(self._ctx, C.byref(t)))
         return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal), int(t.tile))
+
+    # ---- differentiable rendering -------------------------------------------------
+    def set_bricks_dev(self, bricks_ptr: int, n_leaves: int, majorant_scale: float = 1.0, stream_ptr: int = 0):
+        """Replaces the brick pool with a device array (n_leaves x 512 float32)."""
+        N.check(N.lib().dr_set_bricks_dev(self._ctx, C.c_void_p(bricks_ptr), int(n_leaves), float(majorant_scale),
+                                          C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def majorants(self, n_nodes: int) -> np.ndarray:
+        out = np.zeros(n_nodes, np.float32)
+        N.check(N.lib().dr_get_majorants(self._ctx, out.ctypes.data))
+        return out
+
+    def adjoint_tile_async(self, x0, y0, tw, th, spp, seed, sample_base, dsun_ptr: int, dsky_ptr: int, grad_ptr: int,
+                           galb_ptr: int, stream_ptr: int = 0):
+        N.check(N.lib().dr_adjoint_tile_async(self._ctx, x0, y0, tw, th, spp, int(seed), int(sample_base),
+                                              C.c_void_p(dsun_ptr), C.c_void_p(dsky_ptr), C.c_void_p(grad_ptr),
+                                              C.c_void_p(galb_ptr), C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def adjoint_transmittance(self, ro, rd, weights, nsamp: int, seed: int, n_leaves: int):
+        """(d sum_r w_r T_r / d brick samples (n_leaves, 512), T per ray) on the GPU."""
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1)
+        w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        grad = np.zeros(n_leaves * 512, np.float32)
+        T = np.zeros(len(w), np.float64)
+        N.check(N.lib().dr_adjoint_transmittance(self._ctx, ro.ctypes.data, rd.ctypes.data, w.ctypes.data, len(w),
+                                                 int(nsamp), int(seed), grad.ctypes.data, T.ctypes.data))
+        return grad.reshape(n_leaves, 512), T
 
     def counters(self) -> dict:
         c = N.DrCounters()

@@ -84,9 +84,11 @@ typedef struct {
     float proji[16];               /* inverse projection matrix, rows r[0..3] */
     uint32_t w, h;                 /* full image size */
     const float *depth;            /* optional w*h depth texture (distance along the camera ray), or NULL */
-    uint32_t flags;                /* DR_KERNEL_DEPTHCOMP: camera rays stop at depth (src/kernel.h:4) */
+    uint32_t flags;                /* DR_KERNEL_* below */
 } dr_render_params;
-#define DR_KERNEL_DEPTHCOMP 0x1u
+#define DR_KERNEL_DEPTHCOMP 0x1u     /* camera rays stop at depth (src/kernel.h:4) */
+#define DR_KERNEL_FINITE_PATHS 0x2u  /* a path sample whose sun or sky sum is not finite adds nothing (the
+                                        reference's sky term is 0/0 for rd.y == 0, src/kernel.cpp:338-342) */
 
 /* In-kernel counters accumulated over all launches since the last reset. */
 typedef struct {
@@ -209,6 +211,35 @@ int dr_batch_output(dr_batch *batch, uint32_t view, float **sun_dev, float **sky
 int dr_batch_read(dr_batch *batch, uint32_t view, float *sun_out, float *sky_out);
 /* Path indices per launch (tile padding included) and launches so far. */
 int dr_batch_info(dr_batch *batch, uint64_t *n_paths, uint64_t *launches);
+
+/* ---- differentiable rendering (path-replay adjoint) -------------------------
+ * No reference counterpart: the reference renders only (src/kernel.cpp).
+ * The parameters are the brick samples (n_leaves * 512 floats, the scene's
+ * FOG pool) and the single-scatter albedo sigma_s / (sigma_s + sigma_a). */
+/* Replaces the scene's brick pool with a device array (device-to-device copy).
+ * majorant_scale >= 1 recomputes every leaf majorant as majorant_scale x the
+ * brick maximum, floor 0.01 (1: the reference's rule, src/scene.cpp:889-904;
+ * leaves whose majorant is 0 keep 0); 0 keeps the current majorants, which
+ * must then bound the new samples. */
+int dr_set_bricks_dev(dr_ctx *ctx, const float *bricks_dev, uint32_t n_leaves, float majorant_scale, void *stream);
+/* Majorant of every node (0 for internal nodes), host buffer of n_nodes floats. */
+int dr_get_majorants(dr_ctx *ctx, float *out);
+/* Path-replay adjoint of dr_render_tile(_async) with the same arguments:
+ * given dsun_dev / dsky_dev = dL/d(tile sums) (tw*th float4 each, rgb used),
+ * ADDS dL/d(brick sample) into grad_bricks_dev (n_leaves * 512 floats) and
+ * dL/d(albedo) into *grad_albedo_dev.  Each path is replayed from its own
+ * random stream (no stored tape): unbiased for the expected image, with the
+ * leaf majorants held fixed.  A path whose contribution is not finite is
+ * left out.  Enqueued on stream (NULL = context stream). */
+int dr_adjoint_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
+                          uint64_t seed, uint64_t sample_base, const float *dsun_dev, const float *dsky_dev,
+                          float *grad_bricks_dev, double *grad_albedo_dev, void *stream);
+/* Transmittance of n rays (ro, rd: 3n floats) by delta tracking over nsamp
+ * samples (streams (seed, ray, sample)) and the gradient of
+ * sum_r weights[r] * T_r with respect to the brick samples (host buffers:
+ * grad_bricks n_leaves * 512 floats, transmittance n doubles or NULL). */
+int dr_adjoint_transmittance(dr_ctx *ctx, const float *ro, const float *rd, const float *weights, uint32_t n,
+                             uint64_t nsamp, uint64_t seed, float *grad_bricks, double *transmittance);
 
 /* ---- counters ------------------------------------------------------------ */
 int dr_get_counters(dr_ctx *ctx, dr_counters *out);

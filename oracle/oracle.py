@@ -33,7 +33,7 @@ class OrcParams(C.Structure):
         ("mie_pdf", C.c_void_p), ("mie_cdf", C.c_void_p), ("mie_n", C.c_uint32),
         ("viewi", C.c_float * 16), ("proji", C.c_float * 16), ("w", C.c_uint32), ("h", C.c_uint32),
         ("depth", C.c_float), ("depth_map", C.c_void_p), ("depthcomp", C.c_uint32),
-        ("phase_mode", C.c_uint32), ("mie_exact", C.c_void_p),
+        ("phase_mode", C.c_uint32), ("mie_exact", C.c_void_p), ("finite_paths", C.c_uint32),
     ]
 
 
@@ -83,6 +83,11 @@ class Port:
         L.orc_render_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                          C.c_uint64, C.c_uint64, vp, vp, C.POINTER(OrcCounters), C.c_int]
         L.orc_render_tile_mt.restype = C.c_int
+        L.orc_adjoint_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
+                                          C.c_uint64, C.c_uint64, vp, vp, vp, vp, C.c_int]
+        L.orc_adjoint_tile_mt.restype = C.c_int
+        L.orc_adjoint_transmittance.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), vp, vp, vp, u32,
+                                                C.c_uint64, C.c_uint64, vp, vp]
         L.orc_mie_exact_table.argtypes = [vp, u32, vp]
         L.orc_mie_exact_dirs.argtypes = [vp, u32, vp, u32, vp, vp]
         L.orc_shadow_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
@@ -162,6 +167,7 @@ class Port:
             keep.append(dm)
             P.depth_map = dm.ctypes.data
             P.depthcomp = 1 if cfg.get("depthcomp") else 0
+        P.finite_paths = 1 if cfg.get("finite_paths") else 0
         if cfg.get("phase_mode", 0) == 1:
             tab = Port().mie_exact_table(pdf)
             keep.append(tab)
@@ -199,6 +205,43 @@ class Port:
         self.L.orc_shadow_tile_mt(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base, _p(out),
                                   C.byref(cnt), nt)
         return out, cnt.as_dict()
+
+    def adjoint_tile(self, S, P, x0, y0, tw, th, spp, seed, sample_base, dsun, dsky, threads=0):
+        """(d loss / d brick samples (n_leaves, 512) float64, d loss / d albedo) for
+        dsun/dsky = dL/d(tile sums), shape (th, tw, 4)."""
+        dsun = np.ascontiguousarray(dsun, np.float32)
+        dsky = np.ascontiguousarray(dsky, np.float32)
+        grad = np.zeros(S.n_leaves * 512, np.float64)
+        galb = np.zeros(1, np.float64)
+        nt = threads if threads > 0 else (os.cpu_count() or 1)
+        rc = self.L.orc_adjoint_tile_mt(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base, _p(dsun),
+                                        _p(dsky), _p(grad), _p(galb), nt)
+        if rc != 0:
+            raise MemoryError("orc_adjoint_tile_mt")
+        return grad.reshape(-1, 512), float(galb[0])
+
+    def adjoint_transmittance(self, S, P, ro, rd, w, nsamp, seed):
+        ro = np.ascontiguousarray(ro, np.float32)
+        rd = np.ascontiguousarray(rd, np.float32)
+        w = np.ascontiguousarray(w, np.float32)
+        grad = np.zeros(S.n_leaves * 512, np.float64)
+        T = np.zeros(len(w), np.float64)
+        self.L.orc_adjoint_transmittance(C.byref(S), C.byref(P), _p(ro), _p(rd), _p(w), len(w), nsamp, seed,
+                                         _p(grad), _p(T))
+        return grad.reshape(-1, 512), T
+
+    def optical_depth_grad(self, S, ro, rd, tmax=1e30):
+        """FP64 d(optical depth)/d(brick samples) of one ray (quadrature oracle)."""
+        ro = np.ascontiguousarray(ro, np.float64)
+        rd = np.ascontiguousarray(rd, np.float64)
+        grad = np.zeros(S.n_leaves * 512, np.float64)
+        self.L.orc_optical_depth_grad(C.byref(S), _p(ro), _p(rd), tmax, _p(grad))
+        return grad.reshape(-1, 512)
+
+    def optical_depth(self, S, ro, rd, tmax=1e30):
+        ro = np.ascontiguousarray(ro, np.float64)
+        rd = np.ascontiguousarray(rd, np.float64)
+        return float(self.L.orc_optical_depth(C.byref(S), _p(ro), _p(rd), tmax))
 
     def render_path(self, S, P, px, py, seed, sample):
         a = np.zeros(4, np.float32)

@@ -59,6 +59,7 @@ typedef struct {
     uint32_t depthcomp;    /* KERNEL_DEPTHCOMP: camera rays stop at depth_map */
     uint32_t phase_mode;   /* 0 = the reference's sampler, 1 = exact inverse CDF */
     const float *mie_exact;/* exact-mode table (orc_mie_exact_table), 8 n + 4 floats */
+    uint32_t finite_paths; /* a path whose sun or sky sum is not finite adds nothing */
 } orc_params;
 
 typedef struct {
@@ -132,6 +133,15 @@ int orc_shadow_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uin
                        int nthreads);
 void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
                      uint64_t sample, float out[4], orc_counters *cnt);
+/* Path-replay adjoint of orc_render_tile (the GPU adjoint's algorithm):
+ * adds dL/d(brick sample) to grad (doubles) and dL/d(albedo) to *galb for
+ * dsun/dsky = dL/d(tile sums) (tw*th float4). */
+int orc_adjoint_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                        uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
+                        double *grad, double *galb, int nthreads);
+/* Gradient of sum_r w_r T_r (delta-tracking transmittance over nsamp samples). */
+void orc_adjoint_transmittance(const orc_scene *S, const orc_params *P, const float *ro, const float *rd,
+                               const float *wr, uint32_t n, uint64_t nsamp, uint64_t seed, double *grad, double *T);
 void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
                      uint64_t sample, float out_sun[4], float out_sky[4], orc_counters *cnt);
 

@@ -30,8 +30,21 @@ int orc_trav_next(void *T, const orc_node *nodes, uint32_t *node, float *tr0, fl
 
 static inline float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
+/* Visitor of the collision decisions that involved a density lookup (the
+ * adjoint's gradient scatter); NULL for rendering. */
+typedef void (*orc_visit_fn)(void *ctx, const float *brick, const float ce[4], const float rc[3], float rho,
+                             float smax, int real);
+
+static int track_depth_v(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], orc_rng *g,
+                         float depth, float *td_out, orc_counters *cnt, orc_visit_fn visit, void *vctx);
+
 static int track_depth(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], orc_rng *g,
                        float depth, float *td_out, orc_counters *cnt) {
+    return track_depth_v(S, P, ro, rd, g, depth, td_out, cnt, 0, 0);
+}
+
+static int track_depth_v(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], orc_rng *g,
+                         float depth, float *td_out, orc_counters *cnt, orc_visit_fn visit, void *vctx) {
     const float sigma_e = P->sigma_a + P->sigma_s;
     const uint32_t N = S->lvoxc, lv3 = N * N * N;
     _Alignas(16) unsigned char tbuf[2048];
@@ -79,7 +92,13 @@ static int track_depth(const orc_scene *S, const orc_params *P, const float ro[3
                 if (cnt) cnt->density_lookups++;
             }
             const float q = orc_rng_uniform(g);
+            const int looked = rm;
             rm = rm && (rho / smax < q);
+            if (looked && visit) {
+                float rc[3];
+                for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+                visit(vctx, brick, o->ce, rc, rho, smax, !rm);
+            }
             if (!rm) {
                 /* src/kernel.cpp:214-217, 370-384: the lane's mask mm = td < depth
                  * is re-evaluated on the next leaf step; alpha is taken from rm
@@ -156,6 +175,14 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
             rd[k] = srd[k];
         }
         ++r;
+    }
+    /* the reference's sky term is 0/0 for rd.y == 0 (rd.x / rd.y times 0,
+     * src/kernel.cpp:338-342); with finite_paths such a sample adds nothing */
+    if (P->finite_paths) {
+        int ok = 1;
+        for (int k = 0; k < 3; ++k) ok = ok && isfinite(out_sun[k]) && isfinite(out_sky[k]);
+        if (!ok)
+            for (int k = 0; k < 3; ++k) out_sun[k] = out_sky[k] = 0.0f;
     }
 }
 
@@ -305,4 +332,243 @@ double orc_transmittance_mc(const orc_scene *S, const orc_params *P, const float
         esc += (uint64_t)track_depth(S, P, ro, rd, &g, FLT_MAX, &td, 0);
     }
     return (double)esc / (double)nsamp;
+}
+
+
+/* ---- path-replay adjoint ---------------------------------------------------------
+ * The same estimator gradient as the GPU's adjoint (score-function form over
+ * the delta-tracking decisions, majorants fixed; C_after weights; albedo via
+ * the count of f factors), with the same float operations, so per-path totals
+ * and scattered terms equal the GPU's; the gradient sums are doubles here. */
+
+/* corner offsets and trilinear weights of orc_sample_voxel_space */
+static void voxel_weights(const float p[3], const float ce[4], uint32_t N, uint32_t idx[8], float w[8]) {
+    const float nm1 = (float)N - 1.0f;
+    const float top = (float)(N - 1);
+    uint32_t ia[3], ib[3];
+    float nl[3];
+    for (int k = 0; k < 3; ++k) {
+        float ni = ((-0.5f * ((ce[k] - ce[3]) - p[k])) * nm1) / ce[3];
+        float nf = floorf(ni) > 0.0f ? floorf(ni) : 0.0f;
+        float nc = ceilf(ni) < nm1 ? ceilf(ni) : nm1;
+        nl[k] = ni - nf;
+        nc = nc < top ? nc : top;
+        nc = nc > 0.0f ? nc : 0.0f;
+        nf = nf < top ? nf : top;
+        nf = nf > 0.0f ? nf : 0.0f;
+        ia[k] = (uint32_t)nf;
+        ib[k] = (uint32_t)nc;
+    }
+    for (int c = 0; c < 8; ++c) {
+        uint32_t x = (c & 1) ? ib[0] : ia[0], y = (c & 2) ? ib[1] : ia[1], z = (c & 4) ? ib[2] : ia[2];
+        idx[c] = (z * N + y) * N + x;
+        w[c] = ((c & 1) ? nl[0] : 1.0f - nl[0]) * ((c & 2) ? nl[1] : 1.0f - nl[1]) * ((c & 4) ? nl[2] : 1.0f - nl[2]);
+    }
+}
+
+typedef struct {
+    float w;
+    double *grad;
+    const float *bricks;
+    uint32_t N;
+} scatter_ctx;
+
+static void scatter_visit(void *vctx, const float *brick, const float ce[4], const float rc[3], float rho, float smax,
+                          int real) {
+    scatter_ctx *c = (scatter_ctx *)vctx;
+    if (c->w == 0.0f) return;
+    float sc;
+    if (real) {
+        if (!(rho > 0.0f)) return;
+        sc = c->w / rho;
+    } else {
+        const float d = smax - rho;
+        if (!(d > 0.0f)) return;
+        sc = (0.0f - c->w) / d;
+    }
+    uint32_t idx[8];
+    float wt[8];
+    voxel_weights(rc, ce, c->N, idx, wt);
+    double *gb = c->grad + (brick - c->bricks);
+    for (int k = 0; k < 8; ++k)
+        if (wt[k] != 0.0f) gb[idx[k]] += (double)(sc * wt[k]);
+}
+
+static inline float dot3v(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* pass 0 fills tot[12] (sun, sky, m*sun, m*sky); pass 1 scatters with tot known */
+static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
+                         uint64_t sample, const float dsun[3], const float dsky[3], float tot[12], double *grad,
+                         int scatter) {
+    float ro[3], rd[3];
+    int inf;
+    orc_camera_ray(P, px, py, ro, rd, &inf);
+    if (!inf) return;
+    orc_rng g;
+    orc_rng_seed(&g, seed, (uint64_t)py * P->w + px, sample);
+    const float f = P->sigma_s / (P->sigma_a + P->sigma_s);
+    const float depth0 = (P->depth_map && P->depthcomp) ? P->depth_map[(size_t)py * P->w + px] : P->depth;
+    float T[3] = {1.0f, 1.0f, 1.0f};
+    float acc_sun[3] = {0, 0, 0}, acc_sky[3] = {0, 0, 0}, a_sun[3] = {0, 0, 0}, a_sky[3] = {0, 0, 0};
+    scatter_ctx sc = {0.0f, grad, S->bricks, S->lvoxc};
+    for (uint32_t r = 0;; ++r) {
+        float td;
+        int res;
+        if (scatter) {
+            float rs[3], rk[3];
+            for (int k = 0; k < 3; ++k) {
+                rs[k] = tot[k] - acc_sun[k];
+                rk[k] = tot[3 + k] - acc_sky[k];
+            }
+            sc.w = dot3v(dsun, rs) + dot3v(dsky, rk);
+            res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, scatter_visit, &sc);
+        } else {
+            res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, 0, 0);
+        }
+        if (res == 2) break;
+        if (res == 1) {
+            if (r > 0) {
+                float sun[3], sky[3];
+                orc_sun_eval(P, rd, sun);
+                orc_sky_eval(P, rd, sky);
+                const float m = (float)r;
+                for (int k = 0; k < 3; ++k) {
+                    const float cs = T[k] * sun[k], ck = T[k] * sky[k];
+                    acc_sun[k] = acc_sun[k] + cs;
+                    acc_sky[k] = acc_sky[k] + ck;
+                    a_sun[k] = a_sun[k] + m * cs;
+                    a_sky[k] = a_sky[k] + m * ck;
+                }
+            }
+            break;
+        }
+        if (r >= P->scattevs) break;
+        float srd[3], lrd[3], p1[3], p3[3], rc[3];
+        const float u1 = orc_rng_uniform(&g), u2 = orc_rng_uniform(&g);
+        if (P->phase_mode == 1) orc_mie_sample_exact(P, rd, u1, u2, srd);
+        else orc_mie_sample(P, rd, u1, u2, srd);
+        const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
+        orc_sun_sample(P, u3, u4, lrd);
+        orc_mie_eval_rgb(P, dot3(srd, rd), p1);
+        const float p2 = orc_sun_pdf(P, lrd);
+        orc_mie_eval_rgb(P, dot3(lrd, rd), p3);
+        const float q1 = orc_sun_pdf(P, srd);
+        for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
+        const orc_rng g0 = g;
+        float tds;
+        if (track_depth_v(S, P, rc, lrd, &g, FLT_MAX, &tds, 0, 0, 0) == 1) {
+            float sun[3], cn[3];
+            orc_sun_eval(P, lrd, sun);
+            for (int k = 0; k < 3; ++k) cn[k] = (T[k] * ((p3[k] / (p3[k] + p2)) * f)) * sun[k];
+            if (scatter) {
+                scatter_ctx sv = {dot3v(dsun, cn), grad, S->bricks, S->lvoxc};
+                if (sv.w != 0.0f) {
+                    orc_rng g1 = g0;
+                    float t2;
+                    (void)track_depth_v(S, P, rc, lrd, &g1, FLT_MAX, &t2, 0, scatter_visit, &sv);
+                }
+            }
+            const float m = (float)(r + 1);
+            for (int k = 0; k < 3; ++k) {
+                acc_sun[k] = acc_sun[k] + cn[k];
+                a_sun[k] = a_sun[k] + m * cn[k];
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            T[k] = T[k] * ((p1[k] / (p1[k] + q1)) * f);
+            ro[k] = rc[k];
+            rd[k] = srd[k];
+        }
+    }
+    if (!scatter) {
+        for (int k = 0; k < 3; ++k) {
+            tot[k] = acc_sun[k];
+            tot[3 + k] = acc_sky[k];
+            tot[6 + k] = a_sun[k];
+            tot[9 + k] = a_sky[k];
+        }
+    }
+}
+
+typedef struct {
+    const orc_scene *S;
+    const orc_params *P;
+    uint32_t x0, y0, tw, spp, cols, rows;
+    uint64_t seed, base;
+    const float *dsun, *dsky;
+    double *grad, galb;
+    int nthreads, tid;
+} adj_job;
+
+static void *adj_worker(void *arg) {
+    adj_job *J = (adj_job *)arg;
+    const float f = J->P->sigma_s / (J->P->sigma_a + J->P->sigma_s);
+    for (uint32_t j = (uint32_t)J->tid; j < J->rows; j += (uint32_t)J->nthreads)
+        for (uint32_t i = 0; i < J->cols; ++i) {
+            const float *ds = J->dsun + 4 * ((size_t)j * J->tw + i), *dk = J->dsky + 4 * ((size_t)j * J->tw + i);
+            if (dot3v(ds, ds) + dot3v(dk, dk) > 0.0f)
+                for (uint32_t s = 0; s < J->spp; ++s) {
+                    float tot[12] = {0};
+                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 0);
+                    int ok = 1;
+                    for (int k = 0; k < 6; ++k) ok = ok && isfinite(tot[k]);
+                    if (!ok) continue; /* non-finite contribution: left out of the gradient */
+                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 1);
+                    J->galb += (double)((dot3v(ds, tot + 6) + dot3v(dk, tot + 9)) / f);
+                }
+        }
+    return 0;
+}
+
+int orc_adjoint_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                        uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
+                        double *grad, double *galb, int nthreads) {
+    const size_t ng = (size_t)S->n_leaves * S->lvoxc * S->lvoxc * S->lvoxc;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 64) nthreads = 64;
+    adj_job jobs[64];
+    pthread_t ids[64];
+    for (int t = 0; t < nthreads; ++t) {
+        adj_job *J = &jobs[t];
+        memset(J, 0, sizeof(*J));
+        J->S = S; J->P = P; J->x0 = x0; J->y0 = y0; J->tw = tw; J->spp = spp;
+        J->cols = 2 * (tw / 2); J->rows = 2 * (th / 2); J->seed = seed; J->base = sample_base;
+        J->dsun = dsun; J->dsky = dsky; J->nthreads = nthreads; J->tid = t;
+        J->grad = t == 0 ? grad : (double *)calloc(ng, sizeof(double));
+        if (!J->grad) return -1;
+    }
+    for (int t = 1; t < nthreads; ++t) pthread_create(&ids[t], 0, adj_worker, &jobs[t]);
+    adj_worker(&jobs[0]);
+    for (int t = 1; t < nthreads; ++t) pthread_join(ids[t], 0);
+    double ga = 0.0;
+    for (int t = 0; t < nthreads; ++t) {
+        ga += jobs[t].galb;
+        if (t > 0) {
+            for (size_t k = 0; k < ng; ++k) grad[k] += jobs[t].grad[k];
+            free(jobs[t].grad);
+        }
+    }
+    *galb += ga;
+    return 0;
+}
+
+/* Gradient of sum_r w_r T_r over the brick samples (streams (seed, r, s)). */
+void orc_adjoint_transmittance(const orc_scene *S, const orc_params *P, const float *ro, const float *rd,
+                               const float *wr, uint32_t n, uint64_t nsamp, uint64_t seed, double *grad, double *T) {
+    for (uint32_t r = 0; r < n; ++r) {
+        uint64_t esc = 0;
+        scatter_ctx sv = {wr[r] / (float)nsamp, grad, S->bricks, S->lvoxc};
+        for (uint64_t s = 0; s < nsamp; ++s) {
+            orc_rng g;
+            orc_rng_seed(&g, seed, r, s);
+            const orc_rng g0 = g;
+            float td;
+            if (track_depth_v(S, P, ro + 3 * r, rd + 3 * r, &g, FLT_MAX, &td, 0, 0, 0) == 1) {
+                ++esc;
+                orc_rng g1 = g0;
+                (void)track_depth_v(S, P, ro + 3 * r, rd + 3 * r, &g1, FLT_MAX, &td, 0, scatter_visit, &sv);
+            }
+        }
+        if (T) T[r] = (double)esc / (double)nsamp;
+    }
 }

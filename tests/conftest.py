@@ -79,6 +79,7 @@ def settings_from_cfg(cfg: dict):
         sky=SkyState(np.asarray(cfg["sky_configs"]), np.asarray(cfg["sky_radiances"])),
         phase=PhaseTable(cfg["mie_pdf"], cfg["mie_cdf"]), viewi=cfg["viewi"], proji=cfg["proji"], w=cfg["w"],
         h=cfg["h"], depth=cfg.get("depth"), depthcomp=bool(cfg.get("depthcomp", False)),
+        finite_paths=bool(cfg.get("finite_paths", False)),
         phase_mode=int(cfg.get("phase_mode", 0)))
 
 
@@ -133,3 +134,26 @@ def gpu_renderer():
     r.set_params(settings_from_cfg(c0_cfg(64, 64)))
     yield r
     r.close()
+
+
+# A path of the reference estimator whose sky term is 0/0: in the uniform
+# 0.3 cube (128^3), camera at azimuth 0 (256 x 256), pixel (131, 158),
+# stream (1000 + 0x9E3779B9, pixel, 9) escapes at r = 4 along a direction
+# with rd.y == 0 exactly.
+NAN_PATH = {"pixel": (131, 158), "seed": 1000 + 0x9E3779B9, "sample": 9}
+
+
+def uniform_cube_scene(build):
+    """The uniform 0.3 grid of 128^3 as (nodes, bricks, mlevel) from `build`
+    (a builder taking block origins, values, voxel size, maxdepth)."""
+    from droplet_b200 import workloads as W
+
+    org, vals = W.dense_to_blocks(np.full((128, 128, 128), 0.3, np.float32))
+    return build(org, vals, 1 / 128, 12)
+
+
+def orbit_cfg(w: int, h: int, azimuth: float) -> dict:
+    cfg = c0_cfg(w, h)
+    eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], azimuth, W.CAMERA["elevation"])
+    cfg["viewi"], cfg["proji"] = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], w, h)
+    return cfg
