@@ -291,13 +291,17 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """dram bytes per launch from the committed ncu summary, scaled to this frame."""
-    p = os.path.join(ROOT, "profiles", "render_tile_kernel_traffic.json")
+    """DRAM bytes per vertex of the render kernel from the committed ncu summary
+    (profiles/render_persistent_kernel_c1.md, line "dram_bytes_per_vertex: X")."""
+    p = os.path.join(ROOT, "profiles", "render_persistent_kernel_c1.md")
     try:
         with open(p) as f:
-            return json.load(f)
+            for line in f:
+                if line.startswith("dram_bytes_per_vertex:"):
+                    return {"dram_bytes_per_vertex": float(line.split(":")[1])}
     except Exception:
-        return None
+        pass
+    return None
 
 
 def cpu_reference_times(nodes, bricks, cfg, threads: int, steps: int = 1, warmup: int = 0):
@@ -693,6 +697,8 @@ def run_b200(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
                 "traffic": (traffic["dram_bytes_per_vertex"] * cnt["vertices"] / args.steps) if traffic else None,
+                "traffic_source": "ncu dram__bytes_read.sum + write.sum on a 512^2 crop launch, per vertex, scaled "
+                                  "by this frame's vertices (profiles/render_persistent_kernel_c1.md)",
                 "algorithmic_bytes_per_vertex": b_v,
                 "calibration": "B_v from a 16-spp frame (seed 4242) with the octree stack traversal"}
 
