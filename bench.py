@@ -488,6 +488,130 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
     }
 
 
+def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp: int = 256):
+    """The large sparse scene (config 4): 24 puffs (workloads.slab_recipe) on a
+    2048^3 grid, sigma_t = 100, albedo 0.99, 128 scattering events, 3840x2160 at
+    256 spp rendered as 4 camera tiles of 1920x1080: plain (one launch per tile)
+    and batched (one graph launch of the 4 tiles), both timed with CUDA events;
+    then one adjoint step at 512x512 (32 spp, L2 loss against a 128-spp render of
+    the scene, starting from its bricks scaled by 0.9)."""
+    import torch
+
+    from droplet_b200 import adjoint as AD
+    from droplet_b200 import autotune
+    from droplet_b200.renderer import Batch, BatchView, PhaseTable, RenderSettings
+    from droplet_b200.scene import build_octree
+    from droplet_b200.sky import SkyState
+
+    t = time.time()
+    rec = W.slab_recipe(2048)
+    org, vals = W.sparse_field_puffwise(rec)
+    nonzero = int((vals != 0).sum())
+    t_field = time.time() - t
+    t = time.time()
+    oc = build_octree(org, vals, rec.voxel_size, 12)
+    t_build = time.time() - t
+    del vals
+    ss, sa, ev = W.medium("c4")
+
+    def settings(w, h):
+        eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], W.CAMERA["azimuth"], 25.0)
+        viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], w, h)
+        return RenderSettings(sigma_s=ss, sigma_a=sa, scattevs=ev,
+                              sun_dir=cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"]),
+                              sun_color=np.asarray(W.SUN["color"], np.float32), sun_angle=W.SUN["angle"],
+                              sky=SkyState(cfgs, rads), phase=PhaseTable(pdf, cdf), viewi=viewi, proji=proji, w=w,
+                              h=h)
+
+    saved = r.get_tuning()
+    r.upload(oc)
+    big = settings(3840, 2160)
+    r.set_params(big)
+    best, _ = autotune.tune(r, (960, 540, 1920, 1080), 4, key="c4", use_cache=False)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sun = torch.empty((1080, 1920, 4), device="cuda")
+    sky = torch.empty_like(sun)
+    tiles = [(tx * 1920, ty * 1080) for ty in range(2) for tx in range(2)]
+
+    def frame(k):
+        for (x0, y0) in tiles:
+            r.render_tile_async(x0, y0, 1920, 1080, spp, 11, k * spp, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
+
+    for k in range(warmup):
+        frame(k)
+    stream.synchronize()
+    r.reset_counters()
+    ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            frame(warmup + k)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+    cnt = r.counters()
+    plain = cnt["vertices"] / (sum(ms) / 1e3)
+    bt = Batch(r, [oc], [BatchView(0, big, spp, 11, (x0, y0, 1920, 1080)) for (x0, y0) in tiles])
+    bt.set_tuning(*best)
+    for _ in range(warmup):
+        bt.launch(stream.cuda_stream)
+    stream.synchronize()
+    r.reset_counters()
+    bms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            bt.launch(stream.cuda_stream)
+            b.record(stream)
+            b.synchronize()
+            bms.append(a.elapsed_time(b))
+    bcnt = r.counters()
+    bt.close()
+    batched = bcnt["vertices"] / (sum(bms) / 1e3)
+    # one adjoint step at 512x512
+    small = settings(512, 512)
+    with torch.no_grad():
+        tb = torch.tensor(oc.bricks, device="cuda")
+        tsun, tsky = AD.render(tb, torch.tensor(0.99, device="cuda"), r, [AD.DiffView(small, 128, 5)])
+        target = (tsun + tsky)[..., :3].clone()
+    b = (0.9 * tb).clone().requires_grad_(True)
+    alb = torch.tensor(0.99, device="cuda", requires_grad=True)
+    times = []
+    for it in range(2):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        cs = torch.cuda.current_stream()
+        e0.record(cs)
+        s1, k1 = AD.render(b, alb, r, [AD.DiffView(small, 32, 100 + it)])
+        loss = (((s1 + k1)[..., :3] - target) ** 2).sum()
+        e1.record(cs)
+        b.grad = None
+        loss.backward()
+        e2.record(cs)
+        e2.synchronize()
+        times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+    r.set_tuning(*saved)
+    return {
+        "workload": "24 puffs (seeds 20-43, radii U[0.02,0.12], default_rng(2044)) in a 1x1x0.3 slab on a 2048^3 grid, "
+                    "sigma_t 100, albedo 0.99, 128 events, 3840x2160 at 256 spp as 4 tiles of 1920x1080",
+        "nonzero_voxels": nonzero, "occupancy": nonzero / 2048 ** 3, "blocks": int(len(org)),
+        "nodes": int(oc.n_nodes), "leaves": int(oc.n_leaves), "octree_depth": int(oc.mlevel),
+        "bricks_mb": oc.bricks.nbytes / 1e6, "field_s": round(t_field, 1), "build_s": round(t_build, 1),
+        "tuning": list(best),
+        "plain": {"value": plain, "unit": "vertices/s", "ms_per_frame": float(np.mean(ms)), "launch_ms": ms,
+                  "vertices_per_frame": cnt["vertices"] / steps, "paths_per_frame": cnt["paths"] / steps},
+        "batched": {"value": batched, "unit": "vertices/s", "ms_per_frame": float(np.mean(bms)), "launch_ms": bms},
+        "adjoint_512": {"forward_ms": times[-1][0], "adjoint_ms": times[-1][1],
+                        "ratio": times[-1][1] / times[-1][0], "spp": 32,
+                        "grad_norm": float(b.grad.norm()), "loss": float(loss.detach())},
+        "l2": "flushed before each timed frame (256 MB write)",
+    }
+
+
 def seconds_to_rmse(r, stream, region, ms_per_frame: float, target: float = 0.01, ref_spp: int = 4096,
                     chunk: int = 256):
     """Seconds of plain rendering to reach `target` relative RMSE against the
@@ -735,6 +859,12 @@ def run_b200(args):
             f"ratio {adjoint['adjoint_over_forward']:.2f}, fd {adjoint['fd_check']['mean_fd']:.4g} "
             f"vs {adjoint['fd_check']['mean_adjoint']:.4g}")
 
+    large = None
+    if rank == 0 and world == 1 and not args.no_large:
+        large = measure_large(r, pdf, cdf, cfgs, rads)
+        log(f"large: plain {large['plain']['value'] / 1e9:.3f} G/s ({large['plain']['ms_per_frame']:.0f} ms/frame), "
+            f"batched {large['batched']['value'] / 1e9:.3f} G/s, adjoint step {large['adjoint_512']['ratio']:.2f}x")
+
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = measure_batched(r, pdf, cdf, steps=2, warmup=1)
@@ -760,6 +890,7 @@ def run_b200(args):
             "seconds_to_1pct_rmse": rmse,
             "batched": batched,
             "adjoint": adjoint,
+            "large_sparse": large,
             "counters_per_step": {k: v / args.steps for k, v in cnt.items()},
             "kernel_ms": kernel_ms,
         }
@@ -782,6 +913,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload measurement")
     ap.add_argument("--no-rmse", action="store_true", help="skip the seconds-to-1%%-RMSE measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the inverse-rendering (adjoint) measurement")
+    ap.add_argument("--no-large", action="store_true", help="skip the large sparse scene (config 4)")
     ap.add_argument("--fd-groups", type=int, default=8, help="seed groups of the finite-difference check")
     ap.add_argument("--fd-spp", type=int, default=32, help="spp per view of the finite-difference check")
     ap.add_argument("--fd-eps", type=float, default=1e-3, help="brick-sample step of the finite-difference check")

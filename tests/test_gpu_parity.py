@@ -341,3 +341,38 @@ def test_banded_host_render_equals_restatement(port):
                 assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), tuning
             for k in ("vertices", "density_lookups", "mie_evals", "paths"):
                 assert cnt[k] == pcnt[k], (tuning, k)
+
+
+def test_large_sparse_scene_recipe_paths_equal_restatement(port):
+    """The large sparse scene's recipe (24 puffs in a slab, sigma_t 100, 128
+    events) at 256^3: GPU paths equal the restatement's."""
+    from droplet_b200 import camera as cam
+    from droplet_b200 import workloads as W
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import build_octree
+
+    rec = W.slab_recipe(256)
+    org, vals = W.sparse_field_puffwise(rec, device="cpu")
+    oc = build_octree(org, vals, rec.voxel_size, 12)
+    cfg = c0_cfg(160, 90)
+    ss, sa, ev = W.medium("c4")
+    cfg.update(sigma_s=ss, sigma_a=sa, scattevs=ev)
+    eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], W.CAMERA["azimuth"], 25.0)
+    cfg["viewi"], cfg["proji"] = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], 160, 90)
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(oc.nodes, oc.bricks)
+    psun, psky, pcnt = port.render_tile(S, P, 40, 20, 80, 50, 16, seed=4, sample_base=0)
+    assert pcnt["mie_evals"] > 3000  # the tile sees the puffs: paths scatter
+    with Renderer(0) as r:
+        r.upload(oc)
+        r.set_params(settings_from_cfg(cfg))
+        for tuning in ((0, 6, 20, 0, 0), (1, 0, 0, 0, 0)):
+            r.set_tuning(*tuning)
+            r.reset_counters()
+            sun, sky = r.render_tile(40, 20, 80, 50, 16, seed=4, sample_base=0)
+            cnt = r.counters()
+            for g, p in ((sun, psun), (sky, psky)):
+                assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), tuning
+            for k in ("vertices", "density_lookups", "mie_evals", "paths"):
+                assert cnt[k] == pcnt[k], (tuning, k)
