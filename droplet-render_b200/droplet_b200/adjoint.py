@@ -21,7 +21,7 @@ from dataclasses import dataclass, replace
 
 import numpy as np
 
-from .renderer import Renderer, RenderSettings
+from .renderer import Renderer, RenderSettings, stream_handle
 
 
 @dataclass
@@ -45,7 +45,8 @@ def _function():
         def forward(ctx, bricks, albedo, renderer, views, adjoint_seed_offset, majorant_scale):
             bricks = bricks.detach().contiguous()
             stream = torch.cuda.current_stream(bricks.device)
-            renderer.set_bricks_dev(bricks.data_ptr(), bricks.shape[0], majorant_scale, stream.cuda_stream)
+            sh = stream_handle(stream)
+            renderer.set_bricks_dev(bricks.data_ptr(), bricks.shape[0], majorant_scale, sh)
             a = float(albedo.detach().cpu())
             h = max(v.settings.h for v in views)
             w = max(v.settings.w for v in views)
@@ -56,7 +57,7 @@ def _function():
                 vs = torch.empty((v.settings.h, v.settings.w, 4), dtype=torch.float32, device=bricks.device)
                 vk = torch.empty_like(vs)
                 renderer.render_tile_async(0, 0, v.settings.w, v.settings.h, v.spp, v.seed, 0, vs.data_ptr(),
-                                           vk.data_ptr(), stream.cuda_stream)
+                                           vk.data_ptr(), sh)
                 sun[i, :v.settings.h, :v.settings.w] = vs / v.spp
                 sky[i, :v.settings.h, :v.settings.w] = vk / v.spp
             ctx.renderer, ctx.views, ctx.albedo = renderer, views, a
@@ -68,7 +69,7 @@ def _function():
         def backward(ctx, g_sun, g_sky):
             r, views = ctx.renderer, ctx.views
             dev = g_sun.device
-            stream = torch.cuda.current_stream(dev)
+            sh = stream_handle(torch.cuda.current_stream(dev))
             grad = torch.zeros(ctx.shape, dtype=torch.float32, device=dev)
             galb = torch.zeros(1, dtype=torch.float64, device=dev)
             for i, v in enumerate(views):
@@ -79,7 +80,7 @@ def _function():
                 # ds / dk may be freed after this iteration: the caching allocator
                 # reuses their memory only for work queued after the kernel on this stream
                 r.adjoint_tile_async(0, 0, ww, hh, v.spp, v.seed + ctx.offset, 0, ds.data_ptr(), dk.data_ptr(),
-                                     grad.data_ptr(), galb.data_ptr(), stream.cuda_stream)
+                                     grad.data_ptr(), galb.data_ptr(), sh)
             return grad, galb.to(torch.float32).reshape(()), None, None, None, None
 
     return RenderFn

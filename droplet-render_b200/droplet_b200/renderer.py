@@ -83,6 +83,16 @@ class RenderSettings:
         return p
 
 
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream as a stream handle
+
+
+def stream_handle(torch_stream) -> int:
+    """The C-ABI handle of a torch stream.  torch's default stream reports handle 0,
+    which the library reads as "the context's own stream"; it is the legacy
+    default stream, so it is passed as cudaStreamLegacy instead."""
+    return int(torch_stream.cuda_stream) or CUDA_STREAM_LEGACY
+
+
 class Renderer:
     def __init__(self, device: int = 0):
         self._ctx = C.c_void_p()
