@@ -917,7 +917,7 @@ def main():
     ap.add_argument("--fd-groups", type=int, default=8, help="seed groups of the finite-difference check")
     ap.add_argument("--fd-spp", type=int, default=32, help="spp per view of the finite-difference check")
     ap.add_argument("--fd-eps", type=float, default=1e-3, help="brick-sample step of the finite-difference check")
-    ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal,tile (no tuning)")
+    ap.add_argument("--tuning", default="", help="fixed launch shape kernel,blocks_per_sm,event_batch,traversal,tile,visits (no tuning)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -235,13 +235,15 @@ int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
     if (!c || !t) return need(false, DR_ERR_INVALID, "dr_set_tuning: null argument");
     if (!valid_tuning(t))
         return need(false, DR_ERR_INVALID,
-                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1, tile <= 64");
+                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1, tile <= 64, "
+                    "visits <= 255");
     c->tuning.kernel = t->kernel;
     c->tuning.block = kPersistentBlock;
     c->tuning.blocks_per_sm = t->blocks_per_sm;
     c->tuning.event_batch = t->event_batch;
     c->tuning.traversal = t->traversal;
     c->tuning.tile = t->tile;
+    c->tuning.visits = t->visits;
     return DR_OK;
 }
 
@@ -252,6 +254,7 @@ int dr_get_tuning(dr_ctx *c, dr_tuning *t) {
     t->event_batch = c->tuning.event_batch;
     t->traversal = c->tuning.traversal;
     t->tile = c->tuning.tile;
+    t->visits = c->tuning.visits;
     return DR_OK;
 }
 

@@ -256,14 +256,20 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
     }
 }
 
-__device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
-                                          float &tra, float &trb, Count &cnt) {
-    if (!T.active) return false;
-    for (;;) {
+// Up to `budget` loop iterations (child examinations or pops) towards the next
+// leaf: returns kTravLeaf with (leaf, tra, trb), kTravDone when the ray has no
+// further leaf, or kTravMore when the budget ran out first (call again: the
+// state is complete after every iteration).
+enum : uint32_t { kTravMore = 0, kTravLeaf = 1, kTravDone = 2 };
+__device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
+                                                float &tra, float &trb, Count &cnt, uint32_t budget) {
+    if (!T.active) return kTravDone;
+    for (uint32_t it = 0;; ++it) {
+        if (it == budget) return kTravMore;
         if (T.tn >= 8) {
             if (T.l == 0) {
                 T.active = false;
-                return false;
+                return kTravDone;
             }
             const int l = T.l - 1;
             T.l = l;
@@ -301,13 +307,13 @@ __device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *
             leaf = child & ~kLeafBit;
             tra = std_max(std_max(c0[0], c0[1]), c0[2]);
             trb = std_min(std_min(c1[0], c1[1]), c1[2]);
-            return true;
+            return kTravLeaf;
         }
         const int l = T.l;
         if (l + 1 >= kMaxDepth - 1) {  // an internal node at level 15 has no stack room (reference limit)
             T.active = false;
             ++cnt.gave_up;
-            return false;
+            return kTravDone;
         }
         nstack[l] = T.node;
         T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
@@ -321,6 +327,11 @@ __device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *
         }
         T.tn = first_node(T.t0, tm);
     }
+}
+
+__device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
+                                          float &tra, float &trb, Count &cnt) {
+    return trav_next_k(T, S, nstack, leaf, tra, trb, cnt, 0xffffffffu) == kTravLeaf;
 }
 
 // ---- cell walk: the same leaf sequence without a stack -----------------------

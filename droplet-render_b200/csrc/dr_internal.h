@@ -83,6 +83,7 @@ struct Tuning {
     uint32_t event_batch;   // lanes of a warp that must be waiting before events run
     uint32_t traversal;     // 0 = octree stack traversal, 1 = leaf-grid cell walk
     uint32_t tile;          // pixel order of the persistent kernel: 0 = row-major, else square side
+    uint32_t visits;        // stack traversal: node examinations per loop iteration (0 = to the next leaf)
 };
 
 // One view of a batched launch: its parameters, tile and output, the scene it

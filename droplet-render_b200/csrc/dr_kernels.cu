@@ -276,12 +276,14 @@ __device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &
 // no further leaf (or the depth mask stops it): the segment escaped.
 template <bool WALK>
 __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
-                                              uint32_t *nstack, Trav *slow, Count &cnt) {
+                                              uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits) {
     uint32_t leaf = 0;
     float tra = 0.0f, trb = 0.0f;
     uint32_t r;
     if constexpr (!WALK) {
-        r = (L.wmode == 3u && trav_next(L.st.t, S, nstack, leaf, tra, trb, cnt)) ? 1u : 2u;
+        // at most `visits` examinations per loop iteration (0: up to the next leaf)
+        r = L.wmode == 3u ? trav_next_k(L.st.t, S, nstack, leaf, tra, trb, cnt, visits ? visits : 0xffffffffu)
+                          : kTravDone;
     } else if (L.wmode == 1u) {
         r = walk_step(L.st.w, S, leaf, tra, trb, cnt);
     } else if (L.wmode == 2u) {
@@ -466,13 +468,13 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
 template <bool WALK>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
-                                          Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow) {
+                                          Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits) {
     if (events) {
         if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
     }
     if (state == kTrav) {
-        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt);
+        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt, visits);
         if (r == 1u) {
             state = kStep;
         } else if (r == 2u) {
@@ -505,8 +507,10 @@ template <int MINB, bool WALK, bool BATCH>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
                                                                             float4 *sky_out, DevCounters *C,
-                                                                            WorkQueue *Q, uint32_t event_batch,
+                                                                            WorkQueue *Q, uint32_t knobs,
                                                                             BatchArgs B) {
+    // knobs: bits 0-7 the event batch, bits 8-15 the traversal visits per iteration
+    const uint32_t event_batch = knobs & 0xffu, visits = (knobs >> 8) & 0xffu;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
     uint32_t mb;
@@ -566,9 +570,9 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow);
+            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow, visits);
         } else {
-            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow);
+            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits);
         }
     }
     warp_sum_counts(cnt, C, paths);
@@ -1130,6 +1134,7 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
     const int bps = tune.blocks_per_sm && (int)tune.blocks_per_sm < maxb ? (int)tune.blocks_per_sm : maxb;
     blocks = sms * bps;
     event_batch = tune.event_batch ? (tune.event_batch > 32 ? 32u : tune.event_batch) : 8u;
+    event_batch |= (tune.visits > 255 ? 255u : tune.visits) << 8;
     return cudaSuccess;
 }
 

@@ -174,6 +174,8 @@ typedef struct {
     uint32_t event_batch;    /* persistent kernel: waiting lanes before a warp shades (1..32, 0 = 8) */
     uint32_t traversal;      /* persistent kernel: DR_TRAVERSAL_* */
     uint32_t tile;           /* persistent kernel: pixel order in tile x tile squares, 0 = row-major (<= 64) */
+    uint32_t visits;         /* persistent kernel, stack traversal: node examinations per iteration, 0 = to the
+                                next leaf (<= 255) */
 } dr_tuning;
 #define DR_TRAVERSAL_STACK 0u  /* octree descent with a node stack (the reference's order) */
 #define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */

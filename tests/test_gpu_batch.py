@@ -63,7 +63,7 @@ def batch_setup():
 def test_batch_views_equal_restatement(batch_setup, port, tuning):
     r, b, specs, scenes = batch_setup
     b.set_tuning(*tuning)
-    assert b.get_tuning()[1:] == tuning[1:]
+    assert b.get_tuning()[1:5] == tuning[1:5]
     S = [port.scene(oc.nodes, oc.bricks) for oc in scenes]
     for _ in range(2):
         _, k = b.info()
