@@ -236,7 +236,7 @@ int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
     if (!valid_tuning(t))
         return need(false, DR_ERR_INVALID,
                     "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1, tile <= 64, "
-                    "visits <= 255");
+                    "visits <= 255, steps <= 255");
     c->tuning.kernel = t->kernel;
     c->tuning.block = kPersistentBlock;
     c->tuning.blocks_per_sm = t->blocks_per_sm;
@@ -244,6 +244,7 @@ int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
     c->tuning.traversal = t->traversal;
     c->tuning.tile = t->tile;
     c->tuning.visits = t->visits;
+    c->tuning.steps = t->steps;
     return DR_OK;
 }
 
@@ -255,6 +256,7 @@ int dr_get_tuning(dr_ctx *c, dr_tuning *t) {
     t->traversal = c->tuning.traversal;
     t->tile = c->tuning.tile;
     t->visits = c->tuning.visits;
+    t->steps = c->tuning.steps;
     return DR_OK;
 }
 

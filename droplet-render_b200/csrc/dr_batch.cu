@@ -34,7 +34,7 @@ struct dr_batch {
     std::vector<size_t> out_off;  // float4 offset of view v's sun tile; its sky tile follows
     size_t out_n = 0;             // float4 count of all outputs
     DevParams p0{};
-    Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u};
+    Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};
     uint64_t n_paths = 0, launches = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -230,6 +230,7 @@ int dr_batch_set_tuning(dr_batch *b, const dr_tuning *t) {
     b->tuning.traversal = t->traversal;
     b->tuning.tile = t->tile;
     b->tuning.visits = t->visits;
+    b->tuning.steps = t->steps;
     return build_graph(b);
 }
 
@@ -241,6 +242,7 @@ int dr_batch_get_tuning(dr_batch *b, dr_tuning *t) {
     t->traversal = b->tuning.traversal;
     t->tile = b->tuning.tile;
     t->visits = b->tuning.visits;
+    t->steps = b->tuning.steps;
     return DR_OK;
 }
 

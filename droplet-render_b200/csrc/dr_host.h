@@ -119,7 +119,7 @@ struct dr_ctx {
     dr::DevBuf<double> albedo_slots;  // adjoint: partial sums of the albedo gradient (kept zeroed)
     uint32_t n_leaf_nodes = 0;
     bool use_grid = true;
-    dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u};
+    dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};
     std::vector<uint8_t> leaf_flag;  // host copy: node i is a leaf (for validating probe inputs)
     // host-buffer render pipeline (dr_render_tile): row bands rendered on two
     // streams, each copied to pinned staging as soon as it is done

@@ -84,6 +84,7 @@ struct Tuning {
     uint32_t traversal;     // 0 = octree stack traversal, 1 = leaf-grid cell walk
     uint32_t tile;          // pixel order of the persistent kernel: 0 = row-major, else square side
     uint32_t visits;        // stack traversal: node examinations per loop iteration (0 = to the next leaf)
+    uint32_t steps;         // free-flight steps per loop iteration (0 = 1)
 };
 
 // One view of a batched launch: its parameters, tile and output, the scene it

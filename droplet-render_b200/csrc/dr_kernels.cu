@@ -468,7 +468,8 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
 template <bool WALK>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
-                                          Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits) {
+                                          Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits,
+                                          uint32_t steps) {
     if (events) {
         if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
@@ -482,7 +483,8 @@ __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const 
             state = kEvent;
         }
     }
-    if (state == kStep) {
+    // up to `steps` free-flight steps while the lane stays in its leaf
+    for (uint32_t k = 0; k < steps && state == kStep; ++k) {
         const uint32_t rs = track_step(L, cnt);
         if (rs == 1) state = kTrav;
         else if (rs == 2) state = kEvent;
@@ -509,8 +511,10 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
                                                                             float4 *sky_out, DevCounters *C,
                                                                             WorkQueue *Q, uint32_t knobs,
                                                                             BatchArgs B) {
-    // knobs: bits 0-7 the event batch, bits 8-15 the traversal visits per iteration
+    // knobs: bits 0-7 the event batch, bits 8-15 the traversal visits per
+    // iteration (0: to the next leaf), bits 16-23 the tracking steps per iteration
     const uint32_t event_batch = knobs & 0xffu, visits = (knobs >> 8) & 0xffu;
+    const uint32_t steps = ((knobs >> 16) & 0xffu) ? ((knobs >> 16) & 0xffu) : 1u;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
     uint32_t mb;
@@ -570,9 +574,10 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow, visits);
+            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow, visits,
+                      steps);
         } else {
-            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits);
+            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps);
         }
     }
     warp_sum_counts(cnt, C, paths);
@@ -1135,6 +1140,7 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
     blocks = sms * bps;
     event_batch = tune.event_batch ? (tune.event_batch > 32 ? 32u : tune.event_batch) : 8u;
     event_batch |= (tune.visits > 255 ? 255u : tune.visits) << 8;
+    event_batch |= (tune.steps > 255 ? 255u : tune.steps) << 16;
     return cudaSuccess;
 }
 

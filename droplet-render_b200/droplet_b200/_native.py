@@ -109,7 +109,7 @@ class DrCounters(C.Structure):
 
 class DrTuning(C.Structure):
     _fields_ = [("kernel", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("event_batch", C.c_uint32),
-                ("traversal", C.c_uint32), ("tile", C.c_uint32), ("visits", C.c_uint32)]
+                ("traversal", C.c_uint32), ("tile", C.c_uint32), ("visits", C.c_uint32), ("steps", C.c_uint32)]
 
 
 class DrBatchView(C.Structure):

@@ -1,6 +1,6 @@
 """Launch-shape autotuner for the persistent path kernel (single frames and batches).
 
-The persistent kernel has six knobs (`dr_tuning`):
+The persistent kernel has seven knobs (`dr_tuning`):
 * the compiled variant, i.e. resident blocks per SM. 4/5/6/8 trade registers for
   occupancy; the smaller register budgets spill a little to L1-resident local memory.
 * the event batch: how many lanes of a warp must be waiting on a segment end before
@@ -8,8 +8,9 @@ The persistent kernel has six knobs (`dr_tuning`):
 * the traversal: octree descent with a node stack, or the cell walk over the leaf
   grid (faster where leaves are dense along rays, slower through wide empty regions).
 * the tile: pixels handed out row-major or square by square (ray coherence).
-* the visit budget: how many octree nodes the stack traversal examines per loop
-  iteration before the warp moves on (0: up to the next leaf).
+* the work per loop iteration: how many octree nodes the stack traversal examines
+  (0: up to the next leaf) and how many free-flight steps a lane takes before the
+  warp moves on; balancing them keeps traversing and tracking lanes busy alike.
 * the kernel family (persistent, or one thread per path; single frames only).
 
 `tune` searches in two stages: occupancy x event batch first, then traversal x tile
@@ -25,15 +26,17 @@ import time
 
 from . import _native as N
 
-STAGE1 = [(0, bps, batch, 0, 0, 0) for bps in (4, 5, 6, 8) for batch in (8, 16, 24)]
-PER_PATH = (1, 0, 0, 0, 0, 0)
+STAGE1 = [(0, bps, batch, 0, 0, 0, 0) for bps in (4, 5, 6, 8) for batch in (8, 16, 24)]
+PER_PATH = (1, 0, 0, 0, 0, 0, 0)
 
 
 def stage2(best):
+    """Around the best occupancy and event batch: traversal x tile, neighbouring
+    event batches, and the work per loop iteration (visits x steps)."""
     k, bps, batch = best[:3]
-    out = [(k, bps, batch, trav, tile, 0) for trav in (0, 1) for tile in (0, 8, 16)]
-    out += [(k, bps, b2, 0, 0, 0) for b2 in (12, 20, 28, 32) if b2 != batch]
-    out += [(k, bps, batch, 0, 0, v) for v in (1, 2, 4, 8)]
+    out = [(k, bps, batch, trav, tile, 0, 0) for trav in (0, 1) for tile in (0, 8, 16)]
+    out += [(k, bps, b2, 0, 0, 0, 0) for b2 in (12, 20, 28, 32) if b2 != batch]
+    out += [(k, bps, batch, 0, 0, v, st) for v in (2, 4, 8) for st in (1, 2, 4)]
     return out
 
 

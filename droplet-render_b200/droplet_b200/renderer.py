@@ -178,15 +178,16 @@ class Renderer:
         N.check(N.lib().dr_synchronize(self._ctx))
 
     def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
-                   tile: int = 0, visits: int = 0):
-        t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal), int(tile), int(visits))
+                   tile: int = 0, visits: int = 0, steps: int = 0):
+        t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal), int(tile), int(visits),
+                       int(steps))
         N.check(N.lib().dr_set_tuning(self._ctx, C.byref(t)))
 
     def get_tuning(self):
         t = N.DrTuning()
         N.check(N.lib().dr_get_tuning(self._ctx, C.byref(t)))
         return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal), int(t.tile),
-                int(t.visits))
+                int(t.visits), int(t.steps))
 
     # ---- differentiable rendering -------------------------------------------------
     def set_bricks_dev(self, bricks_ptr: int, n_leaves: int, majorant_scale: float = 1.0, stream_ptr: int = 0):
@@ -321,15 +322,15 @@ class Batch:
             pass
 
     def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
-                   tile: int = 0, visits: int = 0):
-        t = N.DrTuning(0, int(blocks_per_sm), int(event_batch), int(traversal), int(tile), int(visits))
+                   tile: int = 0, visits: int = 0, steps: int = 0):
+        t = N.DrTuning(0, int(blocks_per_sm), int(event_batch), int(traversal), int(tile), int(visits), int(steps))
         N.check(N.lib().dr_batch_set_tuning(self._h, C.byref(t)))
 
     def get_tuning(self):
         t = N.DrTuning()
         N.check(N.lib().dr_batch_get_tuning(self._h, C.byref(t)))
         return (int(t.kernel), int(t.blocks_per_sm), int(t.event_batch), int(t.traversal), int(t.tile),
-                int(t.visits))
+                int(t.visits), int(t.steps))
 
     def launch(self, stream_ptr: int = 0):
         N.check(N.lib().dr_batch_launch(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))

@@ -176,6 +176,7 @@ typedef struct {
     uint32_t tile;           /* persistent kernel: pixel order in tile x tile squares, 0 = row-major (<= 64) */
     uint32_t visits;         /* persistent kernel, stack traversal: node examinations per iteration, 0 = to the
                                 next leaf (<= 255) */
+    uint32_t steps;          /* persistent kernel: free-flight steps per iteration, 0 = 1 (<= 255) */
 } dr_tuning;
 #define DR_TRAVERSAL_STACK 0u  /* octree descent with a node stack (the reference's order) */
 #define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */

@@ -227,7 +227,7 @@ def test_every_launch_shape_renders_the_same_paths(gpu_renderer, port):
     try:
         for cand in [(0, 4, 1, 0), (0, 5, 8, 0), (0, 6, 16, 0), (0, 8, 32, 0), (0, 0, 0, 0),
                      (0, 4, 1, 1), (0, 5, 8, 1), (0, 6, 16, 1), (0, 8, 32, 1), (1, 0, 0, 0),
-                     (0, 5, 8, 0, 0, 1), (0, 8, 24, 0, 8, 2), (0, 6, 16, 0, 16, 4)]:
+                     (0, 5, 8, 0, 0, 1), (0, 8, 24, 0, 8, 2, 2), (0, 6, 16, 0, 16, 4, 4)]:
             gpu_renderer.set_tuning(*cand)
             gpu_renderer.reset_counters()
             sun, sky = gpu_renderer.render_tile(4, 6, 56, 52, 40, seed=9, sample_base=3)
