@@ -260,9 +260,13 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
 // leaf: returns kTravLeaf with (leaf, tra, trb), kTravDone when the ray has no
 // further leaf, or kTravMore when the budget ran out first (call again: the
 // state is complete after every iteration).
+// tstack (optional, kMaxDepth x 6 floats): the ancestors' intervals are saved
+// at each descent and read back on a pop; without it a pop rebuilds the
+// interval from the root by replaying the 3-bit child slots (the same floats).
 enum : uint32_t { kTravMore = 0, kTravLeaf = 1, kTravDone = 2 };
 __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
-                                                float &tra, float &trb, Count &cnt, uint32_t budget) {
+                                                float &tra, float &trb, Count &cnt, uint32_t budget,
+                                                float (*tstack)[6] = nullptr) {
     if (!T.active) return kTravDone;
     for (uint32_t it = 0;; ++it) {
         if (it == budget) return kTravMore;
@@ -275,6 +279,14 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
             T.l = l;
             T.node = nstack[l];
             T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
+            if (tstack) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    T.t0[k] = tstack[l][k];
+                    T.t1[k] = tstack[l][3 + k];
+                }
+                continue;
+            }
             float t0[3] = {T.t0r[0], T.t0r[1], T.t0r[2]}, t1[3] = {T.t1r[0], T.t1r[1], T.t1r[2]};
             for (int k = 0; k < l; ++k) {
                 const uint32_t s = (uint32_t)(T.slots >> (3 * k)) & 7u;
@@ -316,6 +328,13 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
             return kTravDone;
         }
         nstack[l] = T.node;
+        if (tstack) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                tstack[l][k] = T.t0[k];
+                tstack[l][3 + k] = T.t1[k];
+            }
+        }
         T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
         T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));
         T.l = l + 1;
@@ -795,7 +814,8 @@ __device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, co
     uint32_t leaf;
     float tra, trb;
     uint32_t budget = kStepBudget;
-    while (trav_next(T, S, nstack, leaf, tra, trb, cnt)) {
+    float tstack[kMaxDepth][6];
+    while (trav_next_k(T, S, nstack, leaf, tra, trb, cnt, 0xffffffffu, tstack) == kTravLeaf) {
         if (!(td < depth)) break;
         const float4 ce = __ldg(&S.leaf[2 * leaf]);
         const float4 meta = __ldg(&S.leaf[2 * leaf + 1]);

@@ -276,13 +276,15 @@ __device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &
 // no further leaf (or the depth mask stops it): the segment escaped.
 template <bool WALK>
 __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
-                                              uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits) {
+                                              uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits,
+                                              float (*tstack)[6]) {
     uint32_t leaf = 0;
     float tra = 0.0f, trb = 0.0f;
     uint32_t r;
     if constexpr (!WALK) {
         // at most `visits` examinations per loop iteration (0: up to the next leaf)
-        r = L.wmode == 3u ? trav_next_k(L.st.t, S, nstack, leaf, tra, trb, cnt, visits ? visits : 0xffffffffu)
+        r = L.wmode == 3u ? trav_next_k(L.st.t, S, nstack, leaf, tra, trb, cnt, visits ? visits : 0xffffffffu,
+                                        tstack)
                           : kTravDone;
     } else if (L.wmode == 1u) {
         r = walk_step(L.st.w, S, leaf, tra, trb, cnt);
@@ -469,13 +471,13 @@ template <bool WALK>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
                                           Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits,
-                                          uint32_t steps) {
+                                          uint32_t steps, float (*tstack)[6]) {
     if (events) {
         if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
     }
     if (state == kTrav) {
-        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt, visits);
+        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt, visits, tstack);
         if (r == 1u) {
             state = kStep;
         } else if (r == 2u) {
@@ -515,6 +517,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     // iteration (0: to the next leaf), bits 16-23 the tracking steps per iteration
     const uint32_t event_batch = knobs & 0xffu, visits = (knobs >> 8) & 0xffu;
     const uint32_t steps = ((knobs >> 16) & 0xffu) ? ((knobs >> 16) & 0xffu) : 1u;
+    float ts[kMaxDepth][6];  // ancestors' intervals of the stack traversal (local memory)
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
     uint32_t mb;
@@ -575,9 +578,9 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
             lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow, visits,
-                      steps);
+                      steps, ts);
         } else {
-            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps);
+            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps, ts);
         }
     }
     warp_sum_counts(cnt, C, paths);
