@@ -35,7 +35,10 @@ def _gpu_adjoint(r, cfg, x0, y0, tw, th, spp, seed, base, dsun, dsky, n_leaves):
     return g.cpu().numpy().astype(np.float64), float(ga.item())
 
 
-def test_adjoint_equals_restatement(adj, port):
+@pytest.mark.parametrize("tuning", [(0, 0, 0, 0, 0, 0, 0), (1, 0, 0, 0, 0, 0, 0)])
+def test_adjoint_equals_restatement(adj, port, tuning):
+    """The adjoint (whatever the forward's launch shape) equals the CPU
+    restatement on the same random streams."""
     r, nodes, bricks = adj
     cfg = c0_cfg(64, 64)
     keep = []
@@ -45,7 +48,12 @@ def test_adjoint_equals_restatement(adj, port):
     dsun = rng.normal(size=(40, 48, 4)).astype(np.float32)
     dsky = rng.normal(size=(40, 48, 4)).astype(np.float32)
     g_cpu, a_cpu = port.adjoint_tile(S, P, 8, 12, 48, 40, 16, 21, 3, dsun, dsky)
-    g_gpu, a_gpu = _gpu_adjoint(r, cfg, 8, 12, 48, 40, 16, 21, 3, dsun, dsky, len(bricks))
+    saved = r.get_tuning()
+    try:
+        r.set_tuning(*tuning)
+        g_gpu, a_gpu = _gpu_adjoint(r, cfg, 8, 12, 48, 40, 16, 21, 3, dsun, dsky, len(bricks))
+    finally:
+        r.set_tuning(*saved)
     scale = np.abs(g_cpu).max()
     assert scale > 0
     assert np.allclose(g_gpu, g_cpu, rtol=1e-3, atol=1e-4 * scale)
