@@ -174,10 +174,12 @@ struct Count {
 // ---- octree traversal ----------------------------------------------------
 // The reference's step traverser (src/KernelOctree.cpp:230-349) keeps t0, t1,
 // tm for all 16 levels.  Here only the current internal node's (t0, t1) stay
-// in registers; an ancestor's interval is rebuilt on pop from the root
-// interval by replaying the child slots (3 bits per level), which repeats the
-// reference's tm = 0.5f*(t0+t1) selections and gives identical floats.
-// Ancestor node ids live in a 16-entry per-thread array (local memory).
+// in registers; ancestor node ids live in a 16-entry per-thread array and the
+// ancestors' (t0, t1) in a 16 x 6 float array (local memory), written on each
+// descent and read back on a pop.  Without that array (the probes) a pop
+// rebuilds the interval from the root by replaying the child slots (3 bits per
+// level), which repeats the reference's tm = 0.5f*(t0+t1) selections: the same
+// floats either way.
 __device__ __forceinline__ uint32_t first_node(const float t0[3], const float tm[3]) {
     uint32_t a = 0;
     if (t0[0] > t0[1]) {
@@ -336,7 +338,7 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
             }
         }
         T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
-        T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));
+        if (!tstack) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));  // replay path only
         T.l = l + 1;
         T.node = child;
         for (int k = 0; k < 3; ++k) {
