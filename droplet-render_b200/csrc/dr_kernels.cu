@@ -737,10 +737,12 @@ __global__ void probe_transmittance_kernel(DevScene S, DevParams P, const float 
 // segment's next-event contribution.  The albedo f enters each contribution as
 // f^m (m = scattering events before it): dC/df = sum m * c / f.
 // Each path is replayed from its random stream twice, as in path replay
-// backpropagation: pass 1 recomputes its total contribution, pass 2 replays the
-// same decisions and scatters gradients.  No per-path tape is stored; a shadow
-// segment is tracked once to learn whether it escapes and, if it did, again
-// from the saved stream state to scatter.
+// backpropagation: pass 1 recomputes its total contribution and keeps one
+// float per path (its weight dsun . C_sun + dsky . C_sky), pass 2 replays the
+// same decisions and scatters gradients.  The passes are separate launches, so
+// the lanes of a warp run the same tracking code; no per-path tape is stored.
+// A shadow segment is tracked once to learn whether it escapes and, if it
+// did, again from the saved stream state to scatter.
 
 struct ScatterVisit {
     float w;  // dL/dC_after of the current segment
@@ -783,8 +785,9 @@ __device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, 
 }
 
 struct PathTotals {
-    float3 sun, sky;    // contribution of the path to the sun and sky sums
+    float w;            // dsun . (sun contribution) + dsky . (sky contribution) of the whole path
     float3 asun, asky;  // sum over contributions of (scattering events before it) * contribution
+    bool ok;            // every component of the path's contribution is finite
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -809,8 +812,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         float td;
         uint32_t res;
         if constexpr (SCATTER) {
-            vis.w = dot3f(dsun, f3(tot.sun.x - acc_sun.x, tot.sun.y - acc_sun.y, tot.sun.z - acc_sun.z)) +
-                    dot3f(dsky, f3(tot.sky.x - acc_sky.x, tot.sky.y - acc_sky.y, tot.sky.z - acc_sky.z));
+            vis.w = tot.w - (dot3f(dsun, acc_sun) + dot3f(dsky, acc_sky));
             res = track_scatter(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
         } else {
             res = track_plain(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
@@ -872,10 +874,11 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         }
     }
     if constexpr (!SCATTER) {
-        tot.sun = acc_sun;
-        tot.sky = acc_sky;
+        tot.w = dot3f(dsun, acc_sun) + dot3f(dsky, acc_sky);
         tot.asun = a_sun;
         tot.asky = a_sky;
+        tot.ok = isfinite(acc_sun.x) && isfinite(acc_sun.y) && isfinite(acc_sun.z) && isfinite(acc_sky.x) &&
+                 isfinite(acc_sky.y) && isfinite(acc_sky.z);
     }
 }
 
@@ -910,50 +913,87 @@ __global__ void sum_slots_kernel(double *out, double *slots) {
     }
 }
 
-// One thread per (pixel, sample), the render kernel's layout; delta images in
-// tile layout (tw x th float4, rgb used).  Gradients go to copy
-// blockIdx.x % copies of the brick-pool gradient (grad + copy * stride): the
-// surface samples every path meets first are hit by all warps at once, and
-// spreading them over copies divides the conflicts on each address; the copies
-// are summed afterwards.
-__global__ void __launch_bounds__(kRenderBlock) adjoint_tile_kernel(DevScene S, DevParams P, TileArgs A,
-                                                                    const void *mie_pack, const float4 *dsun,
-                                                                    const float4 *dsky, float *grad,
-                                                                    uint32_t copies, size_t stride,
-                                                                    double *albedo_slots, DevCounters *C) {
+// Path gi of a tile (one thread per (pixel, sample), the render kernel's
+// layout): its pixel column i and row j in the tile and its sample s.
+__device__ __forceinline__ void tile_path(const TileArgs &A, uint64_t gi, uint32_t &i, uint32_t &j, uint32_t &s) {
+    const uint64_t pl = gi / A.spp;
+    s = (uint32_t)(gi - pl * A.spp);
+    const uint32_t pix = (uint32_t)pl;
+    i = pix % A.cols;
+    j = pix / A.cols;
+}
+
+// Pass 1 over paths [p0, p0 + n) of a tile (delta images in tile layout,
+// tw x th float4, rgb used): wpath[gi - p0] = the path's dsun . C_sun + dsky .
+// C_sky, NaN for a path left out (zero delta at its pixel, or a contribution
+// that is not finite, the sky term's 0/0 for rd.y == 0); the albedo term goes
+// to the slots.
+__global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S, DevParams P, TileArgs A,
+                                                                      uint64_t p0, uint64_t n, const void *mie_pack,
+                                                                      const float4 *dsun, const float4 *dsky,
+                                                                      float *wpath, double *albedo_slots,
+                                                                      DevCounters *C) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
     const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
     const MieSmem M = mie_view(P, smem);
     uint32_t nstack[kMaxDepth];
-    const uint64_t gi = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
+    const uint64_t k = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
     float galb = 0.0f;
-    grad += (size_t)(blockIdx.x % copies) * stride;
-    if (staged && gi < A.n_paths) {
-        const uint64_t pl = gi / A.spp;
-        const uint32_t s = (uint32_t)(gi - pl * A.spp);
-        const uint32_t pix = (uint32_t)pl;
-        const uint32_t i = pix % A.cols, j = pix / A.cols;
+    if (staged && k < n) {
+        uint32_t i, j, s;
+        tile_path(A, p0 + k, i, j, s);
         const size_t o = (size_t)j * A.tw + i;
         const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
         const float3 dsun3 = f3(ds.x, ds.y, ds.z), dsky3 = f3(dk.x, dk.y, dk.z);
+        float w = __int_as_float(0x7fffffff);
         if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
             PathTotals tot{};
-            adjoint_pass<false>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, grad,
+            adjoint_pass<false>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
                                 nstack);
-            // a path whose contribution is not finite (the sky term's 0/0 for
-            // rd.y == 0) is left out of the gradient
-            const bool ok = isfinite(tot.sun.x) && isfinite(tot.sun.y) && isfinite(tot.sun.z) &&
-                            isfinite(tot.sky.x) && isfinite(tot.sky.y) && isfinite(tot.sky.z);
-            if (ok) {
-                adjoint_pass<true>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, grad,
-                                   nstack);
+            if (tot.ok) {
+                w = tot.w;
                 galb = (dot3f(dsun3, tot.asun) + dot3f(dsky3, tot.asky)) / P.albedo;
             }
         }
+        wpath[k] = w;
     }
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
     warp_add(galb, albedo_slots);
+}
+
+// Pass 2 over the same paths: replays each path kept by pass 1 and scatters
+// its gradient.  Gradients go to copy blockIdx.x % copies of the brick-pool
+// gradient (grad + copy * stride): the surface samples every path meets
+// first are hit by all warps at once, and spreading them over copies divides
+// the conflicts on each address; the copies are summed afterwards.
+__global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene S, DevParams P, TileArgs A,
+                                                                       uint64_t p0, uint64_t n, const void *mie_pack,
+                                                                       const float4 *dsun, const float4 *dsky,
+                                                                       const float *wpath, float *grad,
+                                                                       uint32_t copies, size_t stride,
+                                                                       DevCounters *C) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
+    uint32_t nstack[kMaxDepth];
+    const uint64_t k = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
+    grad += (size_t)(blockIdx.x % copies) * stride;
+    if (staged && k < n) {
+        const float w = wpath[k];
+        if (!isnan(w)) {
+            uint32_t i, j, s;
+            tile_path(A, p0 + k, i, j, s);
+            const size_t o = (size_t)j * A.tw + i;
+            const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
+            PathTotals tot{};
+            tot.w = w;
+            adjoint_pass<true>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
+                               f3(dk.x, dk.y, dk.z), tot, grad, nstack);
+        }
+    }
+    if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
 }
 
 // out[k] += sum over copies c of src[c * stride + k].
@@ -1226,21 +1266,31 @@ uint32_t adjoint_slots() { return kSlots; }
 
 cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                 const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
-                                uint32_t copies, double *grad_albedo, double *slots, DevCounters *C,
-                                cudaStream_t st) {
+                                uint32_t copies, float *wpath, uint64_t chunk, double *grad_albedo, double *slots,
+                                DevCounters *C, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
-    const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
-    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    if (chunk == 0 || (chunk + kRenderBlock - 1) / kRenderBlock > 0x7fffffffull) return cudaErrorInvalidValue;
     const size_t stride = (size_t)S.n_leaves * kBrick;
     const bool spread = copies > 1 && copies_buf;
+    cudaError_t e;
     if (spread) {
-        cudaError_t e = cudaMemsetAsync(copies_buf, 0, sizeof(float) * stride * copies, st);
+        e = cudaMemsetAsync(copies_buf, 0, sizeof(float) * stride * copies, st);
         if (e != cudaSuccess) return e;
     }
-    adjoint_tile_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(
-        S, P, A, mie_pack, dsun, dsky, spread ? copies_buf : grad, spread ? copies : 1u, stride, slots, C);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    const size_t smem = mie_smem(P);
+    for (uint64_t p0 = 0; p0 < A.n_paths; p0 += chunk) {
+        const uint64_t n = A.n_paths - p0 < chunk ? A.n_paths - p0 : chunk;
+        const unsigned blocks = (unsigned)((n + kRenderBlock - 1) / kRenderBlock);
+        adjoint_totals_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, wpath, slots,
+                                                                   C);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        adjoint_scatter_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, wpath,
+                                                                    spread ? copies_buf : grad,
+                                                                    spread ? copies : 1u, stride, C);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     if (spread) {
         sum_copies_kernel<<<592, 256, 0, st>>>(grad, copies_buf, copies, stride);
         e = cudaGetLastError();

@@ -42,11 +42,13 @@ cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, co
 // copies > 1: gradients are first spread over `copies` zeroed copies in
 // copies_buf (copies * n_leaves * 512 floats), then summed into grad.
 // The albedo gradient is gathered in adjoint_slots() zeroed doubles (slots),
-// then added to *grad_albedo (and the slots zeroed again).
+// then added to *grad_albedo (and the slots zeroed again).  The paths run in
+// chunks of `chunk`: a totals launch writes one weight per path to wpath
+// (chunk floats), then a scatter launch replays the chunk's paths.
 cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                 const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
-                                uint32_t copies, double *grad_albedo, double *slots, DevCounters *C,
-                                cudaStream_t st);
+                                uint32_t copies, float *wpath, uint64_t chunk, double *grad_albedo, double *slots,
+                                DevCounters *C, cudaStream_t st);
 uint32_t adjoint_slots();
 cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
                                          const float *wr, uint32_t n_rays, uint64_t nsamp, uint64_t seed, float *grad,

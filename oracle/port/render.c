@@ -415,12 +415,9 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
         float td;
         int res;
         if (scatter) {
-            float rs[3], rk[3];
-            for (int k = 0; k < 3; ++k) {
-                rs[k] = tot[k] - acc_sun[k];
-                rk[k] = tot[3 + k] - acc_sky[k];
-            }
-            sc.w = dot3v(dsun, rs) + dot3v(dsky, rk);
+            /* C_after weight: the path's total weight minus what it added before */
+            const float wtot = dot3v(dsun, tot) + dot3v(dsky, tot + 3);
+            sc.w = wtot - (dot3v(dsun, acc_sun) + dot3v(dsky, acc_sky));
             res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, scatter_visit, &sc);
         } else {
             res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, 0, 0);
