@@ -94,7 +94,7 @@ int dr_destroy(dr_ctx *c) {
         c->leaf_nodes.release();
         c->grad_copies.release();
         c->albedo_slots.release();
-        c->path_w.release();
+        c->path_rec.release();
         c->band_work.release();
         for (int k = 0; k < 2; ++k)
             if (c->band_stream[k]) cudaStreamSynchronize(c->band_stream[k]), cudaStreamDestroy(c->band_stream[k]);
@@ -602,12 +602,12 @@ int dr_adjoint_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint
         DR_CUDA(c->albedo_slots.reserve(adjoint_slots()), "adjoint: alloc slots");
         DR_CUDA(cudaMemset(c->albedo_slots.p, 0, sizeof(double) * adjoint_slots()), "adjoint: clear slots");
     }
-    // one weight per path of a chunk (at most 2^24 paths, 64 MB)
-    const uint64_t chunk = std::min<uint64_t>(A.n_paths, 1ull << 24);
-    DR_CUDA(c->path_w.reserve(chunk), "adjoint: alloc path weights");
+    // one 16-byte record per path of a chunk (at most 2^23 paths, 128 MB)
+    const uint64_t chunk = std::min<uint64_t>(A.n_paths, 1ull << 23);
+    DR_CUDA(c->path_rec.reserve(chunk), "adjoint: alloc path records");
     DR_CUDA(launch_adjoint_tile(c->scene, c->params, A, c->mie_pack.p, (const float4 *)dsun_dev,
                                 (const float4 *)dsky_dev, grad_bricks_dev, copies > 1 ? c->grad_copies.p : nullptr,
-                                copies, c->path_w.p, chunk, grad_albedo_dev, c->albedo_slots.p, c->counters.p, st),
+                                copies, c->path_rec.p, chunk, grad_albedo_dev, c->albedo_slots.p, c->counters.p, st),
             "adjoint: launch");
     return DR_OK;
 }

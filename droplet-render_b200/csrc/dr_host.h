@@ -117,7 +117,7 @@ struct dr_ctx {
     dr::DevBuf<uint32_t> leaf_nodes;  // ids of the leaf nodes (majorant updates)
     dr::DevBuf<float> grad_copies;    // adjoint: spread copies of the brick-pool gradient
     dr::DevBuf<double> albedo_slots;  // adjoint: partial sums of the albedo gradient (kept zeroed)
-    dr::DevBuf<float> path_w;         // adjoint: one weight per path of a chunk (totals pass -> scatter pass)
+    dr::DevBuf<uint4> path_rec;       // adjoint: one record per path of a chunk (totals pass -> scatter pass)
     uint32_t n_leaf_nodes = 0;
     bool use_grid = true;
     dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};

@@ -784,10 +784,20 @@ __device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, 
     return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, sv);
 }
 
+constexpr uint32_t kEscBits = 64;  // shadow segments whose outcome pass 1 records
+
 struct PathTotals {
     float w;            // dsun . (sun contribution) + dsky . (sky contribution) of the whole path
+    uint64_t esc;       // bit r: the shadow segment after scattering event r escaped (r < kEscBits)
     float3 asun, asky;  // sum over contributions of (scattering events before it) * contribution
     bool ok;            // every component of the path's contribution is finite
+};
+
+// What pass 1 keeps per path for pass 2 (16 bytes): the weight (NaN: path left
+// out) and the shadow-escape bits.
+struct __align__(16) PathRecord {
+    float w;
+    uint32_t esc_lo, esc_hi, pad;
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -845,21 +855,32 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         const float q1 = sun_hit(P, srd) ? P.sun_pdf : 0.0f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
-        const Rng g0 = g;
+        const bool hit = sun_hit(P, lrd);
+        const float3 cn = f3((T0 * ((p3.x / (p3.x + p2)) * f)) * (hit ? P.sun_color[0] : 0.0f),
+                             (T1 * ((p3.y / (p3.y + p2)) * f)) * (hit ? P.sun_color[1] : 0.0f),
+                             (T2 * ((p3.z / (p3.z + p2)) * f)) * (hit ? P.sun_color[2] : 0.0f));
         float tds;
-        if (track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped) {
-            const bool hit = sun_hit(P, lrd);
-            const float3 cn = f3((T0 * ((p3.x / (p3.x + p2)) * f)) * (hit ? P.sun_color[0] : 0.0f),
-                                 (T1 * ((p3.y / (p3.y + p2)) * f)) * (hit ? P.sun_color[1] : 0.0f),
-                                 (T2 * ((p3.z / (p3.z + p2)) * f)) * (hit ? P.sun_color[2] : 0.0f));
-            if constexpr (SCATTER) {
-                ScatterVisit sv{dot3f(dsun, cn), grad, S.bricks};
+        uint32_t sres;
+        if constexpr (SCATTER) {
+            // segments 0..63: pass 1 recorded whether the shadow escapes, so it
+            // is tracked once with its weight (zero unless it escapes)
+            const bool known = r < kEscBits;
+            const Rng g0 = g;
+            ScatterVisit sv{(known && ((tot.esc >> r) & 1ull)) ? dot3f(dsun, cn) : 0.0f, grad, S.bricks};
+            sres = track_scatter(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
+            if (!known && sres == kTrackEscaped) {
+                sv.w = dot3f(dsun, cn);
                 if (sv.w != 0.0f) {
                     Rng g1 = g0;  // the same draws again: ends in the state g already holds
                     float t2;
                     (void)track_scatter(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
                 }
             }
+        } else {
+            sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
+            if (sres == kTrackEscaped && r < kEscBits) tot.esc |= 1ull << r;
+        }
+        if (sres == kTrackEscaped) {
             const float m = (float)(r + 1);
             acc_sun = f3(acc_sun.x + cn.x, acc_sun.y + cn.y, acc_sun.z + cn.z);
             a_sun = f3(a_sun.x + m * cn.x, a_sun.y + m * cn.y, a_sun.z + m * cn.z);
@@ -924,14 +945,14 @@ __device__ __forceinline__ void tile_path(const TileArgs &A, uint64_t gi, uint32
 }
 
 // Pass 1 over paths [p0, p0 + n) of a tile (delta images in tile layout,
-// tw x th float4, rgb used): wpath[gi - p0] = the path's dsun . C_sun + dsky .
-// C_sky, NaN for a path left out (zero delta at its pixel, or a contribution
-// that is not finite, the sky term's 0/0 for rd.y == 0); the albedo term goes
-// to the slots.
+// tw x th float4, rgb used): rec[gi - p0] = the path's weight dsun . C_sun +
+// dsky . C_sky (NaN for a path left out: zero delta at its pixel, or a
+// contribution that is not finite, the sky term's 0/0 for rd.y == 0) and its
+// shadow-escape bits; the albedo term goes to the slots.
 __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S, DevParams P, TileArgs A,
                                                                       uint64_t p0, uint64_t n, const void *mie_pack,
                                                                       const float4 *dsun, const float4 *dsky,
-                                                                      float *wpath, double *albedo_slots,
+                                                                      PathRecord *rec, double *albedo_slots,
                                                                       DevCounters *C) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
@@ -946,17 +967,19 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S
         const size_t o = (size_t)j * A.tw + i;
         const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
         const float3 dsun3 = f3(ds.x, ds.y, ds.z), dsky3 = f3(dk.x, dk.y, dk.z);
-        float w = __int_as_float(0x7fffffff);
+        PathRecord pr{__int_as_float(0x7fffffff), 0u, 0u, 0u};
         if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
             PathTotals tot{};
             adjoint_pass<false>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
                                 nstack);
             if (tot.ok) {
-                w = tot.w;
+                pr.w = tot.w;
+                pr.esc_lo = (uint32_t)tot.esc;
+                pr.esc_hi = (uint32_t)(tot.esc >> 32);
                 galb = (dot3f(dsun3, tot.asun) + dot3f(dsky3, tot.asky)) / P.albedo;
             }
         }
-        wpath[k] = w;
+        rec[k] = pr;
     }
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
     warp_add(galb, albedo_slots);
@@ -970,7 +993,7 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S
 __global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene S, DevParams P, TileArgs A,
                                                                        uint64_t p0, uint64_t n, const void *mie_pack,
                                                                        const float4 *dsun, const float4 *dsky,
-                                                                       const float *wpath, float *grad,
+                                                                       const PathRecord *rec, float *grad,
                                                                        uint32_t copies, size_t stride,
                                                                        DevCounters *C) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -981,14 +1004,15 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene 
     const uint64_t k = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
     grad += (size_t)(blockIdx.x % copies) * stride;
     if (staged && k < n) {
-        const float w = wpath[k];
-        if (!isnan(w)) {
+        const PathRecord pr = rec[k];
+        if (!isnan(pr.w)) {
             uint32_t i, j, s;
             tile_path(A, p0 + k, i, j, s);
             const size_t o = (size_t)j * A.tw + i;
             const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
             PathTotals tot{};
-            tot.w = w;
+            tot.w = pr.w;
+            tot.esc = ((uint64_t)pr.esc_hi << 32) | pr.esc_lo;
             adjoint_pass<true>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
                                f3(dk.x, dk.y, dk.z), tot, grad, nstack);
         }
@@ -1266,7 +1290,7 @@ uint32_t adjoint_slots() { return kSlots; }
 
 cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                 const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
-                                uint32_t copies, float *wpath, uint64_t chunk, double *grad_albedo, double *slots,
+                                uint32_t copies, void *records, uint64_t chunk, double *grad_albedo, double *slots,
                                 DevCounters *C, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
     if (chunk == 0 || (chunk + kRenderBlock - 1) / kRenderBlock > 0x7fffffffull) return cudaErrorInvalidValue;
@@ -1278,14 +1302,15 @@ cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const Til
         if (e != cudaSuccess) return e;
     }
     const size_t smem = mie_smem(P);
+    PathRecord *rec = (PathRecord *)records;
     for (uint64_t p0 = 0; p0 < A.n_paths; p0 += chunk) {
         const uint64_t n = A.n_paths - p0 < chunk ? A.n_paths - p0 : chunk;
         const unsigned blocks = (unsigned)((n + kRenderBlock - 1) / kRenderBlock);
-        adjoint_totals_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, wpath, slots,
+        adjoint_totals_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, rec, slots,
                                                                    C);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        adjoint_scatter_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, wpath,
+        adjoint_scatter_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, rec,
                                                                     spread ? copies_buf : grad,
                                                                     spread ? copies : 1u, stride, C);
         e = cudaGetLastError();

@@ -43,11 +43,12 @@ cudaError_t launch_probe_transmittance(const DevScene &S, const DevParams &P, co
 // copies_buf (copies * n_leaves * 512 floats), then summed into grad.
 // The albedo gradient is gathered in adjoint_slots() zeroed doubles (slots),
 // then added to *grad_albedo (and the slots zeroed again).  The paths run in
-// chunks of `chunk`: a totals launch writes one weight per path to wpath
-// (chunk floats), then a scatter launch replays the chunk's paths.
+// chunks of `chunk`: a totals launch writes a 16-byte record per path to
+// records (chunk records: the path's weight and which shadow segments escape),
+// then a scatter launch replays the chunk's paths.
 cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                 const float4 *dsun, const float4 *dsky, float *grad, float *copies_buf,
-                                uint32_t copies, float *wpath, uint64_t chunk, double *grad_albedo, double *slots,
+                                uint32_t copies, void *records, uint64_t chunk, double *grad_albedo, double *slots,
                                 DevCounters *C, cudaStream_t st);
 uint32_t adjoint_slots();
 cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
