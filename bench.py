@@ -367,7 +367,10 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
     CUDA events; checks the gradient against central finite differences with
     common random numbers (eps 1e-3, majorants held fixed) on 256 random
     voxels (default_rng(5)): per seed group, the directional derivative along
-    random signs on those voxels."""
+    random signs on those voxels.  Two difference quotients: of the plain
+    render (decisions that flip make it noisy at this eps), and of the
+    reweighted replay on the adjoint's own streams (decisions from the base
+    bricks weighted by their probability ratios: smooth in eps)."""
     import torch
 
     from droplet_b200 import adjoint as AD
@@ -447,6 +450,20 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
             r.synchronize()
         return g, float(ga.item())
 
+    def reweighted_at(pert, seed):
+        # decisions from the uploaded base bricks, each weighted by its
+        # probability ratio under pert: smooth in the perturbation
+        r.set_bricks_dev(base.data_ptr(), nl, 0.0)
+        tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+        for k, v in enumerate(views):
+            r.set_params(AD._with_albedo(v, a0))
+            d4 = torch.zeros((256, 256, 4), device="cuda")
+            d4[..., :3] = delta[k] / fd_spp
+            r.reweighted_loss_async(0, 0, 256, 256, fd_spp, seed + k, 0, d4.data_ptr(), d4.data_ptr(),
+                                    pert.data_ptr(), tot.data_ptr())
+            r.synchronize()
+        return float(tot.item())
+
     # linearised loss: delta = dL/dI at the base point, so both estimators
     # target the same derivative of the expected image
     a0 = 0.99
@@ -454,7 +471,9 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
         dv = [AD.DiffView(v, fd_spp, 50000 + k) for k, v in enumerate(views)]
         sun, sky = AD.render(base, torch.tensor(a0, device="cuda"), r, dv, majorant_scale=0.0)
         delta = 2 * ((sun + sky)[..., :3] - target)
-    fd, ad, fa, aa = [], [], [], []
+    fd, ad, fa, aa, fr = [], [], [], [], []
+    pert_p = (base + eps * u).contiguous()
+    pert_m = (base - eps * u).contiguous()
     t = time.time()
     # the one-thread-per-path kernel sums each pixel's 32-sample groups in a
     # fixed order: the two renders of a difference share their rounding
@@ -464,10 +483,11 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
         seed = 70000 + 1000 * gi
         fd.append((loss_at(base + eps * u, a0, seed) - loss_at(base - eps * u, a0, seed)) / (2 * eps))
         fa.append((loss_at(base, a0 + ea, seed) - loss_at(base, a0 - ea, seed)) / (2 * ea))
+        fr.append((reweighted_at(pert_p, seed) - reweighted_at(pert_m, seed)) / (2 * eps))
         g, ga = adjoint_at(a0, seed)
         ad.append(float((g * u).sum()))
         aa.append(ga)
-    fd, ad, fa, aa = np.array(fd), np.array(ad), np.array(fa), np.array(aa)
+    fd, ad, fa, aa, fr = np.array(fd), np.array(ad), np.array(fa), np.array(aa), np.array(fr)
     diff = fd - ad
     r.set_tuning(*saved)
     return {
@@ -481,6 +501,10 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
                      "mean_fd": float(fd.mean()), "mean_adjoint": float(ad.mean()),
                      "rel_diff_of_means": float(abs(fd.mean() - ad.mean()) / max(abs(ad.mean()), 1e-30)),
                      "se_of_diff": float(diff.std(ddof=1) / np.sqrt(len(diff))),
+                     "reweighted": {"eps": eps, "fd": fr.tolist(), "adjoint": ad.tolist(),
+                                    "max_rel_diff": float(np.max(np.abs(fr - ad) / np.maximum(np.abs(ad), 1e-30))),
+                                    "rel_diff_of_means": float(abs(fr.mean() - ad.mean())
+                                                               / max(abs(ad.mean()), 1e-30))},
                      "albedo": {"eps": ea, "fd": fa.tolist(), "adjoint": aa.tolist(),
                                 "max_rel_diff": float(np.max(np.abs(fa - aa) / np.maximum(np.abs(fa), 1e-30)))},
                      "seconds": round(time.time() - t, 1)},
@@ -857,7 +881,8 @@ def run_b200(args):
                                   fd_eps=args.fd_eps)
         log(f"adjoint: forward {adjoint['forward_ms']:.1f} ms, adjoint {adjoint['adjoint_ms']:.1f} ms, "
             f"ratio {adjoint['adjoint_over_forward']:.2f}, fd {adjoint['fd_check']['mean_fd']:.4g} "
-            f"vs {adjoint['fd_check']['mean_adjoint']:.4g}")
+            f"vs {adjoint['fd_check']['mean_adjoint']:.4g}, reweighted fd max rel diff "
+            f"{adjoint['fd_check']['reweighted']['max_rel_diff']:.2e}")
 
     large = None
     if rank == 0 and world == 1 and not args.no_large:

@@ -612,6 +612,27 @@ int dr_adjoint_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint
     return DR_OK;
 }
 
+int dr_reweighted_loss_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
+                             uint64_t seed, uint64_t sample_base, const float *dsun_dev, const float *dsky_dev,
+                             const float *pert_bricks_dev, double *loss_dev, void *stream) {
+    if (!c || !dsun_dev || !dsky_dev || !pert_bricks_dev || !loss_dev)
+        return need(false, DR_ERR_INVALID, "dr_reweighted_loss_async: null argument");
+    TileArgs A;
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, 0u, A);
+    if (rc != DR_OK) return rc;
+    DeviceGuard g(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (!c->albedo_slots.p) {
+        DR_CUDA(c->albedo_slots.reserve(adjoint_slots()), "reweighted loss: alloc slots");
+        DR_CUDA(cudaMemset(c->albedo_slots.p, 0, sizeof(double) * adjoint_slots()), "reweighted loss: clear slots");
+    }
+    DR_CUDA(launch_reweighted_loss(c->scene, c->params, A, c->mie_pack.p, (const float4 *)dsun_dev,
+                                   (const float4 *)dsky_dev, pert_bricks_dev, loss_dev, c->albedo_slots.p,
+                                   c->counters.p, st),
+            "reweighted loss: launch");
+    return DR_OK;
+}
+
 int dr_adjoint_transmittance(dr_ctx *c, const float *ro, const float *rd, const float *weights, uint32_t n,
                              uint64_t nsamp, uint64_t seed, float *grad_bricks, double *transmittance) {
     if (!c || !ro || !rd || !weights || !grad_bricks || n == 0 || nsamp == 0)

@@ -786,6 +786,35 @@ __device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, 
 
 constexpr uint32_t kEscBits = 64;  // shadow segments whose outcome pass 1 records
 
+// Reweighted replay (the finite-difference check of the adjoint): decisions are
+// drawn from the context's bricks, and each is weighted by its probability under
+// a perturbed brick pool over its probability under the drawn one (rho'/rho
+// for real, (smax - rho')/(smax - rho) for null).  The weighted estimator is
+// unbiased for the perturbed image and smooth in the perturbation, so its
+// central differences with common random numbers are not swamped by decisions
+// that flip.
+struct RatioVisit {
+    float *w;  // running product of the segment's ratios
+    const float *pert;
+    const float *bricks;
+    __device__ __forceinline__ void operator()(const float *brick, const float4 &ce, const float *rc, float rho,
+                                               float smax, bool real) const {
+        const float rp = sample_voxel_space(rc, pert + (brick - bricks), ce);
+        if (real) {
+            if (rho > 0.0f) *w = *w * (rp / rho);
+        } else {
+            const float d = smax - rho;
+            if (d > 0.0f) *w = *w * ((smax - rp) / d);
+        }
+    }
+};
+
+__device__ __noinline__ uint32_t track_ratio(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
+                                             float depth, float &td, uint32_t *nstack, Count &cnt,
+                                             const RatioVisit &rv) {
+    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, rv);
+}
+
 struct PathTotals {
     float w;            // dsun . (sun contribution) + dsky . (sky contribution) of the whole path
     uint64_t esc;       // bit r: the shadow segment after scattering event r escaped (r < kEscBits)
@@ -803,11 +832,16 @@ struct __align__(16) PathRecord {
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
 __device__ __forceinline__ float dot3f(const float3 a, const float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-// Pass 1 (SCATTER = false): fills tot.  Pass 2: scatters with tot known.
-template <bool SCATTER>
+// MODE kPassTotals fills tot; kPassScatter scatters with tot known;
+// kPassRatio fills tot.w for the reweighted replay (pert = perturbed bricks).
+enum : int { kPassTotals = 0, kPassScatter = 1, kPassRatio = 2 };
+template <int MODE>
 __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
                                              uint32_t py, uint64_t seed, uint64_t sample, float3 dsun, float3 dsky,
-                                             PathTotals &tot, float *grad, uint32_t *nstack) {
+                                             PathTotals &tot, float *grad, uint32_t *nstack,
+                                             const float *pert = nullptr) {
+    constexpr bool SCATTER = MODE == kPassScatter;
+    constexpr bool RATIO = MODE == kPassRatio;
     float ro[3], rd[3];
     if (!camera_ray(P, px, py, ro, rd)) return;
     Count cnt;
@@ -824,6 +858,14 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         if constexpr (SCATTER) {
             vis.w = tot.w - (dot3f(dsun, acc_sun) + dot3f(dsky, acc_sky));
             res = track_scatter(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
+        } else if constexpr (RATIO) {
+            // the segment's ratios scale everything the path adds from here on
+            float ws = 1.0f;
+            const RatioVisit rv{&ws, pert, S.bricks};
+            res = track_ratio(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, rv);
+            T0 = T0 * ws;
+            T1 = T1 * ws;
+            T2 = T2 * ws;
         } else {
             res = track_plain(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
         }
@@ -856,7 +898,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         const bool hit = sun_hit(P, lrd);
-        const float3 cn = f3((T0 * ((p3.x / (p3.x + p2)) * f)) * (hit ? P.sun_color[0] : 0.0f),
+        float3 cn = f3((T0 * ((p3.x / (p3.x + p2)) * f)) * (hit ? P.sun_color[0] : 0.0f),
                              (T1 * ((p3.y / (p3.y + p2)) * f)) * (hit ? P.sun_color[1] : 0.0f),
                              (T2 * ((p3.z / (p3.z + p2)) * f)) * (hit ? P.sun_color[2] : 0.0f));
         float tds;
@@ -876,6 +918,11 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
                     (void)track_scatter(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
                 }
             }
+        } else if constexpr (RATIO) {
+            float ws = 1.0f;
+            const RatioVisit rv{&ws, pert, S.bricks};
+            sres = track_ratio(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
+            cn = f3(cn.x * ws, cn.y * ws, cn.z * ws);
         } else {
             sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
             if (sres == kTrackEscaped && r < kEscBits) tot.esc |= 1ull << r;
@@ -970,7 +1017,7 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S
         PathRecord pr{__int_as_float(0x7fffffff), 0u, 0u, 0u};
         if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
             PathTotals tot{};
-            adjoint_pass<false>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
+            adjoint_pass<kPassTotals>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
                                 nstack);
             if (tot.ok) {
                 pr.w = tot.w;
@@ -1013,11 +1060,53 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene 
             PathTotals tot{};
             tot.w = pr.w;
             tot.esc = ((uint64_t)pr.esc_hi << 32) | pr.esc_lo;
-            adjoint_pass<true>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
+            adjoint_pass<kPassScatter>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
                                f3(dk.x, dk.y, dk.z), tot, grad, nstack);
         }
     }
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
+}
+
+// Warp-wide double sum added to one of kSlots accumulators (as warp_add).
+__device__ __forceinline__ void warp_add_d(double v, double *slots) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) {
+        const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        atomicAdd(&slots[w % kSlots], v);
+    }
+}
+
+// Reweighted replay of a tile's paths: the linearised loss sum over paths of
+// dsun . C_sun + dsky . C_sky, each path weighted by its decisions' ratios
+// under pert (paths whose contribution is not finite are left out, as in the
+// adjoint).
+__global__ void __launch_bounds__(kRenderBlock) reweighted_loss_kernel(DevScene S, DevParams P, TileArgs A,
+                                                                       const void *mie_pack, const float4 *dsun,
+                                                                       const float4 *dsky, const float *pert,
+                                                                       double *slots, DevCounters *C) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    const bool staged = stage_mie(mie_pack, mie_bytes(P), smem, &mbar);
+    const MieSmem M = mie_view(P, smem);
+    uint32_t nstack[kMaxDepth];
+    const uint64_t k = (uint64_t)blockIdx.x * kRenderBlock + threadIdx.x;
+    double l = 0.0;
+    if (staged && k < A.n_paths) {
+        uint32_t i, j, s;
+        tile_path(A, k, i, j, s);
+        const size_t o = (size_t)j * A.tw + i;
+        const float4 ds = __ldg(&dsun[o]), dk = __ldg(&dsky[o]);
+        const float3 dsun3 = f3(ds.x, ds.y, ds.z), dsky3 = f3(dk.x, dk.y, dk.z);
+        if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
+            PathTotals tot{};
+            adjoint_pass<kPassRatio>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot,
+                                     nullptr, nstack, pert);
+            if (tot.ok) l = (double)tot.w;
+        }
+    }
+    if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
+    warp_add_d(l, slots);
 }
 
 // out[k] += sum over copies c of src[c * stride + k].
@@ -1322,6 +1411,21 @@ cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const Til
         if (e != cudaSuccess) return e;
     }
     sum_slots_kernel<<<1, 256, 0, st>>>(grad_albedo, slots);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reweighted_loss(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                   const float4 *dsun, const float4 *dsky, const float *pert, double *loss,
+                                   double *slots, DevCounters *C, cudaStream_t st) {
+    if (A.n_paths > 0) {
+        const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
+        if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+        reweighted_loss_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, dsun, dsky,
+                                                                                    pert, slots, C);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    sum_slots_kernel<<<1, 256, 0, st>>>(loss, slots);
     return cudaGetLastError();
 }
 

@@ -51,6 +51,11 @@ cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const Til
                                 uint32_t copies, void *records, uint64_t chunk, double *grad_albedo, double *slots,
                                 DevCounters *C, cudaStream_t st);
 uint32_t adjoint_slots();
+// Reweighted replay of a tile (decisions from S's bricks, weights from pert):
+// adds the linearised loss to *loss through the zeroed slots.
+cudaError_t launch_reweighted_loss(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                                   const float4 *dsun, const float4 *dsky, const float *pert, double *loss,
+                                   double *slots, DevCounters *C, cudaStream_t st);
 cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, const float *ro, const float *rd,
                                          const float *wr, uint32_t n_rays, uint64_t nsamp, uint64_t seed, float *grad,
                                          unsigned long long *escapes, cudaStream_t st);

@@ -162,6 +162,11 @@ SIGNATURES = {
         [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     ),
+    "dr_reweighted_loss_async": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
+         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    ),
     "dr_adjoint_transmittance": (
         C.c_int,
         [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p],

@@ -206,6 +206,16 @@ class Renderer:
                                               C.c_void_p(dsun_ptr), C.c_void_p(dsky_ptr), C.c_void_p(grad_ptr),
                                               C.c_void_p(galb_ptr), C.c_void_p(stream_ptr) if stream_ptr else None))
 
+    def reweighted_loss_async(self, x0, y0, tw, th, spp, seed, sample_base, dsun_ptr: int, dsky_ptr: int,
+                              pert_ptr: int, loss_ptr: int, stream_ptr: int = 0):
+        """Adds to the double at loss_ptr the linearised loss of the tile's paths
+        replayed with decisions from the uploaded bricks, each weighted by its
+        probability ratio under the bricks at pert_ptr (the adjoint's
+        finite-difference check)."""
+        N.check(N.lib().dr_reweighted_loss_async(self._ctx, x0, y0, tw, th, spp, int(seed), int(sample_base),
+                                                 C.c_void_p(dsun_ptr), C.c_void_p(dsky_ptr), C.c_void_p(pert_ptr),
+                                                 C.c_void_p(loss_ptr), C.c_void_p(stream_ptr) if stream_ptr else None))
+
     def adjoint_transmittance(self, ro, rd, weights, nsamp: int, seed: int, n_leaves: int):
         """(d sum_r w_r T_r / d brick samples (n_leaves, 512), T per ray) on the GPU."""
         ro = np.ascontiguousarray(ro, np.float32).reshape(-1)

@@ -237,6 +237,19 @@ int dr_get_majorants(dr_ctx *ctx, float *out);
 int dr_adjoint_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
                           uint64_t seed, uint64_t sample_base, const float *dsun_dev, const float *dsky_dev,
                           float *grad_bricks_dev, double *grad_albedo_dev, void *stream);
+/* Gradient check of dr_adjoint_tile_async: replays the same paths with every
+ * delta-tracking decision drawn from the context's bricks and weighted by its
+ * probability under pert_bricks_dev (n_leaves * 512 floats, same majorants)
+ * over its probability under the context's bricks, and ADDS the linearised
+ * loss  sum over paths of dsun . C_sun + dsky . C_sky  (dsun / dsky as in the
+ * adjoint) into *loss_dev.  Unbiased for the loss of the perturbed field and
+ * smooth in the perturbation: central differences of it with common random
+ * numbers estimate the gradient the adjoint returns.  With pert_bricks_dev =
+ * the context's bricks it is the plain estimator's loss.  Enqueued on stream
+ * (NULL = context stream). */
+int dr_reweighted_loss_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
+                             uint64_t seed, uint64_t sample_base, const float *dsun_dev, const float *dsky_dev,
+                             const float *pert_bricks_dev, double *loss_dev, void *stream);
 /* Transmittance of n rays (ro, rd: 3n floats) by delta tracking over nsamp
  * samples (streams (seed, ray, sample)) and the gradient of
  * sum_r weights[r] * T_r with respect to the brick samples (host buffers:

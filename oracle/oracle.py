@@ -86,6 +86,9 @@ class Port:
         L.orc_adjoint_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                           C.c_uint64, C.c_uint64, vp, vp, vp, vp, C.c_int]
         L.orc_adjoint_tile_mt.restype = C.c_int
+        L.orc_reweighted_loss.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
+                                          C.c_uint64, C.c_uint64, vp, vp, vp]
+        L.orc_reweighted_loss.restype = C.c_double
         L.orc_adjoint_transmittance.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), vp, vp, vp, u32,
                                                 C.c_uint64, C.c_uint64, vp, vp]
         L.orc_mie_exact_table.argtypes = [vp, u32, vp]
@@ -219,6 +222,15 @@ class Port:
         if rc != 0:
             raise MemoryError("orc_adjoint_tile_mt")
         return grad.reshape(-1, 512), float(galb[0])
+
+    def reweighted_loss(self, S, P, x0, y0, tw, th, spp, seed, sample_base, dsun, dsky, pert):
+        """Linearised loss of the reweighted replay: decisions from the scene's
+        bricks, each weighted by its probability ratio under pert (n_leaves, 512)."""
+        dsun = np.ascontiguousarray(dsun, np.float32)
+        dsky = np.ascontiguousarray(dsky, np.float32)
+        pert = np.ascontiguousarray(pert, np.float32)
+        return float(self.L.orc_reweighted_loss(C.byref(S), C.byref(P), x0, y0, tw, th, spp, seed, sample_base,
+                                                _p(dsun), _p(dsky), _p(pert)))
 
     def adjoint_transmittance(self, S, P, ro, rd, w, nsamp, seed):
         ro = np.ascontiguousarray(ro, np.float32)

@@ -139,6 +139,10 @@ void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
 int orc_adjoint_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
                         uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
                         double *grad, double *galb, int nthreads);
+/* Linearised loss of the reweighted replay (decisions from S->bricks, ratios under pert). */
+double orc_reweighted_loss(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                           uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
+                           const float *pert);
 /* Gradient of sum_r w_r T_r (delta-tracking transmittance over nsamp samples). */
 void orc_adjoint_transmittance(const orc_scene *S, const orc_params *P, const float *ro, const float *rd,
                                const float *wr, uint32_t n, uint64_t nsamp, uint64_t seed, double *grad, double *T);

@@ -396,10 +396,32 @@ static void scatter_visit(void *vctx, const float *brick, const float ce[4], con
 
 static inline float dot3v(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
-/* pass 0 fills tot[12] (sun, sky, m*sun, m*sky); pass 1 scatters with tot known */
+/* reweighted replay: each decision drawn from S->bricks is weighted by its
+ * probability under pert over its probability under S->bricks */
+typedef struct {
+    float w;
+    const float *pert, *bricks;
+    uint32_t N;
+} ratio_ctx;
+
+static void ratio_visit(void *vctx, const float *brick, const float ce[4], const float rc[3], float rho, float smax,
+                        int real) {
+    ratio_ctx *c = (ratio_ctx *)vctx;
+    const float rp = orc_sample_voxel_space(rc, c->pert + (brick - c->bricks), ce, c->N);
+    if (real) {
+        if (rho > 0.0f) c->w = c->w * (rp / rho);
+    } else {
+        const float d = smax - rho;
+        if (d > 0.0f) c->w = c->w * ((smax - rp) / d);
+    }
+}
+
+/* pass 0 fills tot[12] (sun, sky, m*sun, m*sky); pass 1 scatters with tot known;
+ * pass 2 fills tot[0..5] with the reweighted replay's contribution (pert) */
 static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, uint32_t py, uint64_t seed,
                          uint64_t sample, const float dsun[3], const float dsky[3], float tot[12], double *grad,
-                         int scatter) {
+                         int pass, const float *pert) {
+    const int scatter = pass == 1, ratio = pass == 2;
     float ro[3], rd[3];
     int inf;
     orc_camera_ray(P, px, py, ro, rd, &inf);
@@ -419,6 +441,10 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
             const float wtot = dot3v(dsun, tot) + dot3v(dsky, tot + 3);
             sc.w = wtot - (dot3v(dsun, acc_sun) + dot3v(dsky, acc_sky));
             res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, scatter_visit, &sc);
+        } else if (ratio) {
+            ratio_ctx rv = {1.0f, pert, S->bricks, S->lvoxc};
+            res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, ratio_visit, &rv);
+            for (int k = 0; k < 3; ++k) T[k] = T[k] * rv.w;
         } else {
             res = track_depth_v(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, 0, 0, 0);
         }
@@ -453,10 +479,13 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         const orc_rng g0 = g;
         float tds;
-        if (track_depth_v(S, P, rc, lrd, &g, FLT_MAX, &tds, 0, 0, 0) == 1) {
+        ratio_ctx rs = {1.0f, pert, S->bricks, S->lvoxc};
+        if (track_depth_v(S, P, rc, lrd, &g, FLT_MAX, &tds, 0, ratio ? ratio_visit : 0, ratio ? &rs : 0) == 1) {
             float sun[3], cn[3];
             orc_sun_eval(P, lrd, sun);
             for (int k = 0; k < 3; ++k) cn[k] = (T[k] * ((p3[k] / (p3[k] + p2)) * f)) * sun[k];
+            if (ratio)
+                for (int k = 0; k < 3; ++k) cn[k] = cn[k] * rs.w;
             if (scatter) {
                 scatter_ctx sv = {dot3v(dsun, cn), grad, S->bricks, S->lvoxc};
                 if (sv.w != 0.0f) {
@@ -477,7 +506,7 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
             rd[k] = srd[k];
         }
     }
-    if (!scatter) {
+    if (!scatter) { /* passes 0 and 2 */
         for (int k = 0; k < 3; ++k) {
             tot[k] = acc_sun[k];
             tot[3 + k] = acc_sky[k];
@@ -506,11 +535,11 @@ static void *adj_worker(void *arg) {
             if (dot3v(ds, ds) + dot3v(dk, dk) > 0.0f)
                 for (uint32_t s = 0; s < J->spp; ++s) {
                     float tot[12] = {0};
-                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 0);
+                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 0, 0);
                     int ok = 1;
                     for (int k = 0; k < 6; ++k) ok = ok && isfinite(tot[k]);
                     if (!ok) continue; /* non-finite contribution: left out of the gradient */
-                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 1);
+                    adjoint_pass(J->S, J->P, J->x0 + i, J->y0 + j, J->seed, J->base + s, ds, dk, tot, J->grad, 1, 0);
                     J->galb += (double)((dot3v(ds, tot + 6) + dot3v(dk, tot + 9)) / f);
                 }
         }
@@ -547,6 +576,30 @@ int orc_adjoint_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, ui
     }
     *galb += ga;
     return 0;
+}
+
+/* Linearised loss of the reweighted replay (the GPU's dr_reweighted_loss_async):
+ * sum over the tile's paths of dsun . C_sun + dsky . C_sky, decisions from
+ * S->bricks weighted by their probability ratios under pert; a path whose
+ * contribution is not finite is left out. */
+double orc_reweighted_loss(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
+                           uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
+                           const float *pert) {
+    double l = 0.0;
+    const uint32_t cols = 2 * (tw / 2), rows = 2 * (th / 2);
+    for (uint32_t j = 0; j < rows; ++j)
+        for (uint32_t i = 0; i < cols; ++i) {
+            const float *ds = dsun + 4 * ((size_t)j * tw + i), *dk = dsky + 4 * ((size_t)j * tw + i);
+            if (!(dot3v(ds, ds) + dot3v(dk, dk) > 0.0f)) continue;
+            for (uint32_t s = 0; s < spp; ++s) {
+                float tot[12] = {0};
+                adjoint_pass(S, P, x0 + i, y0 + j, seed, sample_base + s, ds, dk, tot, 0, 2, pert);
+                int ok = 1;
+                for (int k = 0; k < 6; ++k) ok = ok && isfinite(tot[k]);
+                if (ok) l += (double)(dot3v(ds, tot) + dot3v(dk, tot + 3));
+            }
+        }
+    return l;
 }
 
 /* Gradient of sum_r w_r T_r over the brick samples (streams (seed, r, s)). */

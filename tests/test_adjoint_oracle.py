@@ -118,3 +118,40 @@ def test_sky_zero_over_zero_path_and_finite_paths_flag(port):
     P = port.params(cfg, keep)
     sun, sky, _ = port.render_path(S, P, px, py, NAN_PATH["seed"], NAN_PATH["sample"])
     assert (sky[:3] == 0).all() and (sun[:3] == 0).all() and sun[3] == 1.0
+
+
+def test_density_adjoint_matches_reweighted_finite_differences(port):
+    """The image adjoint's brick-sample derivative equals central differences of
+    the reweighted replay (decisions from the base bricks, each weighted by its
+    probability ratio under the perturbed bricks) on the same random streams;
+    with unperturbed bricks the reweighted loss is the plain render's."""
+    nodes, bricks, _ = golden_octree()
+    w = h = 24
+    spp = 16
+    cfg = c0_cfg(w, h)
+    S = port.scene(nodes, bricks)
+    keep = []
+    P = port.params(cfg, keep)
+    rng = np.random.default_rng(11)
+    dsun = rng.normal(size=(h, w, 4)).astype(np.float32)
+    dsky = rng.normal(size=(h, w, 4)).astype(np.float32)
+    base = np.asarray(bricks, np.float32).reshape(-1, 512)
+    sun, sky, _ = port.render_tile(S, P, 0, 0, w, h, spp, seed=5)
+    plain = float((dsun[..., :3].astype(np.float64) * sun[..., :3]).sum()
+                  + (dsky[..., :3].astype(np.float64) * sky[..., :3]).sum())
+    l0 = port.reweighted_loss(S, P, 0, 0, w, h, spp, 5, 0, dsun, dsky, base)
+    assert abs(l0 - plain) <= 1e-5 * abs(plain)
+    g, _ = port.adjoint_tile(S, P, 0, 0, w, h, spp, 5, 0, dsun, dsky)
+    flat = base.reshape(-1)
+    cand = np.flatnonzero(flat >= 0.05)
+    pick = rng.choice(cand, 256, replace=False)
+    u = np.zeros(flat.size, np.float32)
+    u[pick] = rng.choice([-1.0, 1.0], 256)
+    u = u.reshape(base.shape)
+    eps = 1e-3
+    lp = port.reweighted_loss(S, P, 0, 0, w, h, spp, 5, 0, dsun, dsky, base + eps * u)
+    lm = port.reweighted_loss(S, P, 0, 0, w, h, spp, 5, 0, dsun, dsky, base - eps * u)
+    fd = (lp - lm) / (2 * eps)
+    ad = float((g * u).sum())
+    assert abs(ad) > 0
+    assert abs(fd - ad) <= 1e-3 * abs(ad), (fd, ad)

@@ -227,3 +227,48 @@ def test_autograd_on_default_stream_matches_render(adj):
     assert np.allclose(got, ref, rtol=1e-5, atol=1e-6 * np.abs(ref).max())
     (sun + sky)[..., :3].sum().backward()
     assert float(albedo.grad) != 0.0 and float(b.grad.abs().sum()) > 0
+
+
+def test_reweighted_loss_equals_restatement_and_differences_match_adjoint(adj, port):
+    """dr_reweighted_loss_async equals the CPU restatement on the same streams,
+    and its central differences (eps 1e-3, common random numbers) along random
+    signs on 256 brick samples equal the adjoint's directional derivative."""
+    import torch
+
+    r, nodes, bricks = adj
+    cfg = c0_cfg(64, 64)
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    rng = np.random.default_rng(12)
+    tw, th, spp, seed = 48, 40, 16, 23
+    dsun = rng.normal(size=(th, tw, 4)).astype(np.float32)
+    dsky = rng.normal(size=(th, tw, 4)).astype(np.float32)
+    base = np.asarray(bricks, np.float32).reshape(-1, 512)
+    flat = base.reshape(-1)
+    pick = rng.choice(np.flatnonzero(flat >= 0.05), 256, replace=False)
+    u = np.zeros(flat.size, np.float32)
+    u[pick] = rng.choice([-1.0, 1.0], 256)
+    u = u.reshape(base.shape)
+    eps = 1e-3
+    r.set_params(settings_from_cfg(cfg))
+    ds = torch.as_tensor(dsun, device="cuda").contiguous()
+    dk = torch.as_tensor(dsky, device="cuda").contiguous()
+
+    def gpu_loss(pert):
+        pt = torch.as_tensor(np.ascontiguousarray(pert, np.float32), device="cuda")
+        out = torch.zeros(1, dtype=torch.float64, device="cuda")
+        r.reweighted_loss_async(8, 12, tw, th, spp, seed, 3, ds.data_ptr(), dk.data_ptr(), pt.data_ptr(),
+                                out.data_ptr())
+        torch.cuda.synchronize()
+        return float(out.item())
+
+    lp = gpu_loss(base + eps * u)
+    lp_cpu = port.reweighted_loss(S, P, 8, 12, tw, th, spp, seed, 3, dsun, dsky, base + eps * u)
+    assert abs(lp - lp_cpu) <= 1e-6 * abs(lp_cpu)
+    lm = gpu_loss(base - eps * u)
+    g, _ = _gpu_adjoint(r, cfg, 8, 12, tw, th, spp, seed, 3, dsun, dsky, len(bricks))
+    fd = (lp - lm) / (2 * eps)
+    ad = float((g * u).sum())
+    assert abs(ad) > 0
+    assert abs(fd - ad) <= 1e-3 * abs(ad), (fd, ad)
