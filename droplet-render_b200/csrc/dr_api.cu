@@ -95,6 +95,8 @@ int dr_destroy(dr_ctx *c) {
         c->grad_copies.release();
         c->albedo_slots.release();
         c->path_rec.release();
+        c->occ_nodes.release();
+        c->occ_tris.release();
         c->band_work.release();
         for (int k = 0; k < 2; ++k)
             if (c->band_stream[k]) cudaStreamSynchronize(c->band_stream[k]), cudaStreamDestroy(c->band_stream[k]);
@@ -138,6 +140,11 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
     std::lock_guard<std::mutex> lk(c->mu);
     rc = upload_scene(h, c->bufs, c->use_grid, c->stream, c->scene);
     if (rc != DR_OK) return rc;
+    if (c->occ_n_nodes) {
+        c->scene.occ_nodes = c->occ_nodes.p;
+        c->scene.occ_tris = c->occ_tris.p;
+        c->scene.occ_n_nodes = c->occ_n_nodes;
+    }
     std::vector<uint32_t> ln;
     for (uint32_t i = 0; i < h.n_nodes; ++i)
         if (h.leaf_flag[i]) ln.push_back(i);
@@ -148,6 +155,30 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
     c->n_leaf_nodes = (uint32_t)ln.size();
     c->leaf_flag = std::move(h.leaf_flag);
     c->has_scene = true;
+    return DR_OK;
+}
+
+int dr_set_occluders(dr_ctx *c, const dr_surface *surfaces, uint32_t n_surfaces, uint32_t mode) {
+    if (!c) return need(false, DR_ERR_INVALID, "dr_set_occluders: null argument");
+    OccBvh b;
+    int rc = build_occluder_bvh(surfaces, n_surfaces, mode, b);
+    if (rc != DR_OK) return rc;
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    DR_CUDA(cudaStreamSynchronize(c->stream), "dr_set_occluders: sync");
+    const uint32_t nn = (uint32_t)(b.nodes.size() / 16);
+    if (nn) {
+        DR_CUDA(c->occ_nodes.reserve((size_t)nn * 4), "dr_set_occluders: alloc nodes");
+        DR_CUDA(c->occ_tris.reserve(b.tris.size() / 4), "dr_set_occluders: alloc triangles");
+        DR_CUDA(cudaMemcpy(c->occ_nodes.p, b.nodes.data(), b.nodes.size() * sizeof(float), cudaMemcpyHostToDevice),
+                "dr_set_occluders: copy nodes");
+        DR_CUDA(cudaMemcpy(c->occ_tris.p, b.tris.data(), b.tris.size() * sizeof(float), cudaMemcpyHostToDevice),
+                "dr_set_occluders: copy triangles");
+    }
+    c->occ_n_nodes = nn;
+    c->scene.occ_nodes = nn ? c->occ_nodes.p : nullptr;
+    c->scene.occ_tris = nn ? c->occ_tris.p : nullptr;
+    c->scene.occ_n_nodes = nn;
     return DR_OK;
 }
 
@@ -431,6 +462,24 @@ int dr_probe_leaf_sequence(dr_ctx *c, const float *ro, const float *rd, uint32_t
     DR_CUDA(cudaMemcpy(tr0, b + o_t0, 4ull * n * maxn, cudaMemcpyDeviceToHost), "probe: copy out");
     DR_CUDA(cudaMemcpy(tr1, b + o_t1, 4ull * n * maxn, cudaMemcpyDeviceToHost), "probe: copy out");
     DR_CUDA(cudaMemcpy(counts, b + o_ct, 4ull * n, cudaMemcpyDeviceToHost), "probe: copy out");
+    return DR_OK;
+}
+
+int dr_probe_occlusion(dr_ctx *c, const float *ro, const float *rd, uint32_t n, uint32_t *hit) {
+    if (!c || !ro || !rd || !hit || n == 0) return need(false, DR_ERR_INVALID, "dr_probe_occlusion: bad argument");
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    Scratch S;
+    size_t o_o = S.add(12ull * n), o_d = S.add(12ull * n), o_h = S.add(4ull * n);
+    DR_CUDA(c->scratch.reserve(S.total), "probe: alloc");
+    unsigned char *b = c->scratch.p;
+    DR_CUDA(cudaMemcpy(b + o_o, ro, 12ull * n, cudaMemcpyHostToDevice), "probe: copy");
+    DR_CUDA(cudaMemcpy(b + o_d, rd, 12ull * n, cudaMemcpyHostToDevice), "probe: copy");
+    DR_CUDA(launch_probe_occlusion(c->scene, (const float *)(b + o_o), (const float *)(b + o_d), n,
+                                   (uint32_t *)(b + o_h), c->stream),
+            "probe: launch");
+    DR_CUDA(cudaStreamSynchronize(c->stream), "probe: sync");
+    DR_CUDA(cudaMemcpy(hit, b + o_h, 4ull * n, cudaMemcpyDeviceToHost), "probe: copy out");
     return DR_OK;
 }
 

@@ -786,6 +786,93 @@ __device__ __forceinline__ bool camera_ray(const DevParams &P, uint32_t px, uint
 // the distance of the collision (or of the last leaf exit).
 enum : uint32_t { kTrackCollided = 0, kTrackEscaped = 1, kTrackCut = 2 };
 
+// ---- occluders: SceneOcclusion::Intersect (src/SceneOcclusion.cpp:58-91) ----
+// Embree's query with tnear 0 and tfar MAX_OCCLUSION_DIST reports whether the
+// ray hits any occluder triangle; only that answer is used
+// (src/kernel.cpp:149-153, 375-383).  The triangle test is Moller-Trumbore
+// (1997) without culling, with the division by the determinant folded into
+// the comparisons: hit when u, v >= 0, u + v <= det and 0 <= t <= det * tfar
+// (signs reversed for det < 0; det == 0 is a miss).
+__device__ __forceinline__ bool occ_triangle(const float4 *__restrict__ T, uint32_t i, const float o[3],
+                                             const float d[3]) {
+    const float4 a = __ldg(&T[3 * (size_t)i]), e1 = __ldg(&T[3 * (size_t)i + 1]), e2 = __ldg(&T[3 * (size_t)i + 2]);
+    const float px = d[1] * e2.z - d[2] * e2.y, py = d[2] * e2.x - d[0] * e2.z, pz = d[0] * e2.y - d[1] * e2.x;
+    const float det = e1.x * px + e1.y * py + e1.z * pz;
+    const float sx = o[0] - a.x, sy = o[1] - a.y, sz = o[2] - a.z;
+    const float u = sx * px + sy * py + sz * pz;
+    const float qx = sy * e1.z - sz * e1.y, qy = sz * e1.x - sx * e1.z, qz = sx * e1.y - sy * e1.x;
+    const float v = d[0] * qx + d[1] * qy + d[2] * qz;
+    const float t = e2.x * qx + e2.y * qy + e2.z * qz;
+    const float uv = u + v;
+    if (det > 0.0f) return u >= 0.0f && v >= 0.0f && uv <= det && t >= 0.0f && t <= det * kOccFar;
+    if (det < 0.0f) return u <= 0.0f && v <= 0.0f && uv >= det && t <= 0.0f && t >= det * kOccFar;
+    return false;
+}
+
+// Slab test of a (padded) box against t in [0, tfar]; the far end is widened
+// by 1 + 2 gamma(3) (robust traversal, Ize 2013).  A zero direction component
+// gives infinite slab bounds, which fminf/fmaxf order correctly.
+__device__ __forceinline__ bool occ_box(float x0, float y0, float z0, float x1, float y1, float z1, const float o[3],
+                                        const float inv[3]) {
+    const float ax = (x0 - o[0]) * inv[0], bx = (x1 - o[0]) * inv[0];
+    const float ay = (y0 - o[1]) * inv[1], by = (y1 - o[1]) * inv[1];
+    const float az = (z0 - o[2]) * inv[2], bz = (z1 - o[2]) * inv[2];
+    const float t0 = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.0f));
+    const float t1 = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), kOccFar));
+    return t0 <= t1 * 1.00000048f;
+}
+
+// Any-hit traversal of the occluder BVH.  Every node is visited at most once,
+// so the loop ends within occ_n_nodes iterations; the stack holds at most one
+// entry per level of the (depth-capped) tree.  Not inlined: its stack then sits
+// in its own frame.  Inlined into the shadow-pass kernel, the kernel's local
+// frame came out smaller (384 B) than its node and interval stacks need at once
+// (448 B), and that kernel read out of bounds; every caller's frame now holds
+// all three stacks.
+__device__ __noinline__ bool occluded_bvh(const float4 *__restrict__ nodes, const float4 *__restrict__ tris,
+                                          uint32_t n_nodes, float ox, float oy, float oz, float dx, float dy,
+                                          float dz) {
+    const float o[3] = {ox, oy, oz}, d[3] = {dx, dy, dz};
+    const float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
+    uint32_t stack[kOccMaxDepth + 2];
+    int sp = 0;
+    uint32_t node = 0;
+    for (uint32_t it = 0; it < n_nodes; ++it) {
+        const float4 n0 = __ldg(&nodes[4 * (size_t)node]), n1 = __ldg(&nodes[4 * (size_t)node + 1]);
+        const float4 n2 = __ldg(&nodes[4 * (size_t)node + 2]);
+        const uint4 n3 = __ldg(reinterpret_cast<const uint4 *>(nodes) + 4 * (size_t)node + 3);
+        bool hl = n3.x != kNone && occ_box(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv);
+        bool hr = n3.y != kNone && occ_box(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv);
+        if (hl && n3.z) {
+            for (uint32_t k = 0; k < n3.z; ++k)
+                if (occ_triangle(tris, n3.x + k, o, d)) return true;
+            hl = false;
+        }
+        if (hr && n3.w) {
+            for (uint32_t k = 0; k < n3.w; ++k)
+                if (occ_triangle(tris, n3.y + k, o, d)) return true;
+            hr = false;
+        }
+        if (hl && hr) {
+            if (sp < kOccMaxDepth + 2) stack[sp++] = n3.y;
+            node = n3.x;
+        } else if (hl) {
+            node = n3.x;
+        } else if (hr) {
+            node = n3.y;
+        } else {
+            if (sp == 0) return false;
+            node = stack[--sp];
+        }
+    }
+    return false;
+}
+
+// Whether the ray (o, d) hits an occluder (false without occluders).
+__device__ __forceinline__ bool occluded(const DevScene &S, const float o[3], const float d[3]) {
+    return S.occ_nodes && occluded_bvh(S.occ_nodes, S.occ_tris, S.occ_n_nodes, o[0], o[1], o[2], d[0], d[1], d[2]);
+}
+
 // A tracking visitor sees every collision decision that involved a density
 // lookup: the leaf's brick and box, the position, rho, the majorant and
 // whether the collision was real (rho / smax >= q).  The forward renderer's
@@ -891,6 +978,13 @@ __device__ __forceinline__ void drop_nonfinite(const DevParams &P, float4 &sun, 
 
 // ---- one camera path sample: SampleVolume recursion as a loop --------------
 // (src/kernel.cpp:128-445; see the CPU restatement for the derivation)
+// Alpha of a path sample = what its camera segment did: 0 when it escaped, 1
+// when it collided; a collision at or beyond the depth (cut) counts as 1, but
+// the USE_EMBREE build's depth mask (src/kernel.cpp:379) zeroes it.
+__device__ __forceinline__ float first_alpha(const DevParams &P, uint32_t res) {
+    return (res == kTrackCollided || (res == kTrackCut && !P.embree)) ? 1.0f : 0.0f;
+}
+
 __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
                                             uint32_t py, uint64_t seed, uint64_t sample, float4 &sun_acc,
                                             float4 &sky_acc, uint32_t *nstack, Count &cnt) {
@@ -905,10 +999,10 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
     for (uint32_t r = 0;; ++r) {
         float td;
         const uint32_t res = track(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
-        if (r == 0) sun_acc.w = sky_acc.w = res == kTrackEscaped ? 0.0f : 1.0f;
+        if (r == 0) sun_acc.w = sky_acc.w = first_alpha(P, res);
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
-            if (r > 0) {
+            if (r > 0 && !(P.embree && occluded(S, ro, rd))) {
                 if (sun_hit(P, rd)) {
                     sun_acc.x = sun_acc.x + T0 * P.sun_color[0];
                     sun_acc.y = sun_acc.y + T1 * P.sun_color[1];
@@ -939,7 +1033,8 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         float tds;
-        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped) {
+        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped &&
+            !(P.embree && occluded(S, rc, lrd))) {
             const bool hit = sun_hit(P, lrd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;
@@ -976,18 +1071,22 @@ __device__ __forceinline__ float4 shadow_sample(const DevScene &S, const DevPara
     float lrd[3];
     sun_sample(P, u3, u4, lrd);
     uint32_t res = kTrackEscaped;
+    bool occ = false;
     if (active) {
         const float ro1[3] = {ro[0] + rd[0] * depth, ro[1] + rd[1] * depth, ro[2] + rd[2] * depth};
         float td;
         res = track(S, P, ro1, lrd, g, 3.402823466e+38f, td, nstack, cnt);
+        // USE_EMBREE build: an escaped segment whose ray hits an occluder
+        // gathers nothing, alpha included (src/kernel.cpp:375-383)
+        occ = res == kTrackEscaped && P.embree && occluded(S, ro1, lrd);
     }
     const bool esc = res == kTrackEscaped;
-    const bool lit = P.scattevs > 0u && esc && sun_hit(P, lrd);
+    const bool lit = P.scattevs > 0u && esc && !occ && sun_hit(P, lrd);
     float4 o;
     o.x = __fdiv_rn(lit ? P.sun_color[0] : 0.0f, P.sun_color[0]);
     o.y = __fdiv_rn(lit ? P.sun_color[1] : 0.0f, P.sun_color[1]);
     o.z = __fdiv_rn(lit ? P.sun_color[2] : 0.0f, P.sun_color[2]);
-    o.w = __fdiv_rn((P.scattevs > 0u || !esc) ? 1.0f : 0.0f, 0.0f);
+    o.w = __fdiv_rn(((P.scattevs > 0u || !esc) && !occ) ? 1.0f : 0.0f, 0.0f);
     return o;
 }
 

@@ -202,6 +202,9 @@ int upload_scene(const HostScene &h, SceneBufs &b, bool use_grid, cudaStream_t s
     S.levels = use_grid ? h.levels : 0u;
     S.n = h.n;
     S.mdim = h.mdim;
+    S.occ_nodes = nullptr;
+    S.occ_tris = nullptr;
+    S.occ_n_nodes = 0;
     return DR_OK;
 }
 
@@ -245,7 +248,8 @@ int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned
     d.h = p->h;
     d.depthcomp = (p->flags & DR_KERNEL_DEPTHCOMP) ? 1u : 0u;
     d.finite_paths = (p->flags & DR_KERNEL_FINITE_PATHS) ? 1u : 0u;
-    if (p->flags & ~(DR_KERNEL_DEPTHCOMP | DR_KERNEL_FINITE_PATHS))
+    d.embree = (p->flags & DR_KERNEL_EMBREE) ? 1u : 0u;
+    if (p->flags & ~(DR_KERNEL_DEPTHCOMP | DR_KERNEL_FINITE_PATHS | DR_KERNEL_EMBREE))
         return need(false, DR_ERR_INVALID, "dr_set_params: unknown flags");
     {
         // RenderKernel::Shadow: zfar = (0,0,1,1) * projInv, clip_end = -zfar.z / zfar.w

@@ -97,6 +97,16 @@ int make_tile_args(uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t 
                    uint32_t tile, TileArgs &A);
 bool valid_tuning(const dr_tuning *t);
 
+// Occluder BVH as built on the host (layout of DevScene::occ_nodes/occ_tris,
+// 16 and 12 floats per node and triangle); source[j] = the selected triangle
+// (in surface order) stored at position j.
+struct OccBvh {
+    std::vector<float> nodes;
+    std::vector<float> tris;
+    std::vector<uint32_t> source;
+};
+int build_occluder_bvh(const dr_surface *s, uint32_t n, uint32_t mode, OccBvh &out);
+
 }  // namespace dr
 
 // The context behind the C ABI's opaque dr_ctx handle.
@@ -118,6 +128,8 @@ struct dr_ctx {
     dr::DevBuf<float> grad_copies;    // adjoint: spread copies of the brick-pool gradient
     dr::DevBuf<double> albedo_slots;  // adjoint: partial sums of the albedo gradient (kept zeroed)
     dr::DevBuf<uint4> path_rec;       // adjoint: one record per path of a chunk (totals pass -> scatter pass)
+    dr::DevBuf<float4> occ_nodes, occ_tris;  // occluder BVH (kept across scene uploads)
+    uint32_t occ_n_nodes = 0;
     uint32_t n_leaf_nodes = 0;
     bool use_grid = true;
     dr::Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};

@@ -41,7 +41,19 @@ struct DevScene {
     uint32_t levels;     // leaf depth below the root (0 = no grid; stack traversal only)
     uint32_t n;          // leaf cells per axis
     uint32_t mdim;       // macro cells per axis
+    // Occluder BVH (null: no occluders).  Node i = occ_nodes[4i .. 4i+3]: left
+    // box (min xyz, max x), (max yz, right min xy), (right min z, right max
+    // xyz), then (left ref, right ref, left count, right count) as uint32
+    // bits: count > 0 = leaf of `count` triangles from ref, count 0 = internal
+    // node ref, ref kNone = no child.  Triangle j = occ_tris[3j .. 3j+2]:
+    // v0, e1 = v1 - v0, e2 = v2 - v0 (w unused).
+    const float4 *occ_nodes;
+    const float4 *occ_tris;
+    uint32_t occ_n_nodes;
 };
+
+constexpr int kOccMaxDepth = 48;     // occluder BVH depth (the traversal stack holds one entry per level)
+constexpr float kOccFar = 1e6f;      // MAX_OCCLUSION_DIST, src/SceneOcclusion.h:4
 
 struct DevParams {
     float sigma_s, sigma_a, sigma_e, albedo;   // albedo = sigma_s / (sigma_a + sigma_s) in binary32
@@ -58,6 +70,7 @@ struct DevParams {
     const float *depth;       // w*h or null
     uint32_t depthcomp;       // KERNEL_DEPTHCOMP: camera rays stop at depth
     uint32_t finite_paths;    // a path whose contribution is not finite adds nothing
+    uint32_t embree;          // the reference's USE_EMBREE build: occluder and depth masks on gathered light
     float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
 };
 

@@ -352,14 +352,16 @@ __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
     return 0;
 }
 
-// Segment end: the body of path_sample() between two track() calls.
-template <bool WALK>
+// Segment end: the body of path_sample() between two track() calls.  OCC:
+// occluders are present and the USE_EMBREE build's masks apply (a separate
+// instantiation, so frames without occluders carry no traversal code).
+template <bool WALK, bool OCC>
 __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
                                         const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
                                         uint32_t &state, Trav *slow) {
     const float f = P.albedo;
     if (L.seg == kSegShadow) {
-        if (L.esc == kTrackEscaped) {
+        if (L.esc == kTrackEscaped && !(OCC && occluded(S, L.ro, L.rd))) {
             const bool hit = sun_hit(P, L.rd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;
@@ -377,9 +379,9 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
         begin_segment(L, S, cnt, state, slow);
         return;
     }
-    if (L.r == 0) L.sun.w = L.sky.w = L.esc == kTrackEscaped ? 0.0f : 1.0f;
+    if (L.r == 0) L.sun.w = L.sky.w = first_alpha(P, L.esc);
     if (L.esc == kTrackEscaped) {
-        if (L.r > 0) {
+        if (L.r > 0 && !(OCC && occluded(S, L.ro, L.rd))) {
             if (sun_hit(P, L.rd)) {
                 L.sun.x = L.sun.x + L.T[0] * P.sun_color[0];
                 L.sun.y = L.sun.y + L.T[1] * P.sun_color[1];
@@ -467,13 +469,13 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
 }
 
 // One loop iteration of a lane that holds a path (see render_persistent_kernel).
-template <bool WALK>
+template <bool WALK, bool OCC>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
                                           Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits,
                                           uint32_t steps, float (*tstack)[6]) {
     if (events) {
-        if (state == kEvent) path_event(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
+        if (state == kEvent) path_event<WALK, OCC>(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
     }
     if (state == kTrav) {
@@ -507,7 +509,7 @@ __device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
 // BATCH: the paths of many views (each with its own scene, parameters, tile
 // and output) share one work queue; a lane looks its view up when it fetches
 // a path and reads that view's records from global memory (L1-resident).
-template <int MINB, bool WALK, bool BATCH>
+template <int MINB, bool WALK, bool BATCH, bool OCC>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
                                                                             float4 *sky_out, DevCounters *C,
@@ -577,10 +579,11 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow, visits,
-                      steps, ts);
+            lane_work<WALK, OCC>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow,
+                                 visits, steps, ts);
         } else {
-            lane_work(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps, ts);
+            lane_work<WALK, OCC>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps,
+                                 ts);
         }
     }
     warp_sum_counts(cnt, C, paths);
@@ -624,6 +627,14 @@ __global__ void probe_leaf_kernel(DevScene S, const float *ro, const float *rd, 
         }
     }
     counts[r] = k;
+}
+
+__global__ void probe_occlusion_kernel(DevScene S, const float *ro, const float *rd, uint32_t n, uint32_t *hit) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float o[3] = {ro[3 * (size_t)i], ro[3 * (size_t)i + 1], ro[3 * (size_t)i + 2]};
+    const float d[3] = {rd[3 * (size_t)i], rd[3 * (size_t)i + 1], rd[3 * (size_t)i + 2]};
+    hit[i] = occluded(S, o, d) ? 1u : 0u;
 }
 
 __global__ void probe_density_kernel(DevScene S, const uint32_t *nodes, const float *pts, uint32_t n, float *out) {
@@ -817,13 +828,13 @@ __device__ __noinline__ uint32_t track_ratio(const DevScene S, float sigma_e, co
 
 struct PathTotals {
     float w;            // dsun . (sun contribution) + dsky . (sky contribution) of the whole path
-    uint64_t esc;       // bit r: the shadow segment after scattering event r escaped (r < kEscBits)
+    uint64_t esc;       // bit r: the shadow segment after scattering event r is lit (r < kEscBits)
     float3 asun, asky;  // sum over contributions of (scattering events before it) * contribution
     bool ok;            // every component of the path's contribution is finite
 };
 
 // What pass 1 keeps per path for pass 2 (16 bytes): the weight (NaN: path left
-// out) and the shadow-escape bits.
+// out) and the bits of its lit shadow segments (escaped, no occluder hit).
 struct __align__(16) PathRecord {
     float w;
     uint32_t esc_lo, esc_hi, pad;
@@ -871,7 +882,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         }
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
-            if (r > 0) {
+            if (r > 0 && !(P.embree && occluded(S, ro, rd))) {
                 const bool hit = sun_hit(P, rd);
                 const float3 cs = f3(T0 * (hit ? P.sun_color[0] : 0.0f), T1 * (hit ? P.sun_color[1] : 0.0f),
                                      T2 * (hit ? P.sun_color[2] : 0.0f));
@@ -902,17 +913,20 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
                              (T1 * ((p3.y / (p3.y + p2)) * f)) * (hit ? P.sun_color[1] : 0.0f),
                              (T2 * ((p3.z / (p3.z + p2)) * f)) * (hit ? P.sun_color[2] : 0.0f));
         float tds;
-        uint32_t sres;
+        bool lit;  // the shadow segment escaped and no occluder blocks its ray
         if constexpr (SCATTER) {
-            // segments 0..63: pass 1 recorded whether the shadow escapes, so it
-            // is tracked once with its weight (zero unless it escapes)
+            // segments 0..63: pass 1 recorded whether the shadow is lit, so it
+            // is tracked once with its weight (zero unless it is lit)
             const bool known = r < kEscBits;
             const Rng g0 = g;
             ScatterVisit sv{(known && ((tot.esc >> r) & 1ull)) ? dot3f(dsun, cn) : 0.0f, grad, S.bricks};
-            sres = track_scatter(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
-            if (!known && sres == kTrackEscaped) {
+            const uint32_t sres = track_scatter(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
+            if (known) {
+                lit = (tot.esc >> r) & 1ull;
+            } else {
+                lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
                 sv.w = dot3f(dsun, cn);
-                if (sv.w != 0.0f) {
+                if (lit && sv.w != 0.0f) {
                     Rng g1 = g0;  // the same draws again: ends in the state g already holds
                     float t2;
                     (void)track_scatter(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
@@ -921,13 +935,15 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         } else if constexpr (RATIO) {
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
-            sres = track_ratio(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
+            const uint32_t sres = track_ratio(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
+            lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
             cn = f3(cn.x * ws, cn.y * ws, cn.z * ws);
         } else {
-            sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
-            if (sres == kTrackEscaped && r < kEscBits) tot.esc |= 1ull << r;
+            const uint32_t sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
+            lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
+            if (lit && r < kEscBits) tot.esc |= 1ull << r;
         }
-        if (sres == kTrackEscaped) {
+        if (lit) {
             const float m = (float)(r + 1);
             acc_sun = f3(acc_sun.x + cn.x, acc_sun.y + cn.y, acc_sun.z + cn.z);
             a_sun = f3(a_sun.x + m * cn.x, a_sun.y + m * cn.y, a_sun.z + m * cn.z);
@@ -995,7 +1011,7 @@ __device__ __forceinline__ void tile_path(const TileArgs &A, uint64_t gi, uint32
 // tw x th float4, rgb used): rec[gi - p0] = the path's weight dsun . C_sun +
 // dsky . C_sky (NaN for a path left out: zero delta at its pixel, or a
 // contribution that is not finite, the sky term's 0/0 for rd.y == 0) and its
-// shadow-escape bits; the albedo term goes to the slots.
+// lit-shadow bits; the albedo term goes to the slots.
 __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S, DevParams P, TileArgs A,
                                                                       uint64_t p0, uint64_t n, const void *mie_pack,
                                                                       const float4 *dsun, const float4 *dsky,
@@ -1251,25 +1267,28 @@ cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const Tile
 
 // Variants of the persistent kernel compiled for 4, 5, 6 and 8 resident
 // blocks per SM (fewer registers, some spilled to L1-resident local memory),
-// each with the stack traversal or the cell walk, single frame or batch.
+// each with the stack traversal or the cell walk, single frame or batch, and
+// for single frames with or without occluders.
 using PersistentFn = void (*)(DevScene, DevParams, TileArgs, const void *, float4 *, float4 *, DevCounters *,
                               WorkQueue *, uint32_t, BatchArgs);
-template <bool BATCH>
+template <bool BATCH, bool OCC>
 static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
     if (traversal == 1u) {
-        if (minb >= 8) return render_persistent_kernel<8, true, BATCH>;
-        if (minb >= 6) return render_persistent_kernel<6, true, BATCH>;
-        if (minb >= 5) return render_persistent_kernel<5, true, BATCH>;
-        return render_persistent_kernel<4, true, BATCH>;
+        if (minb >= 8) return render_persistent_kernel<8, true, BATCH, OCC>;
+        if (minb >= 6) return render_persistent_kernel<6, true, BATCH, OCC>;
+        if (minb >= 5) return render_persistent_kernel<5, true, BATCH, OCC>;
+        return render_persistent_kernel<4, true, BATCH, OCC>;
     }
-    if (minb >= 8) return render_persistent_kernel<8, false, BATCH>;
-    if (minb >= 6) return render_persistent_kernel<6, false, BATCH>;
-    if (minb >= 5) return render_persistent_kernel<5, false, BATCH>;
-    return render_persistent_kernel<4, false, BATCH>;
+    if (minb >= 8) return render_persistent_kernel<8, false, BATCH, OCC>;
+    if (minb >= 6) return render_persistent_kernel<6, false, BATCH, OCC>;
+    if (minb >= 5) return render_persistent_kernel<5, false, BATCH, OCC>;
+    return render_persistent_kernel<4, false, BATCH, OCC>;
 }
 
-static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch) {
-    return batch ? persistent_variant_of<true>(minb, traversal) : persistent_variant_of<false>(minb, traversal);
+// Batches carry no occluders (their scenes come from dr_scene_desc records).
+static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch, bool occ = false) {
+    if (batch) return persistent_variant_of<true, false>(minb, traversal);
+    return occ ? persistent_variant_of<false, true>(minb, traversal) : persistent_variant_of<false, false>(minb, traversal);
 }
 
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
@@ -1282,13 +1301,13 @@ int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t sm
 
 // Grid of the persistent kernel: SMs x resident blocks (the tuned count, capped
 // by what fits).
-static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, bool batch, PersistentFn &fn,
-                                   int &blocks, uint32_t &event_batch) {
+static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, bool batch, bool occ,
+                                   PersistentFn &fn, int &blocks, uint32_t &event_batch) {
     int sms = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
     const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
-    fn = persistent_variant(variant, tune.traversal, batch);
+    fn = persistent_variant(variant, tune.traversal, batch, occ);
     int maxb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, kPersistentBlock, smem) != cudaSuccess || maxb < 1)
         maxb = 1;
@@ -1308,7 +1327,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, false, fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, false, S.occ_nodes && P.embree, fn, blocks, batch);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
@@ -1323,7 +1342,7 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, true, fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, true, false, fn, blocks, batch);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
@@ -1340,6 +1359,12 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
                               uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts, cudaStream_t st) {
     probe_leaf_kernel<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, n, maxn, nodes, tr0, tr1, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe_occlusion(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t *hit,
+                                   cudaStream_t st) {
+    probe_occlusion_kernel<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, n, hit);
     return cudaGetLastError();
 }
 

@@ -26,6 +26,8 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
                               uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts, cudaStream_t st);
+cudaError_t launch_probe_occlusion(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t *hit,
+                                   cudaStream_t st);
 cudaError_t launch_probe_density(const DevScene &S, const uint32_t *nodes, const float *pts, uint32_t n, float *out,
                                  cudaStream_t st);
 cudaError_t launch_probe_paths(const DevScene &S, const DevParams &P, const void *mie_pack, const uint32_t *px,

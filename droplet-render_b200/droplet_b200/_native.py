@@ -26,6 +26,7 @@ DR_PHASE_MIE_REFERENCE = 0
 DR_PHASE_MIE_EXACT = 1
 DR_KERNEL_DEPTHCOMP = 0x1
 DR_KERNEL_FINITE_PATHS = 0x2
+DR_KERNEL_EMBREE = 0x4
 
 DR_PROBE_MIE_EVAL_RGB = 0
 DR_PROBE_MIE_SAMPLE = 1
@@ -68,6 +69,11 @@ class DrSceneDesc(C.Structure):
         ("n_leaves", C.c_uint32),
         ("lvoxc", C.c_uint32),
     ]
+
+
+class DrSurface(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("n_vertices", C.c_uint32), ("indices", C.c_void_p),
+                ("n_triangles", C.c_uint32), ("flags", C.c_uint32)]
 
 
 class DrRenderParams(C.Structure):
@@ -130,6 +136,10 @@ SIGNATURES = {
     ),
     "dr_octree_free": (None, [C.POINTER(DrOctree)]),
     "dr_upload_scene": (C.c_int, [C.c_void_p, C.POINTER(DrSceneDesc)]),
+    "dr_set_occluders": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "dr_build_occluder_bvh": (
+        C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
+                  C.POINTER(C.c_uint32)]),
     "dr_set_params": (C.c_int, [C.c_void_p, C.POINTER(DrRenderParams)]),
     "dr_sky_cook": (
         C.c_int,
@@ -189,6 +199,7 @@ SIGNATURES = {
         [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     ),
     "dr_probe_density": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "dr_probe_occlusion": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "dr_probe_paths": (
         C.c_int,
         [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p],

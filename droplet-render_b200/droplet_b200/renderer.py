@@ -51,6 +51,7 @@ class RenderSettings:
     depth: np.ndarray | None = None   # depth texture: distance along each camera ray (shadow pass, compositing)
     depthcomp: bool = False           # KERNEL_DEPTHCOMP: camera rays stop at the depth texture
     finite_paths: bool = False        # a path sample with a non-finite sum adds nothing (DR_KERNEL_FINITE_PATHS)
+    embree: bool = False              # the reference's USE_EMBREE build: occluder and depth masks (DR_KERNEL_EMBREE)
     phase_mode: int = N.DR_PHASE_MIE_REFERENCE
     _keep: list = field(default_factory=list, repr=False)
 
@@ -79,11 +80,42 @@ class RenderSettings:
             p.depth = d.ctypes.data
         else:
             p.depth = None
-        p.flags = (N.DR_KERNEL_DEPTHCOMP if self.depthcomp else 0) | (N.DR_KERNEL_FINITE_PATHS if self.finite_paths else 0)
+        p.flags = ((N.DR_KERNEL_DEPTHCOMP if self.depthcomp else 0) | (N.DR_KERNEL_FINITE_PATHS if self.finite_paths else 0)
+                   | (N.DR_KERNEL_EMBREE if self.embree else 0))
         return p
 
 
 CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream as a stream handle
+
+
+SURFACE_HOLDOUT = 0x2       # SCENEOBJ_HOLDOUT
+OCCLUDE_ALL_SURFACES = 0    # the reference: every surface occludes
+OCCLUDE_HOLDOUT_ONLY = 1    # only holdout surfaces occlude
+
+
+def _surfaces(surfaces):
+    keep = []
+    arr = (N.DrSurface * max(len(surfaces), 1))()
+    for i, (v, ix, flags) in enumerate(surfaces):
+        v = np.ascontiguousarray(v, np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(ix, np.uint32).reshape(-1, 3)
+        keep += [v, ix]
+        arr[i] = N.DrSurface(v.ctypes.data, len(v), ix.ctypes.data, len(ix), int(flags))
+    return arr, keep
+
+
+def build_occluder_bvh(surfaces, mode: int = OCCLUDE_ALL_SURFACES):
+    """The occluder BVH the library builds: (nodes (n, 16) float32 with the
+    last four words uint32 bits, triangles (m, 12), source (m,))."""
+    arr, keep = _surfaces(surfaces)
+    nn, nt = C.c_uint32(0), C.c_uint32(0)
+    N.check(N.lib().dr_build_occluder_bvh(arr, len(keep) // 2, mode, None, C.byref(nn), None, None, C.byref(nt)))
+    nodes = np.zeros((nn.value, 16), np.float32)
+    tris = np.zeros((nt.value, 12), np.float32)
+    src = np.zeros(nt.value, np.uint32)
+    N.check(N.lib().dr_build_occluder_bvh(arr, len(keep) // 2, mode, nodes.ctypes.data, C.byref(nn),
+                                          tris.ctypes.data, src.ctypes.data, C.byref(nt)))
+    return nodes, tris, src
 
 
 def stream_handle(torch_stream) -> int:
@@ -126,6 +158,13 @@ class Renderer:
         bricks = np.ascontiguousarray(oc.bricks, np.float32)
         d = N.DrSceneDesc(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
         N.check(N.lib().dr_upload_scene(self._ctx, C.byref(d)))
+
+    def set_occluders(self, surfaces, mode: int = OCCLUDE_ALL_SURFACES):
+        """Occluder meshes (SceneOcclusion): surfaces = [(vertices (n, 3), indices
+        (m, 3), flags)], flags & SURFACE_HOLDOUT marks a holdout mesh; an empty
+        list removes them.  They act when the settings have embree=True."""
+        arr, keep = _surfaces(surfaces)
+        N.check(N.lib().dr_set_occluders(self._ctx, arr, len(keep) // 2, mode))
 
     def set_params(self, s: RenderSettings):
         p = s.to_c()
@@ -247,6 +286,14 @@ class Renderer:
         N.check(N.lib().dr_probe_leaf_sequence(self._ctx, ro.ctypes.data, rd.ctypes.data, n, maxn, nodes.ctypes.data,
                                                a.ctypes.data, b.ctypes.data, cnt.ctypes.data))
         return nodes, a, b, cnt
+
+    def probe_occlusion(self, ro, rd) -> np.ndarray:
+        """1 per ray that hits an occluder at t in [0, 1e6] (the GPU traversal)."""
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        hit = np.zeros(len(ro), np.uint32)
+        N.check(N.lib().dr_probe_occlusion(self._ctx, ro.ctypes.data, rd.ctypes.data, len(ro), hit.ctypes.data))
+        return hit
 
     def probe_density(self, leaf_nodes, points):
         leaf_nodes = np.ascontiguousarray(leaf_nodes, np.uint32)

@@ -89,6 +89,10 @@ typedef struct {
 #define DR_KERNEL_DEPTHCOMP 0x1u     /* camera rays stop at depth (src/kernel.h:4) */
 #define DR_KERNEL_FINITE_PATHS 0x2u  /* a path sample whose sun or sky sum is not finite adds nothing (the
                                         reference's sky term is 0/0 for rd.y == 0, src/kernel.cpp:338-342) */
+#define DR_KERNEL_EMBREE 0x4u        /* the reference built with USE_EMBREE (its occlusion option): light that a
+                                        segment gathers on escape is zeroed when the segment's ray hits an
+                                        occluder (src/kernel.cpp:149-153, 375-383), and a camera ray cut at its
+                                        depth gets alpha 0 instead of 1 (the same block's depth mask) */
 
 /* In-kernel counters accumulated over all launches since the last reset. */
 typedef struct {
@@ -125,6 +129,35 @@ void dr_octree_free(dr_octree *oct);
 /* Copies nodes and bricks to the device (the reference reads Scene::ob/pvol
  * in place, src/kernel.cpp:225-305). */
 int dr_upload_scene(dr_ctx *ctx, const dr_scene_desc *scene);
+
+/* ---- occlusion geometry: SceneOcclusion (src/SceneOcclusion.cpp:19-91) -------
+ * Triangle meshes (SceneData::Surface: world-space vertices vl, triangle index
+ * list tl, object flags) replace the Embree scene.  With DR_KERNEL_EMBREE set in
+ * the parameters, a segment whose ray (origin, direction; t in [0, 1e6]) hits
+ * any occluder triangle gathers no sun or sky light when it escapes.  Replaces
+ * rtcIntersect4 with a BVH built here and an any-hit traversal on the GPU. */
+typedef struct {
+    const float *vertices;     /* 3 * n_vertices floats */
+    uint32_t n_vertices;
+    const uint32_t *indices;   /* 3 * n_triangles vertex indices */
+    uint32_t n_triangles;
+    uint32_t flags;            /* DR_SURFACE_HOLDOUT (SCENEOBJ_HOLDOUT, src/scene.h:54) */
+} dr_surface;
+#define DR_SURFACE_HOLDOUT 0x2u
+#define DR_OCCLUDE_ALL_SURFACES 0u  /* the reference: `!flags & SCENEOBJ_HOLDOUT` (src/SceneOcclusion.cpp:27) is
+                                       always 0, so every surface occludes */
+#define DR_OCCLUDE_HOLDOUT_ONLY 1u  /* the evident intent: only surfaces flagged DR_SURFACE_HOLDOUT occlude */
+/* Builds the occluder BVH on the host and uploads it; n_surfaces == 0 (or no
+ * triangle selected) removes the occluders.  Kept across dr_upload_scene. */
+int dr_set_occluders(dr_ctx *ctx, const dr_surface *surfaces, uint32_t n_surfaces, uint32_t mode);
+/* The BVH dr_set_occluders would build, for inspection (host buffers, NULL to
+ * query sizes): nodes = 16 floats each (left box min xyz, max xyz, right box
+ * min xyz, max xyz, then left ref, right ref, left count, right count as
+ * uint32 bits; count 0 = internal node ref, else first triangle ref),
+ * triangles = 12 floats each (v0 xyz, 0, e1 = v1 - v0 xyz, 0, e2 = v2 - v0
+ * xyz, 0) in leaf order, source = the selected triangle each came from. */
+int dr_build_occluder_bvh(const dr_surface *surfaces, uint32_t n_surfaces, uint32_t mode, float *nodes,
+                          uint32_t *n_nodes, float *triangles, uint32_t *source, uint32_t *n_triangles);
 
 /* ---- render settings: RenderKernel::Initialize (src/kernel.cpp:497-534) ---- */
 int dr_set_params(dr_ctx *ctx, const dr_render_params *params);
@@ -268,6 +301,9 @@ int dr_probe_leaf_sequence(dr_ctx *ctx, const float *ro, const float *rd, uint32
                            uint32_t *nodes, float *tr0, float *tr1, uint32_t *counts);
 /* SampleVoxelSpace at n points inside leaf nodes[i] (src/kernel.cpp:96-126). */
 int dr_probe_density(dr_ctx *ctx, const uint32_t *nodes, const float *points, uint32_t n, float *out);
+/* Occluder any-hit of n rays (ro, rd: 3n floats): hit[i] = 1 when the ray hits
+ * an occluder triangle at t in [0, 1e6]. */
+int dr_probe_occlusion(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n, uint32_t *hit);
 /* Per-path sample (sun rgba, sky rgba) for n (px, py, sample) triples. */
 int dr_probe_paths(dr_ctx *ctx, const uint32_t *px, const uint32_t *py, const uint64_t *sample, uint32_t n,
                    uint64_t seed, float *out_sun, float *out_sky);

@@ -34,12 +34,13 @@ class OrcParams(C.Structure):
         ("viewi", C.c_float * 16), ("proji", C.c_float * 16), ("w", C.c_uint32), ("h", C.c_uint32),
         ("depth", C.c_float), ("depth_map", C.c_void_p), ("depthcomp", C.c_uint32),
         ("phase_mode", C.c_uint32), ("mie_exact", C.c_void_p), ("finite_paths", C.c_uint32),
+        ("embree", C.c_uint32),
     ]
 
 
 class OrcScene(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("n_nodes", C.c_uint32), ("bricks", C.c_void_p), ("n_leaves", C.c_uint32),
-                ("lvoxc", C.c_uint32)]
+                ("lvoxc", C.c_uint32), ("occ_tris", C.c_void_p), ("occ_n", C.c_uint32)]
 
 
 class OrcCounters(C.Structure):
@@ -86,6 +87,12 @@ class Port:
         L.orc_adjoint_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                           C.c_uint64, C.c_uint64, vp, vp, vp, vp, C.c_int]
         L.orc_adjoint_tile_mt.restype = C.c_int
+        L.orc_occluded.argtypes = [C.POINTER(OrcScene), vp, vp]
+        L.orc_occluded.restype = C.c_int
+        L.orc_shadow_ray.argtypes = [C.POINTER(OrcParams), u32, u32, C.c_uint64, C.c_uint64, vp, vp]
+        L.orc_shadow_ray.restype = C.c_int
+        L.orc_occluded_fp64.argtypes = [C.POINTER(OrcScene), vp, vp, C.POINTER(C.c_double)]
+        L.orc_occluded_fp64.restype = C.c_int
         L.orc_reweighted_loss.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                           C.c_uint64, C.c_uint64, vp, vp, vp]
         L.orc_reweighted_loss.restype = C.c_double
@@ -119,8 +126,66 @@ class Port:
         return nodes, bricks.reshape(nl.value, lv.value ** 3), int(ml.value)
 
     @staticmethod
-    def scene(nodes: np.ndarray, bricks: np.ndarray) -> OrcScene:
-        return OrcScene(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+    def scene(nodes: np.ndarray, bricks: np.ndarray, occ: np.ndarray = None) -> OrcScene:
+        """occ: occluder triangles from occluder_triangles() (kept alive by the caller)."""
+        S = OrcScene(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+        if occ is not None and len(occ):
+            assert occ.dtype == np.float32 and occ.flags.c_contiguous and occ.shape[1] == 12
+            S.occ_tris, S.occ_n = occ.ctypes.data, len(occ)
+        return S
+
+    @staticmethod
+    def occluder_triangles(surfaces, mode: int = 0) -> np.ndarray:
+        """Occluder triangles of SceneOcclusion::Initialize (src/SceneOcclusion.cpp:19-56)
+        in surface order, 12 floats each (v0, e1 = v1 - v0, e2 = v2 - v0; w 0).
+        surfaces: (vertices (n, 3), indices (m, 3), flags); mode 0 = every
+        surface (the reference's `!flags & SCENEOBJ_HOLDOUT` is always 0),
+        1 = only surfaces with flags & 2 (SCENEOBJ_HOLDOUT)."""
+        out = []
+        for v, ix, flags in surfaces:
+            if mode == 1 and not (flags & 2):
+                continue
+            v = np.asarray(v, np.float32).reshape(-1, 3)
+            ix = np.asarray(ix, np.int64).reshape(-1, 3)
+            t = np.zeros((len(ix), 12), np.float32)
+            v0, v1, v2 = v[ix[:, 0]], v[ix[:, 1]], v[ix[:, 2]]
+            t[:, 0:3], t[:, 4:7], t[:, 8:11] = v0, v1 - v0, v2 - v0
+            out.append(t)
+        return np.ascontiguousarray(np.concatenate(out) if out else np.zeros((0, 12), np.float32))
+
+    def occluded(self, S, ro, rd) -> np.ndarray:
+        """Binary32 any-hit answer per ray (the GPU's triangle test, every triangle)."""
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        return np.array([self.L.orc_occluded(C.byref(S), _p(ro[i]), _p(rd[i])) for i in range(len(ro))], np.uint32)
+
+    def shadow_rays(self, P, x0, y0, tw, th, spp, seed, sample_base=0):
+        """(origins, directions, active) of the shadow pass's segments over a tile,
+        in (row, column, sample) order."""
+        n = th * tw * spp
+        ro = np.zeros((n, 3), np.float32)
+        rd = np.zeros((n, 3), np.float32)
+        act = np.zeros(n, bool)
+        k = 0
+        for j in range(th):
+            for i in range(tw):
+                for s in range(spp):
+                    act[k] = self.L.orc_shadow_ray(C.byref(P), x0 + i, y0 + j, seed, sample_base + s, _p(ro[k]),
+                                                   _p(rd[k]))
+                    k += 1
+        return ro, rd, act
+
+    def occluded_fp64(self, S, ro, rd):
+        """(hit, edge margin) per ray of the FP64 test."""
+        ro = np.ascontiguousarray(ro, np.float64).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float64).reshape(-1, 3)
+        hit = np.zeros(len(ro), np.uint32)
+        marg = np.zeros(len(ro))
+        m = C.c_double()
+        for i in range(len(ro)):
+            hit[i] = self.L.orc_occluded_fp64(C.byref(S), _p(ro[i]), _p(rd[i]), C.byref(m))
+            marg[i] = m.value
+        return hit, marg
 
     def leaf_sequence(self, nodes, ro, rd, maxn=4096):
         ro = np.ascontiguousarray(ro, np.float32)
@@ -171,6 +236,7 @@ class Port:
             P.depth_map = dm.ctypes.data
             P.depthcomp = 1 if cfg.get("depthcomp") else 0
         P.finite_paths = 1 if cfg.get("finite_paths") else 0
+        P.embree = 1 if cfg.get("embree") else 0
         if cfg.get("phase_mode", 0) == 1:
             tab = Port().mie_exact_table(pdf)
             keep.append(tab)

@@ -36,6 +36,10 @@ typedef struct {
     const float *bricks;   /* FOG bricks, lvoxc^3 floats each, z-major then y then x */
     uint32_t n_leaves;
     uint32_t lvoxc;
+    /* occluder triangles (SceneOcclusion's Embree scene, src/SceneOcclusion.cpp:19-56),
+     * 12 floats each: v0 xyz, 0, e1 = v1 - v0 xyz, 0, e2 = v2 - v0 xyz, 0; tested one by one */
+    const float *occ_tris;
+    uint32_t occ_n;
 } orc_scene;
 
 typedef struct {
@@ -60,6 +64,7 @@ typedef struct {
     uint32_t phase_mode;   /* 0 = the reference's sampler, 1 = exact inverse CDF */
     const float *mie_exact;/* exact-mode table (orc_mie_exact_table), 8 n + 4 floats */
     uint32_t finite_paths; /* a path whose sun or sky sum is not finite adds nothing */
+    uint32_t embree;       /* the reference built with USE_EMBREE (src/kernel.cpp:149-153, 375-383) */
 } orc_params;
 
 typedef struct {
@@ -139,6 +144,17 @@ void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
 int orc_adjoint_tile_mt(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
                         uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,
                         double *grad, double *galb, int nthreads);
+/* Occlusion query of SceneOcclusion::Intersect (t in [0, 1e6], any triangle):
+ * binary32 Moller-Trumbore, the GPU's arithmetic, over every triangle. */
+int orc_occluded(const orc_scene *S, const float o[3], const float d[3]);
+/* Origin and direction of the shadow pass's segment for one (pixel, sample);
+ * returns 1 when the pixel traces one (geometry before the far plane). */
+int orc_shadow_ray(const orc_params *P, uint32_t px, uint32_t py, uint64_t seed, uint64_t sample, float ro1[3],
+                   float lrd[3]);
+/* The same test in FP64 with the division by the determinant; *margin receives
+ * the smallest of u, v, 1 - u - v of the nearest hit candidate (how far the
+ * answer is from an edge), for pinning the binary32 test. */
+int orc_occluded_fp64(const orc_scene *S, const double o[3], const double d[3], double *margin);
 /* Linearised loss of the reweighted replay (decisions from S->bricks, ratios under pert). */
 double orc_reweighted_loss(const orc_scene *S, const orc_params *P, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th,
                            uint32_t spp, uint64_t seed, uint64_t sample_base, const float *dsun, const float *dsky,

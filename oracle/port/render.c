@@ -114,6 +114,84 @@ static int track_depth_v(const orc_scene *S, const orc_params *P, const float ro
     return 1;
 }
 
+/* ---- occluders: SceneOcclusion::Intersect (src/SceneOcclusion.cpp:58-91) ----
+ * Embree's query (tnear 0, tfar MAX_OCCLUSION_DIST = 1e6) answers whether the
+ * ray hits any occluder triangle.  Restated as Moller-Trumbore (1997) without
+ * culling, the division by the determinant folded into the comparisons. */
+static int occ_triangle(const float *T, const float o[3], const float d[3]) {
+    const float *a = T, *e1 = T + 4, *e2 = T + 8;
+    const float px = d[1] * e2[2] - d[2] * e2[1], py = d[2] * e2[0] - d[0] * e2[2], pz = d[0] * e2[1] - d[1] * e2[0];
+    const float det = e1[0] * px + e1[1] * py + e1[2] * pz;
+    const float sx = o[0] - a[0], sy = o[1] - a[1], sz = o[2] - a[2];
+    const float u = sx * px + sy * py + sz * pz;
+    const float qx = sy * e1[2] - sz * e1[1], qy = sz * e1[0] - sx * e1[2], qz = sx * e1[1] - sy * e1[0];
+    const float v = d[0] * qx + d[1] * qy + d[2] * qz;
+    const float t = e2[0] * qx + e2[1] * qy + e2[2] * qz;
+    const float uv = u + v;
+    if (det > 0.0f) return u >= 0.0f && v >= 0.0f && uv <= det && t >= 0.0f && t <= det * 1e6f;
+    if (det < 0.0f) return u <= 0.0f && v <= 0.0f && uv >= det && t <= 0.0f && t >= det * 1e6f;
+    return 0;
+}
+
+int orc_occluded(const orc_scene *S, const float o[3], const float d[3]) {
+    for (uint32_t i = 0; i < S->occ_n; ++i)
+        if (occ_triangle(S->occ_tris + 12 * (size_t)i, o, d)) return 1;
+    return 0;
+}
+
+int orc_occluded_fp64(const orc_scene *S, const double o[3], const double d[3], double *margin) {
+    int hit = 0;
+    double best = 1e300;
+    for (uint32_t i = 0; i < S->occ_n; ++i) {
+        const float *T = S->occ_tris + 12 * (size_t)i;
+        double a[3], e1[3], e2[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = T[k];
+            e1[k] = T[4 + k]; /* the triangle (v0, v0 + e1, v0 + e2) the binary32 test sees, exactly */
+            e2[k] = T[8 + k];
+        }
+        const double p[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
+        const double det = e1[0] * p[0] + e1[1] * p[1] + e1[2] * p[2];
+        if (det == 0.0) continue;
+        const double s[3] = {o[0] - a[0], o[1] - a[1], o[2] - a[2]};
+        const double u = (s[0] * p[0] + s[1] * p[1] + s[2] * p[2]) / det;
+        const double q[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
+        const double v = (d[0] * q[0] + d[1] * q[1] + d[2] * q[2]) / det;
+        const double t = (e2[0] * q[0] + e2[1] * q[1] + e2[2] * q[2]) / det;
+        if (t < -1e-9 || t > 1e6) continue;
+        double m = u < v ? u : v;
+        if (1.0 - u - v < m) m = 1.0 - u - v;
+        const double am = m < 0 ? -m : m;
+        if (am < best) best = am;
+        if (m >= 0.0 && t >= 0.0) hit = 1;
+    }
+    if (margin) *margin = best;
+    return hit;
+}
+
+/* The shadow pass's segment of one (pixel, sample): origin on the camera ray at
+ * the pixel's depth and the sun-cone direction (orc_shadow_path's first steps);
+ * returns whether the pixel has geometry before the far plane. */
+int orc_shadow_ray(const orc_params *P, uint32_t px, uint32_t py, uint64_t seed, uint64_t sample, float ro1[3],
+                   float lrd[3]) {
+    float ro[3], rd[3];
+    int inf;
+    orc_camera_ray(P, px, py, ro, rd, &inf);
+    const float zz = P->proji[8 + 2] + P->proji[12 + 2], zw = P->proji[8 + 3] + P->proji[12 + 3];
+    const float clip_end = -zz / zw;
+    const float depth = P->depth_map ? P->depth_map[(size_t)py * P->w + px] : FLT_MAX;
+    orc_rng g;
+    orc_rng_seed(&g, seed, (uint64_t)py * P->w + px, sample);
+    const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
+    orc_sun_sample(P, u3, u4, lrd);
+    for (int k = 0; k < 3; ++k) ro1[k] = ro[k] + rd[k] * depth;
+    return inf && depth < clip_end;
+}
+
+static inline int occ_blocks(const orc_scene *S, const orc_params *P, const float o[3], const float d[3]) {
+    return P->embree && S->occ_n && orc_occluded(S, o, d);
+}
+
 int orc_track(const orc_scene *S, const orc_params *P, const float ro[3], const float rd[3], void *rng, float *td,
               orc_counters *cnt) {
     return track_depth(S, P, ro, rd, (orc_rng *)rng, FLT_MAX, td, cnt) != 0;
@@ -136,10 +214,13 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
     for (;;) {
         float td;
         int esc = track_depth(S, P, ro, rd, &g, r == 0 ? depth0 : FLT_MAX, &td, cnt);
-        if (r == 0) out_sun[3] = out_sky[3] = esc == 1 ? 0.0f : 1.0f;
+        /* alpha: the camera segment collided (1) or escaped (0); a collision at
+         * or beyond the depth counts as 1, except in the USE_EMBREE build whose
+         * depth mask zeroes it (src/kernel.cpp:379) */
+        if (r == 0) out_sun[3] = out_sky[3] = (esc == 0 || (esc == 2 && !P->embree)) ? 1.0f : 0.0f;
         if (esc == 2) break;
         if (esc) {
-            if (r > 0) {
+            if (r > 0 && !occ_blocks(S, P, ro, rd)) {
                 float sun[3], sky[3];
                 orc_sun_eval(P, rd, sun);
                 orc_sky_eval(P, rd, sky);
@@ -164,7 +245,7 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
         if (cnt) cnt->mie_evals += 3;
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         float tds;
-        if (track_depth(S, P, rc, lrd, &g, FLT_MAX, &tds, cnt)) {
+        if (track_depth(S, P, rc, lrd, &g, FLT_MAX, &tds, cnt) && !occ_blocks(S, P, rc, lrd)) {
             float sun[3];
             orc_sun_eval(P, lrd, sun);
             for (int k = 0; k < 3; ++k) out_sun[k] = out_sun[k] + (T[k] * ((p3[k] / (p3[k] + p2)) * f)) * sun[k];
@@ -212,16 +293,19 @@ void orc_shadow_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
     const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
     float lrd[3];
     orc_sun_sample(P, u3, u4, lrd);
-    int esc = 1;
+    int esc = 1, occ = 0;
     if (active) {
         float ro1[3], td;
         for (int k = 0; k < 3; ++k) ro1[k] = ro[k] + rd[k] * depth;
         esc = track_depth(S, P, ro1, lrd, &g, FLT_MAX, &td, cnt);
+        /* USE_EMBREE build: an escaped segment whose ray hits an occluder
+         * gathers nothing, alpha included (src/kernel.cpp:375-383) */
+        occ = esc == 1 && occ_blocks(S, P, ro1, lrd);
     }
     float lc[3] = {0.0f, 0.0f, 0.0f};
-    if (P->scattevs > 0 && esc) orc_sun_eval(P, lrd, lc);
+    if (P->scattevs > 0 && esc && !occ) orc_sun_eval(P, lrd, lc);
     const float color_w = 0.0f;
-    const float a = (P->scattevs > 0 || !esc) ? 1.0f : 0.0f;
+    const float a = ((P->scattevs > 0 || !esc) && !occ) ? 1.0f : 0.0f;
     for (int k = 0; k < 3; ++k) out[k] = lc[k] / P->sun_color[k];
     out[3] = a / color_w;
 }
@@ -450,7 +534,7 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
         }
         if (res == 2) break;
         if (res == 1) {
-            if (r > 0) {
+            if (r > 0 && !occ_blocks(S, P, ro, rd)) {
                 float sun[3], sky[3];
                 orc_sun_eval(P, rd, sun);
                 orc_sky_eval(P, rd, sky);
@@ -480,7 +564,8 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
         const orc_rng g0 = g;
         float tds;
         ratio_ctx rs = {1.0f, pert, S->bricks, S->lvoxc};
-        if (track_depth_v(S, P, rc, lrd, &g, FLT_MAX, &tds, 0, ratio ? ratio_visit : 0, ratio ? &rs : 0) == 1) {
+        if (track_depth_v(S, P, rc, lrd, &g, FLT_MAX, &tds, 0, ratio ? ratio_visit : 0, ratio ? &rs : 0) == 1 &&
+            !occ_blocks(S, P, rc, lrd)) {
             float sun[3], cn[3];
             orc_sun_eval(P, lrd, sun);
             for (int k = 0; k < 3; ++k) cn[k] = (T[k] * ((p3[k] / (p3[k] + p2)) * f)) * sun[k];

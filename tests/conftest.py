@@ -80,6 +80,7 @@ def settings_from_cfg(cfg: dict):
         phase=PhaseTable(cfg["mie_pdf"], cfg["mie_cdf"]), viewi=cfg["viewi"], proji=cfg["proji"], w=cfg["w"],
         h=cfg["h"], depth=cfg.get("depth"), depthcomp=bool(cfg.get("depthcomp", False)),
         finite_paths=bool(cfg.get("finite_paths", False)),
+        embree=bool(cfg.get("embree", False)),
         phase_mode=int(cfg.get("phase_mode", 0)))
 
 
@@ -157,3 +158,30 @@ def orbit_cfg(w: int, h: int, azimuth: float) -> dict:
     eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], azimuth, W.CAMERA["elevation"])
     cfg["viewi"], cfg["proji"] = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], w, h)
     return cfg
+
+
+def occluder_surfaces():
+    """Occluder meshes around the config-0 cloud, as (vertices, indices, flags):
+    a holdout UV sphere (radius 0.25) between the cloud and the sun, a ground
+    quad (z = 0.02, not flagged holdout) under it, and 200 small holdout
+    triangles beside it (seeded)."""
+    sd = cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"]).astype(np.float64)
+    c = np.asarray(W.CENTER) + 0.9 * sd
+    nu, nv = 24, 12
+    th = np.linspace(0.0, np.pi, nv + 1)
+    ph = np.linspace(0.0, 2 * np.pi, nu, endpoint=False)
+    verts = [c + 0.25 * np.array([np.sin(t) * np.cos(p), np.sin(t) * np.sin(p), np.cos(t)]) for t in th for p in ph]
+    tris = []
+    for i in range(nv):
+        for j in range(nu):
+            a, b = i * nu + j, i * nu + (j + 1) % nu
+            d, e = (i + 1) * nu + j, (i + 1) * nu + (j + 1) % nu
+            tris += [(a, d, b), (b, d, e)]
+    sphere = (np.asarray(verts, np.float32), np.asarray(tris, np.uint32), 0x2)
+    ground = (np.array([[-20, -20, 0.02], [20, -20, 0.02], [20, 20, 0.02], [-20, 20, 0.02]], np.float32),
+              np.array([[0, 1, 2], [0, 2, 3]], np.uint32), 0x0)
+    rng = np.random.default_rng(31)
+    base = rng.uniform([1.1, 0.0, 0.0], [1.6, 1.0, 1.0], (200, 3))
+    v = (base[:, None, :] + rng.normal(scale=0.05, size=(200, 3, 3))).reshape(-1, 3).astype(np.float32)
+    small = (v, np.arange(600, dtype=np.uint32).reshape(-1, 3), 0x2)
+    return [sphere, ground, small]
