@@ -32,7 +32,13 @@ Inputs the reference takes from places outside the rendering path:
     reference): SetSkyDataset(path) or DROPLET_HOSEK_DATASET (the model's C
     header), or SetSkyState(configs, radiances).  Turbidity and ground albedo
     are read from world.droplet.turbidity / ground_albedo when present, else
-    the reference's fixed 7 and 0.15 (src/kernel.cpp:525).
+    the reference's fixed 7 and 0.15 (src/kernel.cpp:525);
+  * occlusion geometry: with world.droplet.occlusion set, the reference (built
+    with Embree) occludes with the triangle meshes its node trees produce
+    (SceneData::Surface, src/main.cpp:406-419, src/SceneOcclusion.cpp:19-56).
+    Here they come from `scene.droplet_surfaces`, a list of
+    {"vertices": (n, 3), "indices": (m, 3), "holdout": bool}; every surface
+    occludes, as in the reference, unless SetOccluderMode(holdout_only=True).
 """
 from __future__ import annotations
 
@@ -63,6 +69,7 @@ _tile_size = (0, 0)
 _phase = None
 _sky_dataset = None
 _sky_state = None
+_holdout_only = False     # occluders: every surface (the reference) or holdout meshes only
 _device = int(os.environ.get("DROPLET_DEVICE", "0"))
 
 
@@ -88,6 +95,14 @@ def SetSkyState(configs, radiances):
     from droplet_b200.sky import SkyState
 
     _sky_state = SkyState(np.asarray(configs, np.float64).reshape(3, 9), np.asarray(radiances, np.float64).reshape(3))
+
+
+def SetOccluderMode(holdout_only: bool):
+    """False (default): every surface occludes, as the reference's
+    `!flags & SCENEOBJ_HOLDOUT` test makes it (src/SceneOcclusion.cpp:27);
+    True: only surfaces marked holdout, the option's documented intent."""
+    global _holdout_only
+    _holdout_only = bool(holdout_only)
 
 
 def LastError():
@@ -150,7 +165,15 @@ def _parse(scene, data, tilex, tiley, w, h):
     if getattr(scene, "droplet_depth", None) is not None:
         depth = np.ascontiguousarray(scene.droplet_depth, np.float32).reshape(h, w)
     depthcomp = bool(getattr(world, "depthcomp", False))
+    occlusion = bool(getattr(world, "occlusion", False))
+    surfaces = []
+    if occlusion:
+        for srf in getattr(scene, "droplet_surfaces", None) or []:
+            surfaces.append((np.ascontiguousarray(srf["vertices"], np.float32).reshape(-1, 3),
+                             np.ascontiguousarray(srf["indices"], np.uint32).reshape(-1, 3),
+                             0x2 if srf.get("holdout") else 0x0))
     return {
+        "occlusion": occlusion, "surfaces": surfaces,
         "viewi": viewi, "proji": proji, "w": int(w), "h": int(h), "tilex": int(tilex), "tiley": int(tiley),
         "sun": suns[0], "scattevs": int(sam.scatterevs), "sigma_s": float(sam.msigmas), "sigma_a": float(sam.msigmaa),
         "maxdepth": int(grid.maxdepth), "volume": vol, "depth": depth, "depthcomp": depthcomp,
@@ -199,8 +222,10 @@ def _build(job):
         st = RenderSettings(sigma_s=job["sigma_s"], sigma_a=job["sigma_a"], scattevs=job["scattevs"], sun_dir=sd,
                             sun_color=sc, sun_angle=sa, sky=_sky(sd, job["turbidity"], job["ground_albedo"]),
                             phase=PhaseTable(pdf, cdf), viewi=job["viewi"], proji=job["proji"], w=job["w"],
-                            h=job["h"], depth=job["depth"], depthcomp=job["depthcomp"])
+                            h=job["h"], depth=job["depth"], depthcomp=job["depthcomp"], embree=job["occlusion"])
         r = Renderer(_device)
+        if job["occlusion"]:
+            r.set_occluders(job["surfaces"], 1 if _holdout_only else 0)
         r.upload(oc)
         r.set_params(st)
         with _lock:

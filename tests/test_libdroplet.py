@@ -176,3 +176,52 @@ def test_addon_shadow_pass(lib):
         ref, _ = r.render_shadow_tile(8, 8, 32, 32, 100)
     assert np.array_equal(got[:, :3], ref.reshape(-1, 4)[:, :3])
     assert (got[:, :3] < 100).any() and np.isposinf(got[:, 3]).all()
+
+
+def test_begin_render_reads_occluders_with_the_occlusion_option(lib):
+    from conftest import occluder_surfaces
+
+    scene = fake_scene()
+    scene.droplet_surfaces = [{"vertices": v, "indices": ix, "holdout": bool(f & 2)} for v, ix, f in occluder_surfaces()]
+    lib.BeginRender(scene, NS(), 32, 32, 64, 64, 1)
+    assert lib._job["occlusion"] is False and lib._job["surfaces"] == []
+    wait_ready(lib)
+    lib.EndRender()
+    scene.world.droplet.occlusion = True
+    lib.BeginRender(scene, NS(), 32, 32, 64, 64, 1)
+    job = lib._job
+    assert job["occlusion"] is True
+    assert [len(ix) for _, ix, _ in job["surfaces"]] == [len(ix) for _, ix, _ in occluder_surfaces()]
+    assert [f for _, _, f in job["surfaces"]] == [f for _, _, f in occluder_surfaces()]
+    wait_ready(lib)
+
+
+@pytest.mark.gpu
+def test_addon_flow_with_occluders_matches_renderer(lib):
+    """With world.droplet.occlusion the module renders what the renderer renders
+    with the same occluders and the USE_EMBREE build's masks."""
+    from conftest import golden_octree, occluder_surfaces, settings_from_cfg
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree
+
+    scene = fake_scene()
+    scene.world.droplet.occlusion = True
+    scene.droplet_surfaces = [{"vertices": v, "indices": ix, "holdout": bool(f & 2)} for v, ix, f in occluder_surfaces()]
+    lib.BeginRender(scene, NS(), 32, 32, 64, 64, 1)
+    wait_ready(lib)
+    lib.Render(16, 16, 32, 32, 16)
+    wait_ready(lib)
+    assert lib.LastError() is None
+    sun = np.asarray(lib.QueryResult(0), np.float64).reshape(32, 32, 4)
+    nodes, bricks, mlevel = golden_octree()
+    cfg = c0_cfg(64, 64)
+    cfg["embree"] = True
+    with Renderer(0) as r:
+        r.set_occluders(occluder_surfaces())
+        r.upload(Octree(nodes, bricks, mlevel))
+        r.set_params(settings_from_cfg(cfg))
+        ref, _ = r.render_tile(16, 16, 32, 32, 16)
+        r.set_occluders([])
+        plain, _ = r.render_tile(16, 16, 32, 32, 16, sample_base=0)
+    assert np.allclose(sun, ref, rtol=1e-3, atol=1e-5 * np.abs(ref).max())
+    assert sun[..., :3].sum() < 0.97 * plain[..., :3].sum()
