@@ -96,6 +96,7 @@ int dr_destroy(dr_ctx *c) {
         c->albedo_slots.release();
         c->path_rec.release();
         c->occ_nodes.release();
+        c->env.release();
         c->occ_tris.release();
         c->band_work.release();
         for (int k = 0; k < 2; ++k)
@@ -198,6 +199,13 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
         DR_CUDA(cudaMemcpy(c->depth.p, p->depth, sizeof(float) * p->w * p->h, cudaMemcpyHostToDevice),
                 "dr_set_params: copy depth");
         d.depth = c->depth.p;
+    }
+    if (p->env_mode == DR_ENV_MAP) {
+        const size_t n = (size_t)p->env_w * p->env_h * 4;
+        DR_CUDA(c->env.reserve(n), "dr_set_params: alloc environment map");
+        DR_CUDA(cudaMemcpy(c->env.p, p->env_map, sizeof(float) * n, cudaMemcpyHostToDevice),
+                "dr_set_params: copy environment map");
+        d.env_map = c->env.p;
     }
     c->params = d;
     c->has_params = true;
@@ -530,16 +538,19 @@ int dr_probe_paths(dr_ctx *c, const uint32_t *px, const uint32_t *py, const uint
 }
 
 int dr_probe_sampler(dr_ctx *c, uint32_t what, const float *in, uint32_t n, float *out) {
-    if (!c || !in || !out || n == 0 || what > DR_PROBE_MIE_EXACT_DIR)
+    if (!c || !in || !out || n == 0 || what > DR_PROBE_ENV_MAP)
         return need(false, DR_ERR_INVALID, "dr_probe_sampler: bad argument");
     if (!c->has_params) return need(false, DR_ERR_STATE, "dr_probe_sampler: no parameters");
     if (what == DR_PROBE_MIE_EXACT_DIR && c->params.phase_mode != DR_PHASE_MIE_EXACT)
         return need(false, DR_ERR_STATE, "dr_probe_sampler: the exact sampler needs DR_PHASE_MIE_EXACT");
-    const size_t in_n = what == DR_PROBE_MIE_SAMPLE ? 5ull * n
+    if (what == DR_PROBE_ENV_MAP && c->params.env_mode != DR_ENV_MAP)
+        return need(false, DR_ERR_STATE, "dr_probe_sampler: the environment map probe needs DR_ENV_MAP");
+    const size_t in_n = (what == DR_PROBE_MIE_SAMPLE || what == DR_PROBE_HG_SAMPLE) ? 5ull * n
                         : what == DR_PROBE_SUN_SAMPLE ? 2ull * n
-                        : what == DR_PROBE_SKY ? 3ull * n
+                        : (what == DR_PROBE_SKY || what == DR_PROBE_SKY_LIGHT || what == DR_PROBE_ENV_MAP) ? 3ull * n
                         : (size_t)n;
-    const size_t out_n = what == DR_PROBE_MIE_THETA ? (size_t)n : what == DR_PROBE_MIE_EXACT_DIR ? 2ull * n : 3ull * n;
+    const size_t out_n = (what == DR_PROBE_MIE_THETA || what == DR_PROBE_HG_EVAL) ? (size_t)n
+                         : what == DR_PROBE_MIE_EXACT_DIR ? 2ull * n : 3ull * n;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     Scratch S;

@@ -22,7 +22,7 @@ struct dr_batch {
     dr_ctx *ctx = nullptr;
     cudaStream_t stream = nullptr;  // capture stream
     std::vector<std::unique_ptr<SceneBufs>> scene_bufs;
-    std::vector<std::unique_ptr<DevBuf<float>>> depth_bufs;
+    std::vector<std::unique_ptr<DevBuf<float>>> depth_bufs;  // per-view depth textures and environment maps
     DevBuf<DevScene> scenes;
     DevBuf<BatchView> views;
     DevBuf<uint64_t> begins;
@@ -79,8 +79,10 @@ int build_graph(dr_batch *b) {
     B.step = b->step.p;
     DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");
     cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
+    bool ext = false;  // a view with the HG phase or an environment other than the Hosek sky
+    for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
     if (e == cudaSuccess)
-        e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning,
+        e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
                                 b->ctx->device, b->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
@@ -185,6 +187,15 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
             BATCH_CUDA(cudaMemcpy(d.p, p->depth, sizeof(float) * p->w * p->h, cudaMemcpyHostToDevice),
                        "dr_batch_create: copy depth");
             hv[v].P.depth = d.p;
+        }
+        if (p->env_mode == DR_ENV_MAP) {
+            const size_t n = (size_t)p->env_w * p->env_h * 4;
+            b->depth_bufs.emplace_back(new DevBuf<float>());
+            DevBuf<float> &d = *b->depth_bufs.back();
+            BATCH_CUDA(d.reserve(n), "dr_batch_create: alloc environment map");
+            BATCH_CUDA(cudaMemcpy(d.p, p->env_map, sizeof(float) * n, cudaMemcpyHostToDevice),
+                       "dr_batch_create: copy environment map");
+            hv[v].P.env_map = d.p;
         }
     }
     BATCH_CUDA(b->scenes.reserve(n_scenes), "dr_batch_create: alloc scenes");

@@ -17,6 +17,9 @@ __device__ __forceinline__ float sse_min(float a, float b) { return a < b ? a : 
 __device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; } // std::max
 __device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; } // std::min
 __device__ __forceinline__ float lerp_ref(float a, float b, float t) { return t * (b - a) + a; }  // t.madd(b-a, a)
+// sfloat1::saturate = _mm_max_ps(_mm_min_ps(x, 1), 0): NaN gives 1.  The NaN case
+// is explicit so that no rewrite into a hardware saturate (NaN -> 0) applies.
+__device__ __forceinline__ float sat_ref(float x) { return x != x ? 1.0f : sse_max(sse_min(x, 1.0f), 0.0f); }
 
 // ---- bit-reproducible transcendentals --------------------------------------
 // Same operation sequences as the CPU restatement, built from IEEE binary32
@@ -709,6 +712,36 @@ __device__ __forceinline__ void mie_sample(const MieSmem &M, const float iv[3], 
     compose_dir(iv, st, ct, ph, out);
 }
 
+// ---- phase function: HGPhase, src/KernelSampler.cpp:164-204 (DR_PHASE_HG) ----
+// g = HGPhase::g1 (blcloudsampling.phasea); the same value for r, g and b.
+__device__ __forceinline__ float hg_eval(float g, float ct) {
+    const float den = 12.566371f * dpow((1.0f + g * g) - (2.0f * g) * ct, 1.5f);  // float(4 SM_PI) * pow(., 1.5)
+    return (1.0f - g * g) / den;
+}
+
+__device__ __forceinline__ void hg_sample(float g, const float iv[3], float u1, float u2, float out[3]) {
+    const float sq = (1.0f - g * g) / ((1.0f - g) + (2.0f * g) * u1);
+    const float ct = ((1.0f + g * g) - sq * sq) / (2.0f * g);
+    const float st = sqrtf(sse_max(1.0f - ct * ct, 0.0f));
+    compose_dir(iv, st, ct, (2.0f * kPi) * u2, out);
+}
+
+// The path's phase function: PhaseFunction::EvaluateRGB / Sample of the
+// selected model (src/main.cpp:522-536).
+__device__ __forceinline__ float3 phase_eval_rgb(const DevParams &P, const MieSmem &M, float ct) {
+    if (P.phase_mode == kPhaseHG) {
+        const float v = hg_eval(P.hg_g, ct);
+        return make_float3(v, v, v);
+    }
+    return mie_eval_rgb(M, ct);
+}
+
+__device__ __forceinline__ void phase_sample(const DevParams &P, const MieSmem &M, const float iv[3], float u1, float u2,
+                                             float out[3]) {
+    if (P.phase_mode == kPhaseHG) hg_sample(P.hg_g, iv, u1, u2, out);
+    else mie_sample(M, iv, u1, u2, out);
+}
+
 // ---- sun: SunLight, src/KernelSampler.cpp:318-345 --------------------------
 __device__ __forceinline__ float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
@@ -739,7 +772,7 @@ __device__ __forceinline__ float3 sky_eval(const DevParams &P, const float rd[3]
     const float czp = acr * (rdd * slph + clph);
     const float cph = (sth * slth) * czp + cth * clth;
     const float gmma = acos_ref(cph);
-    const float gacs = sse_max(sse_min(cph, 1.0f), 0.0f);
+    const float gacs = sat_ref(cph);
     const float thcs = sse_max(rdz, 0.0f);
     const float raym = gacs * gacs;
     float out[3];
@@ -755,6 +788,90 @@ __device__ __forceinline__ float3 sky_eval(const DevParams &P, const float rd[3]
         out[i] = 1e-3f * dpow(ca, 2.2f);
     }
     return make_float3(out[0], out[1], out[2]);
+}
+
+// atan2 of smmath.inl (src/smmath.inl:430-445): polynomial in min/max ratio,
+// then the octant corrections.
+__device__ __forceinline__ float atan2_ref(float y, float x) {
+    const float X = sse_max(0.0f - x, x), Y = sse_max(0.0f - y, y);
+    float a = sse_min(X, Y) / sse_max(X, Y);
+    const float b = a * a;
+    float p = -0.013480470f * b + 0.057477314f;
+    p = p * b - 0.121239071f;
+    p = p * b + 0.195635925f;
+    p = p * b - 0.332994597f;
+    p = p * b + 0.999995630f;
+    a = a * p;
+    if (Y > X) a = 1.57079637f - a;  // float(0.5 SM_PI)
+    if (x < 0.0f) a = kPi - a;
+    if (y < 0.0f) a = 0.0f - a;
+    return a;
+}
+
+// MapEnv::Evaluate (src/KernelSampler.cpp:384-417): bilinear lookup of an
+// equirectangular RGBA map (theta rows from acos(-rd.z), phi columns from
+// atan2(rd.y, -rd.x)); texel indices are formed in binary32 as there.
+__device__ __forceinline__ float3 env_map_eval(const DevParams &P, const float rd[3]) {
+    const float fw = (float)P.env_w, fh = (float)P.env_h;
+    const float tha = acos_ref(0.0f - rd[2]) / kPi;
+    const float thb = fh * sat_ref(tha);
+    float thc = floorf(thb);
+    thc = sse_min(thc, (float)(P.env_h - 2));
+    thc = sse_max(thc, 0.0f);
+    const float tht = thb - thc;
+    const float pha = 0.5f + atan2_ref(rd[1], 0.0f - rd[0]) / 6.2831855f;  // float(2 SM_PI)
+    const float phb = fw * sat_ref(pha);
+    float phc = floorf(phb);
+    phc = sse_min(phc, (float)(P.env_w - 2));
+    phc = sse_max(phc, 0.0f);
+    const float pht = phb - phc;
+    const float4 *T = reinterpret_cast<const float4 *>(P.env_map);
+    const float4 ca = __ldg(&T[(uint32_t)(fw * thc + phc)]), cb = __ldg(&T[(uint32_t)(fw * (thc + 1.0f) + phc)]);
+    const float4 da = __ldg(&T[(uint32_t)(fw * thc + phc + 1.0f)]),
+                 db = __ldg(&T[(uint32_t)(fw * (thc + 1.0f) + phc + 1.0f)]);
+    return make_float3(lerp_ref(lerp_ref(ca.x, cb.x, tht), lerp_ref(da.x, db.x, tht), pht),
+                       lerp_ref(lerp_ref(ca.y, cb.y, tht), lerp_ref(da.y, db.y, tht), pht),
+                       lerp_ref(lerp_ref(ca.z, cb.z, tht), lerp_ref(da.z, db.z, tht), pht));
+}
+
+// Light gathered from the sky on escape: the Hosek model (the reference built
+// with USE_ARHOSEK_SKYMODEL), or pow(environment, 2.2) of its default build
+// with NullEnv (zero) or MapEnv (src/kernel.cpp:361-364).
+__device__ __forceinline__ float3 sky_light(const DevParams &P, const float rd[3]) {
+    if (P.env_mode == kEnvHosek) return sky_eval(P, rd);
+    if (P.env_mode == kEnvNone) return make_float3(dpow(0.0f, 2.2f), dpow(0.0f, 2.2f), dpow(0.0f, 2.2f));
+    const float3 e = env_map_eval(P, rd);
+    return make_float3(dpow(e.x, 2.2f), dpow(e.y, 2.2f), dpow(e.z, 2.2f));
+}
+
+// Feature bits of a kernel instantiation.  Frames that use neither run the
+// instantiation without their code (its register use and size stay those of
+// the Mie/Hosek path).
+enum : uint32_t {
+    kFeatOcc = 1,  // occluders present and the USE_EMBREE build's masks apply
+    kFeatExt = 2,  // HG phase or an environment other than the Hosek sky
+    kFeatAll = 3,
+};
+
+// Escape light of a segment: the Hosek sky, or (kFeatExt) whichever
+// environment the parameters select.
+template <uint32_t FEAT>
+__device__ __forceinline__ float3 escape_sky(const DevParams &P, const float rd[3]) {
+    if constexpr ((FEAT & kFeatExt) != 0) return sky_light(P, rd);
+    else return sky_eval(P, rd);
+}
+
+template <uint32_t FEAT>
+__device__ __forceinline__ float3 path_phase_eval(const DevParams &P, const MieSmem &M, float ct) {
+    if constexpr ((FEAT & kFeatExt) != 0) return phase_eval_rgb(P, M, ct);
+    else return mie_eval_rgb(M, ct);
+}
+
+template <uint32_t FEAT>
+__device__ __forceinline__ void path_phase_sample(const DevParams &P, const MieSmem &M, const float iv[3], float u1,
+                                                  float u2, float out[3]) {
+    if constexpr ((FEAT & kFeatExt) != 0) phase_sample(P, M, iv, u1, u2, out);
+    else mie_sample(M, iv, u1, u2, out);
 }
 
 // ---- camera ray, K_ParallelRender (src/kernel.cpp:461-474) -----------------
@@ -985,6 +1102,7 @@ __device__ __forceinline__ float first_alpha(const DevParams &P, uint32_t res) {
     return (res == kTrackCollided || (res == kTrackCut && !P.embree)) ? 1.0f : 0.0f;
 }
 
+template <uint32_t FEAT = kFeatAll>
 __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
                                             uint32_t py, uint64_t seed, uint64_t sample, float4 &sun_acc,
                                             float4 &sky_acc, uint32_t *nstack, Count &cnt) {
@@ -1002,7 +1120,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
         if (r == 0) sun_acc.w = sky_acc.w = first_alpha(P, res);
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
-            if (r > 0 && !(P.embree && occluded(S, ro, rd))) {
+            if (r > 0 && !((FEAT & kFeatOcc) && P.embree && occluded(S, ro, rd))) {
                 if (sun_hit(P, rd)) {
                     sun_acc.x = sun_acc.x + T0 * P.sun_color[0];
                     sun_acc.y = sun_acc.y + T1 * P.sun_color[1];
@@ -1012,7 +1130,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
                     sun_acc.y = sun_acc.y + T1 * 0.0f;
                     sun_acc.z = sun_acc.z + T2 * 0.0f;
                 }
-                const float3 sky = sky_eval(P, rd);
+                const float3 sky = escape_sky<FEAT>(P, rd);
                 sky_acc.x = sky_acc.x + T0 * sky.x;
                 sky_acc.y = sky_acc.y + T1 * sky.y;
                 sky_acc.z = sky_acc.z + T2 * sky.z;
@@ -1022,19 +1140,19 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
         if (r >= P.scattevs) break;
         float srd[3], lrd[3], rc[3];
         const float u1 = g.uniform(), u2 = g.uniform();
-        mie_sample(M, rd, u1, u2, srd);
+        path_phase_sample<FEAT>(P, M, rd, u1, u2, srd);
         const float u3 = g.uniform(), u4 = g.uniform();
         sun_sample(P, u3, u4, lrd);
-        const float3 p1 = mie_eval_rgb(M, dot3(srd, rd));
+        const float3 p1 = path_phase_eval<FEAT>(P, M, dot3(srd, rd));
         const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
-        const float3 p3 = mie_eval_rgb(M, dot3(lrd, rd));
+        const float3 p3 = path_phase_eval<FEAT>(P, M, dot3(lrd, rd));
         const float q1 = sun_hit(P, srd) ? P.sun_pdf : 0.0f;
         cnt.mie_evals += 3;
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         float tds;
         if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped &&
-            !(P.embree && occluded(S, rc, lrd))) {
+            !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd))) {
             const bool hit = sun_hit(P, lrd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;

@@ -210,10 +210,27 @@ int upload_scene(const HostScene &h, SceneBufs &b, bool use_grid, cudaStream_t s
 
 int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned char> &pack) {
     if (!p) return need(false, DR_ERR_INVALID, "dr_set_params: null argument");
+    if (p->phase_mode != DR_PHASE_MIE_REFERENCE && p->phase_mode != DR_PHASE_MIE_EXACT && p->phase_mode != DR_PHASE_HG)
+        return need(false, DR_ERR_INVALID, "dr_set_params: unknown phase mode");
+    if (p->phase_mode == DR_PHASE_HG && !(std::fabs(p->hg_g) < 1.0f))
+        return need(false, DR_ERR_INVALID, "dr_set_params: HG anisotropy needs |g| < 1");
+    // the HG phase needs no table: stage a 4-entry placeholder when none is given
+    static const float kNoTable[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    dr_render_params q = *p;
+    if (p->phase_mode == DR_PHASE_HG && (!p->mie_pdf || !p->mie_cdf || p->mie_n == 0)) {
+        q.mie_pdf = kNoTable;
+        q.mie_cdf = kNoTable;
+        q.mie_n = 4;
+    }
+    p = &q;
     if (!p->mie_pdf || !p->mie_cdf || p->mie_n < 4 || p->mie_n > kMieMax || (p->mie_n % 4))
         return need(false, DR_ERR_INVALID, "dr_set_params: phase tables need 4 <= mie_n <= 4096, mie_n % 4 == 0");
-    if (p->phase_mode != DR_PHASE_MIE_REFERENCE && p->phase_mode != DR_PHASE_MIE_EXACT)
-        return need(false, DR_ERR_INVALID, "dr_set_params: unknown phase mode");
+    if (p->env_mode != DR_ENV_HOSEK && p->env_mode != DR_ENV_NONE && p->env_mode != DR_ENV_MAP)
+        return need(false, DR_ERR_INVALID, "dr_set_params: unknown environment mode");
+    // texel indices are formed in binary32 (as MapEnv::Evaluate does): exact below 2^24
+    if (p->env_mode == DR_ENV_MAP && (!p->env_map || p->env_w < 2 || p->env_h < 2 ||
+                                      (uint64_t)p->env_w * p->env_h > (1ull << 24)))
+        return need(false, DR_ERR_INVALID, "dr_set_params: environment map needs 2 <= w, h and w*h <= 2^24 texels");
     if (p->phase_mode == DR_PHASE_MIE_EXACT && p->mie_n > 512)
         return need(false, DR_ERR_INVALID, "dr_set_params: the exact phase sampler takes mie_n <= 512");
     for (uint32_t i = 0; i < p->mie_n; ++i)
@@ -249,6 +266,11 @@ int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned
     d.depthcomp = (p->flags & DR_KERNEL_DEPTHCOMP) ? 1u : 0u;
     d.finite_paths = (p->flags & DR_KERNEL_FINITE_PATHS) ? 1u : 0u;
     d.embree = (p->flags & DR_KERNEL_EMBREE) ? 1u : 0u;
+    d.hg_g = p->hg_g;
+    d.env_mode = p->env_mode;
+    d.env_w = p->env_mode == DR_ENV_MAP ? p->env_w : 0u;
+    d.env_h = p->env_mode == DR_ENV_MAP ? p->env_h : 0u;
+    d.env_map = nullptr;  // the caller copies the texels to the device
     if (p->flags & ~(DR_KERNEL_DEPTHCOMP | DR_KERNEL_FINITE_PATHS | DR_KERNEL_EMBREE))
         return need(false, DR_ERR_INVALID, "dr_set_params: unknown flags");
     {

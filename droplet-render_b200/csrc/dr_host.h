@@ -120,6 +120,7 @@ struct dr_ctx {
     dr::SceneBufs bufs;
     dr::DevBuf<unsigned char> mie_pack;
     dr::DevBuf<float> depth;
+    dr::DevBuf<float> env;            // environment map texels (DR_ENV_MAP)
     dr::DevBuf<dr::DevCounters> counters;
     dr::DevBuf<float4> tile_sun, tile_sky;
     dr::DevBuf<unsigned char> scratch;

@@ -52,6 +52,9 @@ struct DevScene {
     uint32_t occ_n_nodes;
 };
 
+constexpr uint32_t kPhaseHG = 2;     // DR_PHASE_HG
+constexpr uint32_t kEnvHosek = 0, kEnvNone = 1, kEnvMap = 2;  // DR_ENV_*
+
 constexpr int kOccMaxDepth = 48;     // occluder BVH depth (the traversal stack holds one entry per level)
 constexpr float kOccFar = 1e6f;      // MAX_OCCLUSION_DIST, src/SceneOcclusion.h:4
 
@@ -71,6 +74,10 @@ struct DevParams {
     uint32_t depthcomp;       // KERNEL_DEPTHCOMP: camera rays stop at depth
     uint32_t finite_paths;    // a path whose contribution is not finite adds nothing
     uint32_t embree;          // the reference's USE_EMBREE build: occluder and depth masks on gathered light
+    float hg_g;               // kPhaseHG: anisotropy
+    uint32_t env_mode;        // kEnvHosek, kEnvNone or kEnvMap
+    const float *env_map;     // kEnvMap: env_w * env_h RGBA texels (device)
+    uint32_t env_w, env_h;
     float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
 };
 

@@ -83,6 +83,7 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
 // One thread per (pixel, sample) path; thread g renders pixel g / spp, sample
 // g % spp, so a warp holds 32 consecutive samples of a pixel when spp % 32 == 0
 // and reduces them with a fixed shuffle tree before one float4 atomic.
+template <uint32_t FEAT>
 __global__ void __launch_bounds__(kRenderBlock) render_tile_kernel(DevScene S, DevParams P, TileArgs A,
                                                                    const void *mie_pack, float4 *sun_out,
                                                                    float4 *sky_out, DevCounters *C) {
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(kRenderBlock) render_tile_kernel(DevScene S, D
         float ro[3], rd[3];
         if (camera_ray(P, A.x0 + i, A.y0 + j, ro, rd)) {
             paths = 1;
-            path_sample(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, sa, sk, nstack, cnt);
+            path_sample<FEAT>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, sa, sk, nstack, cnt);
         }
     }
     if (!staged) cnt.gave_up += (g < A.n_paths) ? 1u : 0u;
@@ -352,16 +353,14 @@ __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
     return 0;
 }
 
-// Segment end: the body of path_sample() between two track() calls.  OCC:
-// occluders are present and the USE_EMBREE build's masks apply (a separate
-// instantiation, so frames without occluders carry no traversal code).
-template <bool WALK, bool OCC>
+// Segment end: the body of path_sample() between two track() calls.
+template <bool WALK, uint32_t FEAT>
 __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
                                         const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
                                         uint32_t &state, Trav *slow) {
     const float f = P.albedo;
     if (L.seg == kSegShadow) {
-        if (L.esc == kTrackEscaped && !(OCC && occluded(S, L.ro, L.rd))) {
+        if (L.esc == kTrackEscaped && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
             const bool hit = sun_hit(P, L.rd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
                         s2 = hit ? P.sun_color[2] : 0.0f;
@@ -381,7 +380,7 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
     }
     if (L.r == 0) L.sun.w = L.sky.w = first_alpha(P, L.esc);
     if (L.esc == kTrackEscaped) {
-        if (L.r > 0 && !(OCC && occluded(S, L.ro, L.rd))) {
+        if (L.r > 0 && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
             if (sun_hit(P, L.rd)) {
                 L.sun.x = L.sun.x + L.T[0] * P.sun_color[0];
                 L.sun.y = L.sun.y + L.T[1] * P.sun_color[1];
@@ -391,7 +390,7 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
                 L.sun.y = L.sun.y + L.T[1] * 0.0f;
                 L.sun.z = L.sun.z + L.T[2] * 0.0f;
             }
-            const float3 sky = sky_eval(P, L.rd);
+            const float3 sky = escape_sky<FEAT>(P, L.rd);
             L.sky.x = L.sky.x + L.T[0] * sky.x;
             L.sky.y = L.sky.y + L.T[1] * sky.y;
             L.sky.z = L.sky.z + L.T[2] * sky.z;
@@ -407,12 +406,13 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
     }
     float lrd[3];
     const float u1 = L.g.uniform(), u2 = L.g.uniform();
-    mie_sample(M, L.rd, u1, u2, L.srd);
+    if constexpr ((FEAT & kFeatExt) != 0) phase_sample(P, M, L.rd, u1, u2, L.srd);
+    else mie_sample(M, L.rd, u1, u2, L.srd);
     const float u3 = L.g.uniform(), u4 = L.g.uniform();
     sun_sample(P, u3, u4, lrd);
-    const float3 p1 = mie_eval_rgb(M, dot3(L.srd, L.rd));
+    const float3 p1 = (FEAT & kFeatExt) ? phase_eval_rgb(P, M, dot3(L.srd, L.rd)) : mie_eval_rgb(M, dot3(L.srd, L.rd));
     const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
-    const float3 p3 = mie_eval_rgb(M, dot3(lrd, L.rd));
+    const float3 p3 = (FEAT & kFeatExt) ? phase_eval_rgb(P, M, dot3(lrd, L.rd)) : mie_eval_rgb(M, dot3(lrd, L.rd));
     const float q1 = sun_hit(P, L.srd) ? P.sun_pdf : 0.0f;
     cnt.mie_evals += 3;
     L.sw[0] = L.T[0] * ((p3.x / (p3.x + p2)) * f);
@@ -469,13 +469,13 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
 }
 
 // One loop iteration of a lane that holds a path (see render_persistent_kernel).
-template <bool WALK, bool OCC>
+template <bool WALK, uint32_t FEAT>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
                                           Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits,
                                           uint32_t steps, float (*tstack)[6]) {
     if (events) {
-        if (state == kEvent) path_event<WALK, OCC>(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
+        if (state == kEvent) path_event<WALK, FEAT>(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
     }
     if (state == kTrav) {
@@ -509,7 +509,7 @@ __device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
 // BATCH: the paths of many views (each with its own scene, parameters, tile
 // and output) share one work queue; a lane looks its view up when it fetches
 // a path and reads that view's records from global memory (L1-resident).
-template <int MINB, bool WALK, bool BATCH, bool OCC>
+template <int MINB, bool WALK, bool BATCH, uint32_t FEAT>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
                                                                             float4 *sky_out, DevCounters *C,
@@ -579,10 +579,10 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work<WALK, OCC>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow,
+            lane_work<WALK, FEAT>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow,
                                  visits, steps, ts);
         } else {
-            lane_work<WALK, OCC>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps,
+            lane_work<WALK, FEAT>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps,
                                  ts);
         }
     }
@@ -708,6 +708,21 @@ __global__ void probe_sampler_kernel(DevParams P, const void *mie_pack, uint32_t
         mie_exact_dir(M.ex, M.n, in[i], ct, st);
         out[2 * i] = ct;
         out[2 * i + 1] = st;
+    } else if (what == 6u) {
+        out[i] = hg_eval(P.hg_g, in[i]);
+    } else if (what == 7u) {
+        const float iv[3] = {in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+        float d[3];
+        hg_sample(P.hg_g, iv, in[3 * n + i], in[4 * n + i], d);
+        out[3 * i] = d[0];
+        out[3 * i + 1] = d[1];
+        out[3 * i + 2] = d[2];
+    } else if (what == 8u || (what == 9u && P.env_mode == kEnvMap)) {
+        const float rd[3] = {in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+        const float3 s = what == 8u ? sky_light(P, rd) : env_map_eval(P, rd);
+        out[3 * i] = s.x;
+        out[3 * i + 1] = s.y;
+        out[3 * i + 2] = s.z;
     }
 }
 
@@ -846,7 +861,7 @@ __device__ __forceinline__ float dot3f(const float3 a, const float3 b) { return 
 // MODE kPassTotals fills tot; kPassScatter scatters with tot known;
 // kPassRatio fills tot.w for the reweighted replay (pert = perturbed bricks).
 enum : int { kPassTotals = 0, kPassScatter = 1, kPassRatio = 2 };
-template <int MODE>
+template <int MODE, uint32_t FEAT>
 __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams &P, const MieSmem &M, uint32_t px,
                                              uint32_t py, uint64_t seed, uint64_t sample, float3 dsun, float3 dsky,
                                              PathTotals &tot, float *grad, uint32_t *nstack,
@@ -882,11 +897,11 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         }
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
-            if (r > 0 && !(P.embree && occluded(S, ro, rd))) {
+            if (r > 0 && !((FEAT & kFeatOcc) && P.embree && occluded(S, ro, rd))) {
                 const bool hit = sun_hit(P, rd);
                 const float3 cs = f3(T0 * (hit ? P.sun_color[0] : 0.0f), T1 * (hit ? P.sun_color[1] : 0.0f),
                                      T2 * (hit ? P.sun_color[2] : 0.0f));
-                const float3 sk = sky_eval(P, rd);
+                const float3 sk = escape_sky<FEAT>(P, rd);
                 const float3 ck = f3(T0 * sk.x, T1 * sk.y, T2 * sk.z);
                 const float m = (float)r;
                 acc_sun = f3(acc_sun.x + cs.x, acc_sun.y + cs.y, acc_sun.z + cs.z);
@@ -899,12 +914,12 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         if (r >= P.scattevs) break;
         float srd[3], lrd[3], rc[3];
         const float u1 = g.uniform(), u2 = g.uniform();
-        mie_sample(M, rd, u1, u2, srd);
+        path_phase_sample<FEAT>(P, M, rd, u1, u2, srd);
         const float u3 = g.uniform(), u4 = g.uniform();
         sun_sample(P, u3, u4, lrd);
-        const float3 p1 = mie_eval_rgb(M, dot3(srd, rd));
+        const float3 p1 = path_phase_eval<FEAT>(P, M, dot3(srd, rd));
         const float p2 = sun_hit(P, lrd) ? P.sun_pdf : 0.0f;
-        const float3 p3 = mie_eval_rgb(M, dot3(lrd, rd));
+        const float3 p3 = path_phase_eval<FEAT>(P, M, dot3(lrd, rd));
         const float q1 = sun_hit(P, srd) ? P.sun_pdf : 0.0f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
@@ -924,7 +939,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
             if (known) {
                 lit = (tot.esc >> r) & 1ull;
             } else {
-                lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
+                lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
                 sv.w = dot3f(dsun, cn);
                 if (lit && sv.w != 0.0f) {
                     Rng g1 = g0;  // the same draws again: ends in the state g already holds
@@ -936,11 +951,11 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
             const uint32_t sres = track_ratio(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
-            lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
+            lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             cn = f3(cn.x * ws, cn.y * ws, cn.z * ws);
         } else {
             const uint32_t sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
-            lit = sres == kTrackEscaped && !(P.embree && occluded(S, rc, lrd));
+            lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             if (lit && r < kEscBits) tot.esc |= 1ull << r;
         }
         if (lit) {
@@ -1012,6 +1027,7 @@ __device__ __forceinline__ void tile_path(const TileArgs &A, uint64_t gi, uint32
 // dsky . C_sky (NaN for a path left out: zero delta at its pixel, or a
 // contribution that is not finite, the sky term's 0/0 for rd.y == 0) and its
 // lit-shadow bits; the albedo term goes to the slots.
+template <uint32_t FEAT>
 __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S, DevParams P, TileArgs A,
                                                                       uint64_t p0, uint64_t n, const void *mie_pack,
                                                                       const float4 *dsun, const float4 *dsky,
@@ -1033,7 +1049,7 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S
         PathRecord pr{__int_as_float(0x7fffffff), 0u, 0u, 0u};
         if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
             PathTotals tot{};
-            adjoint_pass<kPassTotals>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
+            adjoint_pass<kPassTotals, FEAT>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot, nullptr,
                                 nstack);
             if (tot.ok) {
                 pr.w = tot.w;
@@ -1053,6 +1069,7 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_totals_kernel(DevScene S
 // gradient (grad + copy * stride): the surface samples every path meets
 // first are hit by all warps at once, and spreading them over copies divides
 // the conflicts on each address; the copies are summed afterwards.
+template <uint32_t FEAT>
 __global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene S, DevParams P, TileArgs A,
                                                                        uint64_t p0, uint64_t n, const void *mie_pack,
                                                                        const float4 *dsun, const float4 *dsky,
@@ -1076,7 +1093,7 @@ __global__ void __launch_bounds__(kRenderBlock) adjoint_scatter_kernel(DevScene 
             PathTotals tot{};
             tot.w = pr.w;
             tot.esc = ((uint64_t)pr.esc_hi << 32) | pr.esc_lo;
-            adjoint_pass<kPassScatter>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
+            adjoint_pass<kPassScatter, FEAT>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, f3(ds.x, ds.y, ds.z),
                                f3(dk.x, dk.y, dk.z), tot, grad, nstack);
         }
     }
@@ -1097,6 +1114,7 @@ __device__ __forceinline__ void warp_add_d(double v, double *slots) {
 // dsun . C_sun + dsky . C_sky, each path weighted by its decisions' ratios
 // under pert (paths whose contribution is not finite are left out, as in the
 // adjoint).
+template <uint32_t FEAT>
 __global__ void __launch_bounds__(kRenderBlock) reweighted_loss_kernel(DevScene S, DevParams P, TileArgs A,
                                                                        const void *mie_pack, const float4 *dsun,
                                                                        const float4 *dsky, const float *pert,
@@ -1116,7 +1134,7 @@ __global__ void __launch_bounds__(kRenderBlock) reweighted_loss_kernel(DevScene 
         const float3 dsun3 = f3(ds.x, ds.y, ds.z), dsky3 = f3(dk.x, dk.y, dk.z);
         if (dot3f(dsun3, dsun3) + dot3f(dsky3, dsky3) > 0.0f) {
             PathTotals tot{};
-            adjoint_pass<kPassRatio>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot,
+            adjoint_pass<kPassRatio, FEAT>(S, P, M, A.x0 + i, A.y0 + j, A.seed, A.sample_base + s, dsun3, dsky3, tot,
                                      nullptr, nstack, pert);
             if (tot.ok) l = (double)tot.w;
         }
@@ -1247,12 +1265,23 @@ static size_t mie_smem(const DevParams &P) {
     return (size_t)P.mie_n * 20u + (P.phase_mode == 1u ? (2u * (size_t)P.mie_n + 1u) * 16u : 0u);
 }
 
+// Feature bits a frame needs.
+static uint32_t frame_features(const DevScene &S, const DevParams &P) {
+    return ((S.occ_nodes && P.embree) ? kFeatOcc : 0u) |
+           ((P.phase_mode == kPhaseHG || P.env_mode != kEnvHosek) ? kFeatExt : 0u);
+}
+
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
     const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
-    render_tile_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out, C);
+    if (frame_features(S, P))
+        render_tile_kernel<kFeatAll><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out,
+                                                                                       sky_out, C);
+    else
+        render_tile_kernel<0><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out,
+                                                                                C);
     return cudaGetLastError();
 }
 
@@ -1267,28 +1296,41 @@ cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const Tile
 
 // Variants of the persistent kernel compiled for 4, 5, 6 and 8 resident
 // blocks per SM (fewer registers, some spilled to L1-resident local memory),
-// each with the stack traversal or the cell walk, single frame or batch, and
-// for single frames with or without occluders.
+// each with the stack traversal or the cell walk, single frame or batch.  The
+// feature variants (occluders, HG phase / environment maps) exist for 5 and 8
+// blocks per SM; a tuned 4 or 6 maps to the nearest of those.
 using PersistentFn = void (*)(DevScene, DevParams, TileArgs, const void *, float4 *, float4 *, DevCounters *,
                               WorkQueue *, uint32_t, BatchArgs);
-template <bool BATCH, bool OCC>
+template <bool BATCH, uint32_t FEAT>
 static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
-    if (traversal == 1u) {
-        if (minb >= 8) return render_persistent_kernel<8, true, BATCH, OCC>;
-        if (minb >= 6) return render_persistent_kernel<6, true, BATCH, OCC>;
-        if (minb >= 5) return render_persistent_kernel<5, true, BATCH, OCC>;
-        return render_persistent_kernel<4, true, BATCH, OCC>;
+    if constexpr (FEAT != 0) {
+        if (traversal == 1u) return minb >= 7 ? render_persistent_kernel<8, true, BATCH, FEAT>
+                                              : render_persistent_kernel<5, true, BATCH, FEAT>;
+        return minb >= 7 ? render_persistent_kernel<8, false, BATCH, FEAT> : render_persistent_kernel<5, false, BATCH, FEAT>;
+    } else {
+        if (traversal == 1u) {
+            if (minb >= 8) return render_persistent_kernel<8, true, BATCH, 0>;
+            if (minb >= 6) return render_persistent_kernel<6, true, BATCH, 0>;
+            if (minb >= 5) return render_persistent_kernel<5, true, BATCH, 0>;
+            return render_persistent_kernel<4, true, BATCH, 0>;
+        }
+        if (minb >= 8) return render_persistent_kernel<8, false, BATCH, 0>;
+        if (minb >= 6) return render_persistent_kernel<6, false, BATCH, 0>;
+        if (minb >= 5) return render_persistent_kernel<5, false, BATCH, 0>;
+        return render_persistent_kernel<4, false, BATCH, 0>;
     }
-    if (minb >= 8) return render_persistent_kernel<8, false, BATCH, OCC>;
-    if (minb >= 6) return render_persistent_kernel<6, false, BATCH, OCC>;
-    if (minb >= 5) return render_persistent_kernel<5, false, BATCH, OCC>;
-    return render_persistent_kernel<4, false, BATCH, OCC>;
 }
 
 // Batches carry no occluders (their scenes come from dr_scene_desc records).
-static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch, bool occ = false) {
-    if (batch) return persistent_variant_of<true, false>(minb, traversal);
-    return occ ? persistent_variant_of<false, true>(minb, traversal) : persistent_variant_of<false, false>(minb, traversal);
+static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch, uint32_t feat = 0) {
+    if (batch) return (feat & kFeatExt) ? persistent_variant_of<true, kFeatExt>(minb, traversal)
+                                        : persistent_variant_of<true, 0>(minb, traversal);
+    switch (feat & (kFeatOcc | kFeatExt)) {
+    case kFeatOcc: return persistent_variant_of<false, kFeatOcc>(minb, traversal);
+    case kFeatExt: return persistent_variant_of<false, kFeatExt>(minb, traversal);
+    case kFeatOcc | kFeatExt: return persistent_variant_of<false, kFeatOcc | kFeatExt>(minb, traversal);
+    default: return persistent_variant_of<false, 0>(minb, traversal);
+    }
 }
 
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
@@ -1301,13 +1343,13 @@ int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t sm
 
 // Grid of the persistent kernel: SMs x resident blocks (the tuned count, capped
 // by what fits).
-static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, bool batch, bool occ,
+static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, bool batch, uint32_t feat,
                                    PersistentFn &fn, int &blocks, uint32_t &event_batch) {
     int sms = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
     const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
-    fn = persistent_variant(variant, tune.traversal, batch, occ);
+    fn = persistent_variant(variant, tune.traversal, batch, feat);
     int maxb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, kPersistentBlock, smem) != cudaSuccess || maxb < 1)
         maxb = 1;
@@ -1327,7 +1369,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, false, S.occ_nodes && P.embree, fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, false, frame_features(S, P), fn, blocks, batch);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
@@ -1336,13 +1378,13 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 }
 
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, int device,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext, int device,
                                 cudaStream_t st) {
     const size_t smem = mie_smem(P0);
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, true, false, fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatExt : 0u, fn, blocks, batch);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
@@ -1416,17 +1458,25 @@ cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const Til
         if (e != cudaSuccess) return e;
     }
     const size_t smem = mie_smem(P);
+    const uint32_t feat = frame_features(S, P);
     PathRecord *rec = (PathRecord *)records;
     for (uint64_t p0 = 0; p0 < A.n_paths; p0 += chunk) {
         const uint64_t n = A.n_paths - p0 < chunk ? A.n_paths - p0 : chunk;
         const unsigned blocks = (unsigned)((n + kRenderBlock - 1) / kRenderBlock);
-        adjoint_totals_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, rec, slots,
-                                                                   C);
+        if (feat)
+            adjoint_totals_kernel<kFeatAll><<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky,
+                                                                             rec, slots, C);
+        else
+            adjoint_totals_kernel<0><<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, rec,
+                                                                      slots, C);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        adjoint_scatter_kernel<<<blocks, kRenderBlock, smem, st>>>(S, P, A, p0, n, mie_pack, dsun, dsky, rec,
-                                                                    spread ? copies_buf : grad,
-                                                                    spread ? copies : 1u, stride, C);
+        if (feat)
+            adjoint_scatter_kernel<kFeatAll><<<blocks, kRenderBlock, smem, st>>>(
+                S, P, A, p0, n, mie_pack, dsun, dsky, rec, spread ? copies_buf : grad, spread ? copies : 1u, stride, C);
+        else
+            adjoint_scatter_kernel<0><<<blocks, kRenderBlock, smem, st>>>(
+                S, P, A, p0, n, mie_pack, dsun, dsky, rec, spread ? copies_buf : grad, spread ? copies : 1u, stride, C);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -1445,8 +1495,12 @@ cudaError_t launch_reweighted_loss(const DevScene &S, const DevParams &P, const 
     if (A.n_paths > 0) {
         const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
         if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
-        reweighted_loss_kernel<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, dsun, dsky,
-                                                                                    pert, slots, C);
+        if (frame_features(S, P))
+            reweighted_loss_kernel<kFeatAll><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(
+                S, P, A, mie_pack, dsun, dsky, pert, slots, C);
+        else
+            reweighted_loss_kernel<0><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, dsun,
+                                                                                        dsky, pert, slots, C);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -20,7 +20,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 // which fix the shared phase tables), then one increment of *step; Q->next is
 // cleared on st first.  The three launches are what a batch's graph captures.
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, int device,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext, int device,
                                 cudaStream_t st);
 // Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);

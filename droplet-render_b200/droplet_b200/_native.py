@@ -24,6 +24,10 @@ DR_NONE = 0xFFFFFFFF
 
 DR_PHASE_MIE_REFERENCE = 0
 DR_PHASE_MIE_EXACT = 1
+DR_PHASE_HG = 2
+DR_ENV_HOSEK = 0
+DR_ENV_NONE = 1
+DR_ENV_MAP = 2
 DR_KERNEL_DEPTHCOMP = 0x1
 DR_KERNEL_FINITE_PATHS = 0x2
 DR_KERNEL_EMBREE = 0x4
@@ -34,6 +38,10 @@ DR_PROBE_SUN_SAMPLE = 2
 DR_PROBE_SKY = 3
 DR_PROBE_MIE_THETA = 4
 DR_PROBE_MIE_EXACT_DIR = 5
+DR_PROBE_HG_EVAL = 6
+DR_PROBE_HG_SAMPLE = 7
+DR_PROBE_SKY_LIGHT = 8
+DR_PROBE_ENV_MAP = 9
 
 
 class DrError(RuntimeError):
@@ -96,6 +104,11 @@ class DrRenderParams(C.Structure):
         ("h", C.c_uint32),
         ("depth", C.c_void_p),
         ("flags", C.c_uint32),
+        ("hg_g", C.c_float),
+        ("env_mode", C.c_uint32),
+        ("env_map", C.c_void_p),
+        ("env_w", C.c_uint32),
+        ("env_h", C.c_uint32),
     ]
 
 

@@ -52,7 +52,10 @@ class RenderSettings:
     depthcomp: bool = False           # KERNEL_DEPTHCOMP: camera rays stop at the depth texture
     finite_paths: bool = False        # a path sample with a non-finite sum adds nothing (DR_KERNEL_FINITE_PATHS)
     embree: bool = False              # the reference's USE_EMBREE build: occluder and depth masks (DR_KERNEL_EMBREE)
-    phase_mode: int = N.DR_PHASE_MIE_REFERENCE
+    phase_mode: int = N.DR_PHASE_MIE_REFERENCE  # DR_PHASE_MIE_REFERENCE / _MIE_EXACT / _HG
+    hg_g: float = 0.0                 # DR_PHASE_HG: anisotropy (blcloudsampling.phasea)
+    env_mode: int = N.DR_ENV_HOSEK    # DR_ENV_HOSEK (sky state), DR_ENV_NONE, DR_ENV_MAP
+    env_map: np.ndarray | None = None  # DR_ENV_MAP: (h, w, 4) RGBA texels, row-major as MapEnv stores them
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> N.DrRenderParams:
@@ -64,11 +67,21 @@ class RenderSettings:
         for i in range(3):
             p.sky_configs[i][:] = [float(v) for v in self.sky.configs[i]]
         p.sky_radiances[:] = [float(v) for v in self.sky.radiances]
-        pdf = np.ascontiguousarray(self.phase.pdf, np.float32)
-        cdf = np.ascontiguousarray(self.phase.cdf, np.float32)
-        self._keep = [pdf, cdf]
-        p.mie_pdf, p.mie_cdf, p.mie_n = pdf.ctypes.data, cdf.ctypes.data, len(pdf)
+        self._keep = []
+        if self.phase is not None:
+            pdf = np.ascontiguousarray(self.phase.pdf, np.float32)
+            cdf = np.ascontiguousarray(self.phase.cdf, np.float32)
+            self._keep = [pdf, cdf]
+            p.mie_pdf, p.mie_cdf, p.mie_n = pdf.ctypes.data, cdf.ctypes.data, len(pdf)
         p.phase_mode = int(self.phase_mode)
+        p.hg_g = float(self.hg_g)
+        p.env_mode = int(self.env_mode)
+        if self.env_mode == N.DR_ENV_MAP:
+            e = np.ascontiguousarray(self.env_map, np.float32)
+            if e.ndim != 3 or e.shape[2] != 4:
+                raise ValueError("env_map must be (h, w, 4)")
+            self._keep.append(e)
+            p.env_map, p.env_h, p.env_w = e.ctypes.data, e.shape[0], e.shape[1]
         p.viewi[:] = [float(v) for v in np.asarray(self.viewi, np.float32).ravel()]
         p.proji[:] = [float(v) for v in np.asarray(self.proji, np.float32).ravel()]
         p.w, p.h = int(self.w), int(self.h)
@@ -316,7 +329,7 @@ class Renderer:
 
     def probe_sampler(self, what: int, inputs: np.ndarray, n: int):
         x = np.ascontiguousarray(inputs, np.float32).reshape(-1)
-        width = {N.DR_PROBE_MIE_THETA: 1, N.DR_PROBE_MIE_EXACT_DIR: 2}.get(what, 3)
+        width = {N.DR_PROBE_MIE_THETA: 1, N.DR_PROBE_MIE_EXACT_DIR: 2, N.DR_PROBE_HG_EVAL: 1}.get(what, 3)
         out = np.zeros(width * n, np.float32)
         N.check(N.lib().dr_probe_sampler(self._ctx, int(what), x.ctypes.data, int(n), out.ctypes.data))
         return out if width == 1 else out.reshape(n, width)

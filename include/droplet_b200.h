@@ -64,6 +64,11 @@ typedef struct {
 
 #define DR_PHASE_MIE_REFERENCE 0u  /* the reference's tabulated sampler (src/KernelSampler.cpp:257-285) */
 #define DR_PHASE_MIE_EXACT 1u      /* exact inverse CDF of the tabulated phase x sin(theta); mie_n <= 512 */
+#define DR_PHASE_HG 2u             /* HGPhase (src/KernelSampler.cpp:164-204), anisotropy hg_g; Mie tables optional */
+
+#define DR_ENV_HOSEK 0u  /* sky light from the Hosek-Wilkie state (the reference built with USE_ARHOSEK_SKYMODEL) */
+#define DR_ENV_NONE 1u   /* NullEnv: no sky light (its default build without an environment texture) */
+#define DR_ENV_MAP 2u    /* MapEnv (src/KernelSampler.cpp:377-417): pow(bilinear equirectangular texel, 2.2) */
 
 /* Everything RenderKernel::Initialize receives (src/kernel.cpp:497-534) plus
  * the sun light (src/main.cpp:374-404) and the sky state the reference
@@ -85,6 +90,10 @@ typedef struct {
     uint32_t w, h;                 /* full image size */
     const float *depth;            /* optional w*h depth texture (distance along the camera ray), or NULL */
     uint32_t flags;                /* DR_KERNEL_* below */
+    float hg_g;                    /* DR_PHASE_HG: HGPhase::g1 (blcloudsampling.phasea), |g| < 1 */
+    uint32_t env_mode;             /* DR_ENV_*: where escaping light comes from (src/kernel.cpp:329-364) */
+    const float *env_map;          /* DR_ENV_MAP: env_w * env_h RGBA floats, row-major (MapEnv::Initialize) */
+    uint32_t env_w, env_h;         /* DR_ENV_MAP: texels, each >= 2, env_w * env_h <= 2^24 */
 } dr_render_params;
 #define DR_KERNEL_DEPTHCOMP 0x1u     /* camera rays stop at depth (src/kernel.h:4) */
 #define DR_KERNEL_FINITE_PATHS 0x2u  /* a path sample whose sun or sky sum is not finite adds nothing (the
@@ -314,6 +323,10 @@ int dr_probe_paths(dr_ctx *ctx, const uint32_t *px, const uint32_t *py, const ui
 #define DR_PROBE_SKY 3u            /* in: rd[3n]           out: 3n */
 #define DR_PROBE_MIE_THETA 4u      /* in: u1[n]            out: n (theta / pi) */
 #define DR_PROBE_MIE_EXACT_DIR 5u  /* in: u1[n]            out: 2n (ct, st) of the exact sampler */
+#define DR_PROBE_HG_EVAL 6u        /* in: ct[n]            out: n  (HGPhase::Evaluate) */
+#define DR_PROBE_HG_SAMPLE 7u      /* in: iv[3n],u1[n],u2[n] out: 3n */
+#define DR_PROBE_SKY_LIGHT 8u      /* in: rd[3n]           out: 3n (light of an escaping ray, per env_mode) */
+#define DR_PROBE_ENV_MAP 9u        /* in: rd[3n]           out: 3n (MapEnv::Evaluate, before the 2.2 power) */
 int dr_probe_sampler(dr_ctx *ctx, uint32_t what, const float *in, uint32_t n, float *out);
 /* Fraction of nsamp delta-tracked segments along each ray that escape. */
 int dr_probe_transmittance(dr_ctx *ctx, const float *ro, const float *rd, uint32_t n_rays, uint64_t nsamp,

@@ -8,6 +8,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libdroplet_ref.so")
+REF_ENV_LIB = os.path.join(HERE, "_ref", "libdroplet_ref_env.so")  # built without USE_ARHOSEK_SKYMODEL
 PORT_LIB = os.path.join(HERE, "_port", "liboracle_port.so")
 NODE_DTYPE = np.dtype([("ce", "<f4", 4), ("chn", "<u4", 8), ("volx", "<u4", 2), ("qval", "<f4", 2)])
 assert NODE_DTYPE.itemsize == 64
@@ -34,7 +35,8 @@ class OrcParams(C.Structure):
         ("viewi", C.c_float * 16), ("proji", C.c_float * 16), ("w", C.c_uint32), ("h", C.c_uint32),
         ("depth", C.c_float), ("depth_map", C.c_void_p), ("depthcomp", C.c_uint32),
         ("phase_mode", C.c_uint32), ("mie_exact", C.c_void_p), ("finite_paths", C.c_uint32),
-        ("embree", C.c_uint32),
+        ("embree", C.c_uint32), ("hg_g", C.c_float), ("env_mode", C.c_uint32), ("env_map", C.c_void_p),
+        ("env_w", C.c_uint32), ("env_h", C.c_uint32),
     ]
 
 
@@ -87,6 +89,13 @@ class Port:
         L.orc_adjoint_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                           C.c_uint64, C.c_uint64, vp, vp, vp, vp, C.c_int]
         L.orc_adjoint_tile_mt.restype = C.c_int
+        L.orc_hg_eval.argtypes = [f32, f32]
+        L.orc_hg_eval.restype = f32
+        L.orc_hg_sample.argtypes = [f32, vp, f32, f32, vp]
+        L.orc_atan2_ref.argtypes = [f32, f32]
+        L.orc_atan2_ref.restype = f32
+        L.orc_env_map_eval.argtypes = [C.POINTER(OrcParams), vp, vp]
+        L.orc_sky_light.argtypes = [C.POINTER(OrcParams), vp, vp]
         L.orc_occluded.argtypes = [C.POINTER(OrcScene), vp, vp]
         L.orc_occluded.restype = C.c_int
         L.orc_shadow_ray.argtypes = [C.POINTER(OrcParams), u32, u32, C.c_uint64, C.c_uint64, vp, vp]
@@ -152,6 +161,33 @@ class Port:
             t[:, 0:3], t[:, 4:7], t[:, 8:11] = v0, v1 - v0, v2 - v0
             out.append(t)
         return np.ascontiguousarray(np.concatenate(out) if out else np.zeros((0, 12), np.float32))
+
+    def hg_eval(self, g, ct):
+        return np.array([self.L.orc_hg_eval(g, float(c)) for c in np.asarray(ct, np.float32)], np.float32)
+
+    def hg_sample(self, g, iv, u1, u2):
+        iv = np.ascontiguousarray(iv, np.float32).reshape(-1, 3)
+        out = np.zeros_like(iv)
+        for i in range(len(iv)):
+            self.L.orc_hg_sample(g, _p(iv[i]), float(u1[i]), float(u2[i]), _p(out[i]))
+        return out
+
+    def atan2_ref(self, y, x):
+        return np.array([self.L.orc_atan2_ref(float(a), float(b)) for a, b in zip(y, x)], np.float32)
+
+    def env_map_eval(self, P, rd):
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        out = np.zeros_like(rd)
+        for i in range(len(rd)):
+            self.L.orc_env_map_eval(C.byref(P), _p(rd[i]), _p(out[i]))
+        return out
+
+    def sky_light(self, P, rd):
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        out = np.zeros_like(rd)
+        for i in range(len(rd)):
+            self.L.orc_sky_light(C.byref(P), _p(rd[i]), _p(out[i]))
+        return out
 
     def occluded(self, S, ro, rd) -> np.ndarray:
         """Binary32 any-hit answer per ray (the GPU's triangle test, every triangle)."""
@@ -237,10 +273,18 @@ class Port:
             P.depthcomp = 1 if cfg.get("depthcomp") else 0
         P.finite_paths = 1 if cfg.get("finite_paths") else 0
         P.embree = 1 if cfg.get("embree") else 0
+        P.hg_g = float(cfg.get("hg_g", 0.0))
+        P.env_mode = int(cfg.get("env_mode", 0))
+        if P.env_mode == 2:
+            em = np.ascontiguousarray(cfg["env_map"], np.float32)
+            keep.append(em)
+            P.env_map, P.env_h, P.env_w = em.ctypes.data, em.shape[0], em.shape[1]
         if cfg.get("phase_mode", 0) == 1:
             tab = Port().mie_exact_table(pdf)
             keep.append(tab)
             P.phase_mode, P.mie_exact = 1, tab.ctypes.data
+        elif cfg.get("phase_mode", 0) == 2:
+            P.phase_mode = 2
         return P
 
     def mie_exact_table(self, pdf: np.ndarray) -> np.ndarray:
@@ -359,7 +403,43 @@ class Reference:
         L.ref_mie_sample.argtypes = [vp, vp, vp, u32, vp]
         L.ref_sun_ops.argtypes = [vp, vp, f32, vp, vp, vp, u32, vp, vp, vp]
         L.ref_rng_draw.argtypes = [vp, u32, vp]
+        L.ref_hg_eval.argtypes = [f32, vp, u32, vp]
+        L.ref_hg_sample.argtypes = [f32, vp, vp, vp, u32, vp]
+        L.ref_atan2.argtypes = [vp, vp, u32, vp]
+        L.ref_env_eval.argtypes = [u32, u32, vp, vp, u32, vp]
+        L.ref_has_hosek.restype = C.c_int
+        L.ref_render_ex.argtypes = [vp, vp, vp, vp, vp, f32, f64, f64, u32, f32, f32, u32, u32, u32, u32, u32, u32,
+                                    u32, vp, vp, vp, u32, C.c_int, f32, u32, u32, vp]
+        L.ref_render_ex.restype = C.c_int
         self.L = L
+
+    def hg_eval(self, g, ct):
+        ct = np.ascontiguousarray(ct, np.float32)
+        out = np.zeros_like(ct)
+        self.L.ref_hg_eval(g, _p(ct), len(ct), _p(out))
+        return out
+
+    def hg_sample(self, g, iv, u1, u2):
+        iv = np.ascontiguousarray(iv, np.float32).reshape(-1, 3)
+        u1 = np.ascontiguousarray(u1, np.float32)
+        u2 = np.ascontiguousarray(u2, np.float32)
+        out = np.zeros_like(iv)
+        self.L.ref_hg_sample(g, _p(iv), _p(u1), _p(u2), len(iv), _p(out))
+        return out
+
+    def atan2(self, y, x):
+        y = np.ascontiguousarray(y, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros_like(y)
+        self.L.ref_atan2(_p(y), _p(x), len(y), _p(out))
+        return out
+
+    def env_eval(self, env_map, rd):
+        em = np.ascontiguousarray(env_map, np.float32)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        out = np.zeros_like(rd)
+        self.L.ref_env_eval(em.shape[1], em.shape[0], _p(em), _p(rd), len(rd), _p(out))
+        return out
 
     def set_threads(self, n: int):
         self.L.ref_set_threads(int(n))
@@ -456,6 +536,30 @@ class _RefScene:
                                    1 if cfg.get("depthcomp") else 0)
         if rc != 0:
             raise RuntimeError("ref_render failed")
+        return sun, sky
+
+    def render_ex(self, cfg: dict, x0, y0, tw, th, spp):
+        """render() with the phase function (cfg phase_mode 2 = HG, hg_g) and the
+        environment map (cfg env_mode 2, env_map (h, w, 4)) of the configuration."""
+        viewi = np.ascontiguousarray(cfg["viewi"], np.float32)
+        proji = np.ascontiguousarray(cfg["proji"], np.float32)
+        sd = np.ascontiguousarray(cfg["sun_dir"], np.float32)
+        sc = np.ascontiguousarray(cfg["sun_color"], np.float32)
+        sun = np.zeros((th, tw, 4), np.float32)
+        sky = np.zeros((th, tw, 4), np.float32)
+        depth = None if cfg.get("depth") is None else np.ascontiguousarray(cfg["depth"], np.float32).reshape(-1)
+        em = None
+        if cfg.get("env_mode", 0) == 2:
+            em = np.ascontiguousarray(cfg["env_map"], np.float32)
+        rc = self.ref.L.ref_render_ex(self.h, _p(viewi), _p(proji), _p(sd), _p(sc), float(cfg["sun_angle"]),
+                                      float(cfg["turbidity"]), float(cfg["ground_albedo"]), int(cfg["scattevs"]),
+                                      float(cfg["sigma_s"]), float(cfg["sigma_a"]), int(cfg["w"]), int(cfg["h"]),
+                                      x0, y0, tw, th, spp, _p(sun), _p(sky), None if depth is None else _p(depth),
+                                      1 if cfg.get("depthcomp") else 0, 2 if cfg.get("phase_mode", 0) == 2 else 0,
+                                      float(cfg.get("hg_g", 0.0)), 0 if em is None else em.shape[1],
+                                      0 if em is None else em.shape[0], None if em is None else _p(em))
+        if rc != 0:
+            raise RuntimeError("ref_render_ex failed")
         return sun, sky
 
     def shadow(self, cfg: dict, x0, y0, tw, th, spp):

@@ -65,6 +65,10 @@ typedef struct {
     const float *mie_exact;/* exact-mode table (orc_mie_exact_table), 8 n + 4 floats */
     uint32_t finite_paths; /* a path whose sun or sky sum is not finite adds nothing */
     uint32_t embree;       /* the reference built with USE_EMBREE (src/kernel.cpp:149-153, 375-383) */
+    float hg_g;            /* phase_mode 2: HGPhase::g1 */
+    uint32_t env_mode;     /* 0 Hosek sky, 1 NullEnv, 2 MapEnv */
+    const float *env_map;  /* env_mode 2: env_w * env_h RGBA floats, row-major */
+    uint32_t env_w, env_h;
 } orc_params;
 
 typedef struct {
@@ -105,6 +109,18 @@ void orc_mie_exact_table(const float *pdf_rgb, uint32_t n, float *out);
 void orc_mie_exact_dir(const float *tab, uint32_t n, float u1, float *ct, float *st);
 void orc_mie_exact_dirs(const float *tab, uint32_t n, const float *u1, uint32_t count, float *ct, float *st);
 void orc_mie_sample_exact(const orc_params *P, const float iv[3], float u1, float u2, float out[3]);
+/* HGPhase (src/KernelSampler.cpp:164-204) */
+float orc_hg_eval(float g, float ct);
+void orc_hg_sample(float g, const float iv[3], float u1, float u2, float out[3]);
+/* the reference's polynomial atan2 (src/smmath.inl:430-445) */
+float orc_atan2_ref(float y, float x);
+/* MapEnv::Evaluate (src/KernelSampler.cpp:384-417), before the 2.2 power */
+void orc_env_map_eval(const orc_params *P, const float rd[3], float out[3]);
+/* light of an escaping ray: the Hosek sky, or pow(environment, 2.2) (src/kernel.cpp:329-364) */
+void orc_sky_light(const orc_params *P, const float rd[3], float out[3]);
+/* phase function of the path: Mie (either sampler) or HG */
+void orc_phase_eval_rgb(const orc_params *P, float ct, float out[3]);
+void orc_phase_sample(const orc_params *P, const float iv[3], float u1, float u2, float out[3]);
 void orc_sun_eval(const orc_params *P, const float rd[3], float out[3]);
 float orc_sun_pdf(const orc_params *P, const float v[3]);
 void orc_sun_sample(const orc_params *P, float u1, float u2, float out[3]);

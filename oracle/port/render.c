@@ -223,7 +223,7 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
             if (r > 0 && !occ_blocks(S, P, ro, rd)) {
                 float sun[3], sky[3];
                 orc_sun_eval(P, rd, sun);
-                orc_sky_eval(P, rd, sky);
+                orc_sky_light(P, rd, sky);
                 for (int k = 0; k < 3; ++k) {
                     out_sun[k] = out_sun[k] + T[k] * sun[k];
                     out_sky[k] = out_sky[k] + T[k] * sky[k];
@@ -234,13 +234,12 @@ void orc_render_path(const orc_scene *S, const orc_params *P, uint32_t px, uint3
         if (r >= P->scattevs) break;
         float srd[3], lrd[3], p1[3], p3[3], rc[3];
         const float u1 = orc_rng_uniform(&g), u2 = orc_rng_uniform(&g);
-        if (P->phase_mode == 1) orc_mie_sample_exact(P, rd, u1, u2, srd);
-        else orc_mie_sample(P, rd, u1, u2, srd);
+        orc_phase_sample(P, rd, u1, u2, srd);
         const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
         orc_sun_sample(P, u3, u4, lrd);
-        orc_mie_eval_rgb(P, dot3(srd, rd), p1);
+        orc_phase_eval_rgb(P, dot3(srd, rd), p1);
         const float p2 = orc_sun_pdf(P, lrd);
-        orc_mie_eval_rgb(P, dot3(lrd, rd), p3);
+        orc_phase_eval_rgb(P, dot3(lrd, rd), p3);
         const float q1 = orc_sun_pdf(P, srd);
         if (cnt) cnt->mie_evals += 3;
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
@@ -537,7 +536,7 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
             if (r > 0 && !occ_blocks(S, P, ro, rd)) {
                 float sun[3], sky[3];
                 orc_sun_eval(P, rd, sun);
-                orc_sky_eval(P, rd, sky);
+                orc_sky_light(P, rd, sky);
                 const float m = (float)r;
                 for (int k = 0; k < 3; ++k) {
                     const float cs = T[k] * sun[k], ck = T[k] * sky[k];
@@ -552,13 +551,12 @@ static void adjoint_pass(const orc_scene *S, const orc_params *P, uint32_t px, u
         if (r >= P->scattevs) break;
         float srd[3], lrd[3], p1[3], p3[3], rc[3];
         const float u1 = orc_rng_uniform(&g), u2 = orc_rng_uniform(&g);
-        if (P->phase_mode == 1) orc_mie_sample_exact(P, rd, u1, u2, srd);
-        else orc_mie_sample(P, rd, u1, u2, srd);
+        orc_phase_sample(P, rd, u1, u2, srd);
         const float u3 = orc_rng_uniform(&g), u4 = orc_rng_uniform(&g);
         orc_sun_sample(P, u3, u4, lrd);
-        orc_mie_eval_rgb(P, dot3(srd, rd), p1);
+        orc_phase_eval_rgb(P, dot3(srd, rd), p1);
         const float p2 = orc_sun_pdf(P, lrd);
-        orc_mie_eval_rgb(P, dot3(lrd, rd), p3);
+        orc_phase_eval_rgb(P, dot3(lrd, rd), p3);
         const float q1 = orc_sun_pdf(P, srd);
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         const orc_rng g0 = g;

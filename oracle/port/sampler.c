@@ -309,6 +309,90 @@ void orc_sky_eval(const orc_params *P, const float rd[3], float out[3]) {
     }
 }
 
+/* ---- HGPhase, src/KernelSampler.cpp:164-204 ------------------------------------
+ * Evaluate: (1 - g g) / (4 SM_PI pow(1 + g g - 2 g ct, 1.5)), 4 SM_PI rounded to
+ * binary32; Sample: sq = (1 - g g) / (1 - g + 2 g u1), ct = (1 + g g - sq sq) /
+ * (2 g), composed with SamplingBasis like the Mie sampler. */
+float orc_hg_eval(float g, float ct) {
+    float den = 12.566371f * orc_pow((1.0f + g * g) - (2.0f * g) * ct, 1.5f);
+    return (1.0f - g * g) / den;
+}
+
+void orc_hg_sample(float g, const float iv[3], float u1, float u2, float out[3]) {
+    float sq = (1.0f - g * g) / ((1.0f - g) + (2.0f * g) * u1);
+    float ct = ((1.0f + g * g) - sq * sq) / (2.0f * g);
+    float st = sqrtf(sse_max(1.0f - ct * ct, 0.0f));
+    float b1[3], b2[3];
+    sampling_basis(iv, b1, b2);
+    compose_dir(b1, b2, iv, st, ct, (2.0f * ORC_PI) * u2, out);
+}
+
+void orc_phase_eval_rgb(const orc_params *P, float ct, float out[3]) {
+    if (P->phase_mode == 2) {
+        out[0] = out[1] = out[2] = orc_hg_eval(P->hg_g, ct);
+        return;
+    }
+    orc_mie_eval_rgb(P, ct, out);
+}
+
+void orc_phase_sample(const orc_params *P, const float iv[3], float u1, float u2, float out[3]) {
+    if (P->phase_mode == 2) orc_hg_sample(P->hg_g, iv, u1, u2, out);
+    else if (P->phase_mode == 1) orc_mie_sample_exact(P, iv, u1, u2, out);
+    else orc_mie_sample(P, iv, u1, u2, out);
+}
+
+/* atan2 of smmath.inl: a = min/max of |x|, |y|, the odd polynomial, then the
+ * octant corrections (0.5 SM_PI and SM_PI rounded to binary32). */
+float orc_atan2_ref(float y, float x) {
+    float X = sse_max(0.0f - x, x), Y = sse_max(0.0f - y, y);
+    float a = sse_min(X, Y) / sse_max(X, Y);
+    float b = a * a;
+    float p = -0.013480470f * b + 0.057477314f;
+    p = p * b - 0.121239071f;
+    p = p * b + 0.195635925f;
+    p = p * b - 0.332994597f;
+    p = p * b + 0.999995630f;
+    a = a * p;
+    if (Y > X) a = 1.57079637f - a;
+    if (x < 0.0f) a = ORC_PI - a;
+    if (y < 0.0f) a = 0.0f - a;
+    return a;
+}
+
+/* MapEnv::Evaluate: theta row from acos(-rd.z) / pi, phi column from
+ * 0.5 + atan2(rd.y, -rd.x) / (2 pi); saturate = max(min(x, 1), 0) (NaN -> 1);
+ * texel indices formed in binary32 (w * row + column). */
+void orc_env_map_eval(const orc_params *P, const float rd[3], float out[3]) {
+    const float fw = (float)P->env_w, fh = (float)P->env_h;
+    float tha = orc_acos_ref(0.0f - rd[2]) / ORC_PI;
+    float thb = fh * sse_max(sse_min(tha, 1.0f), 0.0f);
+    float thc = floorf(thb);
+    thc = sse_min(thc, (float)(P->env_h - 2));
+    thc = sse_max(thc, 0.0f);
+    float tht = thb - thc;
+    float pha = 0.5f + orc_atan2_ref(rd[1], 0.0f - rd[0]) / 6.2831855f;
+    float phb = fw * sse_max(sse_min(pha, 1.0f), 0.0f);
+    float phc = floorf(phb);
+    phc = sse_min(phc, (float)(P->env_w - 2));
+    phc = sse_max(phc, 0.0f);
+    float pht = phb - phc;
+    const float *T = P->env_map;
+    const float *ca = T + 4 * (size_t)(uint32_t)(fw * thc + phc), *cb = T + 4 * (size_t)(uint32_t)(fw * (thc + 1.0f) + phc);
+    const float *da = T + 4 * (size_t)(uint32_t)(fw * thc + phc + 1.0f),
+                *db = T + 4 * (size_t)(uint32_t)(fw * (thc + 1.0f) + phc + 1.0f);
+    for (int i = 0; i < 3; ++i) out[i] = lerp_ref(lerp_ref(ca[i], cb[i], tht), lerp_ref(da[i], db[i], tht), pht);
+}
+
+void orc_sky_light(const orc_params *P, const float rd[3], float out[3]) {
+    if (P->env_mode == 0) {
+        orc_sky_eval(P, rd, out);
+        return;
+    }
+    float e[3] = {0.0f, 0.0f, 0.0f};
+    if (P->env_mode == 2) orc_env_map_eval(P, rd, e);
+    for (int i = 0; i < 3; ++i) out[i] = orc_pow(e[i], 2.2f);
+}
+
 /* K_ParallelRender ray generation for pixel (px, py), src/kernel.cpp:461-474 */
 void orc_camera_ray(const orc_params *P, uint32_t px, uint32_t py, float ro[3], float rd[3], int *in_frame) {
     float hx = 0.0f - (((2.0f * ((float)px + 0.5f)) / (float)P->w) - 1.0f);

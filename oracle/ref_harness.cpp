@@ -127,11 +127,18 @@ extern "C" float ref_solar_elevation(const float sun_dir[3]) {
  * (7, 0.15) of src/kernel.cpp:525.  Outputs are the two tile buffers phb[0]
  * (sun) and phb[1] (sky) as float4 per pixel, row-major in the tile; pixels the
  * reference leaves unwritten (outside the frame, odd last row/column) are 0. */
+struct PhaseEnv {
+    int phase;               /* 0 MiePhase, 2 HGPhase */
+    float g;                 /* HGPhase::g1 */
+    unsigned env_w, env_h;   /* MapEnv texels (0: NullEnv) */
+    const float *env_rgba;
+};
+
 static int ref_run(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
                    const float sun_color[3], float sun_angle, double turbidity, double albedo, unsigned scattevs,
                    float sigma_s, float sigma_a, unsigned w, unsigned h, unsigned x0, unsigned y0, unsigned tw,
                    unsigned th, unsigned spp, const float *depth, unsigned flags, int shadow, float *out_sun,
-                   float *out_sky) {
+                   float *out_sky, const PhaseEnv &pe = PhaseEnv{0, 0.0f, 0, 0, 0}) {
     Scene *s = (Scene *)p;
     KernelSampler::BaseLight::DeleteAll();
     dfloat3 D(sun_dir[0], sun_dir[1], sun_dir[2]);
@@ -145,13 +152,27 @@ static int ref_run(void *p, const float viewi[16], const float proji[16], const 
     }
     std::vector<float> dcopy;
     if (depth) dcopy.assign(depth, depth + (size_t)w * h);
+    /* phase function and environment as DRE_BeginRender selects them (src/main.cpp:522-587) */
+    KernelSampler::PhaseFunction *ppf = &KernelSampler::MiePhase::gmie;
+    if (pe.phase == 2) {
+        KernelSampler::HGPhase::ghg.g1 = pe.g;
+        ppf = &KernelSampler::HGPhase::ghg;
+    }
+    KernelSampler::BaseEnv *penv = &KernelSampler::NullEnv::nenv;
+    if (pe.env_w) {
+        dfloat4 *t = KernelSampler::MapEnv::genv.Initialize(pe.env_w, pe.env_h);
+        std::memcpy((void *)t, pe.env_rgba, (size_t)pe.env_w * pe.env_h * 16);
+        penv = &KernelSampler::MapEnv::genv;
+    }
     RenderKernel k;
-    if (!k.Initialize(s, 0, &vi, &pi, &KernelSampler::MiePhase::gmie, &KernelSampler::NullEnv::nenv,
-                      depth ? dcopy.data() : 0, scattevs, sigma_s, sigma_a, tw, th, w, h, flags))
+    if (!k.Initialize(s, 0, &vi, &pi, ppf, penv, depth ? dcopy.data() : 0, scattevs, sigma_s, sigma_a, tw, th, w, h,
+                      flags))
         return -1;
+#ifdef USE_ARHOSEK_SKYMODEL
     arhosekskymodelstate_free(k.pskyms);
     float se = ref_solar_elevation(sun_dir);
     k.pskyms = arhosek_rgb_skymodelstate_alloc_init(turbidity, albedo, se);
+#endif
     std::memset(k.phb[0], 0, (size_t)tw * th * 16);
     std::memset(k.phb[1], 0, (size_t)tw * th * 16);
     if (shadow)
@@ -161,6 +182,7 @@ static int ref_run(void *p, const float viewi[16], const float proji[16], const 
     std::memcpy(out_sun, k.phb[0], (size_t)tw * th * 16);
     if (out_sky) std::memcpy(out_sky, k.phb[1], (size_t)tw * th * 16);
     k.Destroy();
+    if (pe.env_w) KernelSampler::MapEnv::genv.Destroy();  // as DRE_EndRender does (src/main.cpp:691-693)
     KernelSampler::BaseLight::DeleteAll();
     return 0;
 }
@@ -174,6 +196,30 @@ extern "C" int ref_render(void *p, const float viewi[16], const float proji[16],
                           const float *depth, unsigned flags) {
     return ref_run(p, viewi, proji, sun_dir, sun_color, sun_angle, turbidity, albedo, scattevs, sigma_s, sigma_a, w,
                    h, x0, y0, tw, th, spp, depth, flags, 0, out_sun, out_sky);
+}
+
+/* ref_render with the phase function (0 Mie, 2 HG with anisotropy g) and the
+ * environment (env_w == 0: NullEnv, else a MapEnv of env_w x env_h RGBA
+ * texels) chosen as DRE_BeginRender does; the environment is read only by the
+ * build without USE_ARHOSEK_SKYMODEL. */
+extern "C" int ref_render_ex(void *p, const float viewi[16], const float proji[16], const float sun_dir[3],
+                             const float sun_color[3], float sun_angle, double turbidity, double albedo,
+                             unsigned scattevs, float sigma_s, float sigma_a, unsigned w, unsigned h, unsigned x0,
+                             unsigned y0, unsigned tw, unsigned th, unsigned spp, float *out_sun, float *out_sky,
+                             const float *depth, unsigned flags, int phase, float g, unsigned env_w, unsigned env_h,
+                             const float *env_rgba) {
+    const PhaseEnv pe{phase, g, env_w, env_h, env_rgba};
+    return ref_run(p, viewi, proji, sun_dir, sun_color, sun_angle, turbidity, albedo, scattevs, sigma_s, sigma_a, w,
+                   h, x0, y0, tw, th, spp, depth, flags, 0, out_sun, out_sky, pe);
+}
+
+/* Whether this library is the reference built with USE_ARHOSEK_SKYMODEL. */
+extern "C" int ref_has_hosek(void) {
+#ifdef USE_ARHOSEK_SKYMODEL
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 /* RenderKernel::Shadow over one tile (src/kernel.cpp:569-607): phb[0] only. */

@@ -81,7 +81,8 @@ def settings_from_cfg(cfg: dict):
         h=cfg["h"], depth=cfg.get("depth"), depthcomp=bool(cfg.get("depthcomp", False)),
         finite_paths=bool(cfg.get("finite_paths", False)),
         embree=bool(cfg.get("embree", False)),
-        phase_mode=int(cfg.get("phase_mode", 0)))
+        phase_mode=int(cfg.get("phase_mode", 0)), hg_g=float(cfg.get("hg_g", 0.0)),
+        env_mode=int(cfg.get("env_mode", 0)), env_map=cfg.get("env_map"))
 
 
 def depth_texture(w: int, h: int) -> np.ndarray:

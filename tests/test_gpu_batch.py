@@ -42,13 +42,19 @@ def batch_setup():
     rec = W.config0_recipe(48, 12)
     org, vals = W.sparse_field(rec)
     oc1 = build_octree(org, vals, rec.voxel_size, 12)
+    from test_phase_env import env_map
+
     c3 = view_cfg(64, 64, 200.0, 60, 30.0, 12)
     c3["depth"] = depth_texture(64, 64)
     c3["depthcomp"] = True
+    c1 = view_cfg(96, 80, 35.0, 45, 45.0, 16)
+    c1["env_mode"] = 1  # NullEnv
+    c2 = view_cfg(40, 40, 120.0, 12, 70.0, 500)
+    c2.update(phase_mode=2, hg_g=0.6, env_mode=2, env_map=env_map())  # HG phase, MapEnv
     specs = [  # (scene, cfg, region, spp, seed)
         (0, view_cfg(64, 64, -90.0, 30, 20.0, 8), None, 24, 3),
-        (1, view_cfg(96, 80, 35.0, 45, 45.0, 16), (8, 4, 72, 60), 16, 4),
-        (0, view_cfg(40, 40, 120.0, 12, 70.0, 500), None, 40, 5),
+        (1, c1, (8, 4, 72, 60), 16, 4),
+        (0, c2, None, 40, 5),
         (1, c3, (2, 2, 61, 59), 8, 6),
     ]
     r = Renderer(0)

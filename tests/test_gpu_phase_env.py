@@ -1,0 +1,121 @@
+"""The HG phase and the environment light (NullEnv / MapEnv) on the GPU against
+the CPU restatement: samplers and lookups bit-exact, path samples bit-exact,
+tiles of every kernel and the adjoint equal (the restatement is pinned to the
+compiled reference in test_phase_env)."""
+import numpy as np
+import pytest
+
+from conftest import c0_cfg, golden_octree, settings_from_cfg
+from droplet_b200 import _native as N
+from test_phase_env import _dirs, env_map
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def renderer():
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree
+
+    nodes, bricks, mlevel = golden_octree()
+    r = Renderer(0)
+    r.upload(Octree(nodes, bricks, mlevel))
+    yield r
+    r.close()
+
+
+def _cfg(phase, env):
+    cfg = c0_cfg(64, 64)
+    if phase == "hg":
+        cfg["phase_mode"], cfg["hg_g"] = 2, 0.75
+    cfg["env_mode"] = {"hosek": 0, "none": 1, "map": 2}[env]
+    if env == "map":
+        cfg["env_map"] = env_map()
+    return cfg
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def test_samplers_and_lookups_bit_exact(renderer, port):
+    cfg = _cfg("hg", "map")
+    renderer.set_params(settings_from_cfg(cfg))
+    keep = []
+    P = port.params(cfg, keep)
+    rng = np.random.default_rng(8)
+    ct = rng.uniform(-1, 1, 4000).astype(np.float32)
+    assert np.array_equal(bits(renderer.probe_sampler(N.DR_PROBE_HG_EVAL, ct, len(ct))), bits(port.hg_eval(0.75, ct)))
+    iv = _dirs(3000, 9)[:3000]
+    u1, u2 = rng.random(3000).astype(np.float32), rng.random(3000).astype(np.float32)
+    got = renderer.probe_sampler(N.DR_PROBE_HG_SAMPLE, np.concatenate([iv.reshape(-1), u1, u2]), 3000)
+    assert np.array_equal(bits(got), bits(port.hg_sample(0.75, iv, u1, u2)))
+    rd = _dirs(5000, 10)
+    assert np.array_equal(bits(renderer.probe_sampler(N.DR_PROBE_ENV_MAP, rd, len(rd))), bits(port.env_map_eval(P, rd)))
+    assert np.array_equal(bits(renderer.probe_sampler(N.DR_PROBE_SKY_LIGHT, rd, len(rd))), bits(port.sky_light(P, rd)))
+
+
+@pytest.mark.parametrize("phase,env", [("hg", "hosek"), ("mie", "map"), ("hg", "none")])
+def test_path_samples_bit_exact(renderer, port, phase, env):
+    nodes, bricks, _ = golden_octree()
+    cfg = _cfg(phase, env)
+    renderer.set_params(settings_from_cfg(cfg))
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    rng = np.random.default_rng(14)
+    n = 2000
+    px = rng.integers(16, 48, n).astype(np.uint32)
+    py = rng.integers(20, 44, n).astype(np.uint32)
+    sm = rng.integers(0, 1 << 40, n).astype(np.uint64)
+    a, b = renderer.probe_paths(px, py, sm, seed=79)
+    for i in range(n):
+        pa, pb, _ = port.render_path(S, P, int(px[i]), int(py[i]), 79, int(sm[i]))
+        assert np.array_equal(bits(a[i]), bits(pa)), (i, a[i], pa)
+        assert np.array_equal(bits(b[i]), bits(pb)), (i, b[i], pb)
+
+
+@pytest.mark.parametrize("tuning", [(0, 0, 0, 0, 0, 0, 0), (1, 0, 0, 0, 0, 0, 0), (0, 8, 24, 1, 8, 4, 4)])
+def test_tiles_equal_restatement(renderer, port, tuning):
+    nodes, bricks, _ = golden_octree()
+    cfg = _cfg("hg", "map")
+    renderer.set_params(settings_from_cfg(cfg))
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    saved = renderer.get_tuning()
+    try:
+        renderer.set_tuning(*tuning)
+        sun, sky = renderer.render_tile(8, 10, 48, 44, 32, seed=5, sample_base=0)
+    finally:
+        renderer.set_tuning(*saved)
+    psun, psky, _ = port.render_tile(S, P, 8, 10, 48, 44, 32, seed=5, sample_base=0)
+    for g, p in ((sun, psun), (sky, psky)):
+        assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), tuning
+    assert sky[..., :3].sum() > 0
+
+
+def test_adjoint_equals_restatement(renderer, port):
+    import torch
+
+    nodes, bricks, _ = golden_octree()
+    cfg = _cfg("hg", "map")
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    rng = np.random.default_rng(10)
+    dsun = rng.normal(size=(40, 48, 4)).astype(np.float32)
+    dsky = rng.normal(size=(40, 48, 4)).astype(np.float32)
+    g_cpu, a_cpu = port.adjoint_tile(S, P, 8, 12, 48, 40, 16, 21, 3, dsun, dsky)
+    renderer.set_params(settings_from_cfg(cfg))
+    ds = torch.as_tensor(dsun, device="cuda").contiguous()
+    dk = torch.as_tensor(dsky, device="cuda").contiguous()
+    g = torch.zeros((len(bricks), 512), dtype=torch.float32, device="cuda")
+    ga = torch.zeros(1, dtype=torch.float64, device="cuda")
+    renderer.adjoint_tile_async(8, 12, 48, 40, 16, 21, 3, ds.data_ptr(), dk.data_ptr(), g.data_ptr(), ga.data_ptr())
+    torch.cuda.synchronize()
+    g_gpu = g.cpu().numpy().astype(np.float64)
+    scale = np.abs(g_cpu).max()
+    assert scale > 0
+    assert np.allclose(g_gpu, g_cpu, rtol=1e-3, atol=1e-4 * scale)
+    assert abs(float(ga.item()) - a_cpu) <= 1e-4 * abs(a_cpu) + 1e-6
