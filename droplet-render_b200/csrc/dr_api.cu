@@ -147,8 +147,8 @@ int dr_upload_scene(dr_ctx *c, const dr_scene_desc *s) {
         c->scene.occ_n_nodes = c->occ_n_nodes;
     }
     std::vector<uint32_t> ln;
-    for (uint32_t i = 0; i < h.n_nodes; ++i)
-        if (h.leaf_flag[i]) ln.push_back(i);
+    for (uint32_t i = 0; i < h.n_nodes; ++i)  // leaves whose majorant comes from their fog brick
+        if ((h.leaf_flag[i] & 2u) && !(h.leaf_flag[i] & 4u)) ln.push_back(i);
     DR_CUDA(c->leaf_nodes.reserve(ln.size()), "dr_upload_scene: alloc leaf list");
     if (!ln.empty())
         DR_CUDA(cudaMemcpy(c->leaf_nodes.p, ln.data(), ln.size() * 4, cudaMemcpyHostToDevice),
@@ -495,8 +495,8 @@ int dr_probe_density(dr_ctx *c, const uint32_t *nodes, const float *points, uint
     if (!c || !nodes || !points || !out || n == 0) return need(false, DR_ERR_INVALID, "dr_probe_density: bad argument");
     if (!c->has_scene) return need(false, DR_ERR_STATE, "dr_probe_density: no scene");
     for (uint32_t i = 0; i < n; ++i)
-        if (nodes[i] >= c->leaf_flag.size() || !c->leaf_flag[nodes[i]])
-            return need(false, DR_ERR_INVALID, "dr_probe_density: node is not a leaf of the scene");
+        if (nodes[i] >= c->leaf_flag.size() || !(c->leaf_flag[nodes[i]] & 2u))
+            return need(false, DR_ERR_INVALID, "dr_probe_density: node is not a leaf with a fog brick");
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
     Scratch S;

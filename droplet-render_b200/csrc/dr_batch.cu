@@ -36,6 +36,7 @@ struct dr_batch {
     DevParams p0{};
     Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};
     uint64_t n_paths = 0, launches = 0;
+    bool any_sdf = false;  // a scene with surface (SDF) leaves
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -79,7 +80,7 @@ int build_graph(dr_batch *b) {
     B.step = b->step.p;
     DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");
     cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
-    bool ext = false;  // a view with the HG phase or an environment other than the Hosek sky
+    bool ext = b->any_sdf;  // surface leaves, or a view with the HG phase or a non-Hosek environment
     for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
     if (e == cudaSuccess)
         e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
@@ -161,6 +162,7 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
     for (uint32_t i = 0; i < n_scenes; ++i) {
         b->scene_bufs.emplace_back(new SceneBufs());
         rc = upload_scene(hs[i], *b->scene_bufs.back(), c->use_grid, b->stream, ds[i]);
+        b->any_sdf = b->any_sdf || ds[i].sdf_bricks != nullptr;
         if (rc != DR_OK) return fail(rc);
     }
     size_t total = 0;

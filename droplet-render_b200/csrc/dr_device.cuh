@@ -850,7 +850,8 @@ __device__ __forceinline__ float3 sky_light(const DevParams &P, const float rd[3
 enum : uint32_t {
     kFeatOcc = 1,  // occluders present and the USE_EMBREE build's masks apply
     kFeatExt = 2,  // HG phase or an environment other than the Hosek sky
-    kFeatAll = 3,
+    kFeatSdf = 4,  // surface (SDF) leaves in the scene
+    kFeatAll = 7,
 };
 
 // Escape light of a segment: the Hosek sky, or (kFeatExt) whichever
@@ -998,18 +999,21 @@ struct NoVisit {
     __device__ __forceinline__ void operator()(const float *, const float4 &, const float *, float, float, bool) const {}
 };
 
-template <class Visit>
+// SDF: the scene may hold surface leaves (src/kernel.cpp:241-305); without it
+// every leaf is a fog leaf and the surface tests are not compiled in.
+template <class Visit, bool SDF = true>
 __device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
                                             Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
                                             const Visit &visit);
 
+template <bool SDF = true>
 __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
                                           Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
     const NoVisit nv;
-    return track_v(S, P.sigma_e, ro, rd, g, depth, td_out, nstack, cnt, nv);
+    return track_v<NoVisit, SDF>(S, P.sigma_e, ro, rd, g, depth, td_out, nstack, cnt, nv);
 }
 
-template <class Visit>
+template <class Visit, bool SDF>
 __device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
                                             Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
                                             const Visit &visit) {
@@ -1026,15 +1030,37 @@ __device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, co
         const float4 ce = __ldg(&S.leaf[2 * leaf]);
         const float4 meta = __ldg(&S.leaf[2 * leaf + 1]);
         const float smax = meta.x;
-        const float *brick = S.bricks + (size_t)__float_as_uint(meta.y) * kBrick;
+        const uint32_t fogx = __float_as_uint(meta.y);
+        const float *brick = S.bricks + (size_t)fogx * kBrick;
+        const float *sbrick = nullptr;  // surface brick of an SDF leaf
+        if constexpr (SDF) {
+            const uint32_t sdfx = __float_as_uint(meta.z);
+            if (sdfx != kNone) sbrick = S.sdf_bricks + (size_t)sdfx * kBrick;
+        }
         const float lo = td;
         const float tr0 = tra - td, tr1 = trb - td;
-        // src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
-        // fog leaves, so the masked selects are bitwise blends: past the leaf
-        // entry, td keeps all but its lowest bit and s0 becomes the lowest bit
-        // of tr0 (0 or the smallest denormal).
         float s0;
-        if (tra > td) {
+        if (SDF && sbrick) {
+            // src/kernel.cpp:253-263: an SDF leaf is entered (td = tra, s0 = tr0)
+            // only when the ray is before it and the distance there is positive;
+            // otherwise tracking starts from td with s0 = 0
+            bool skip = false;
+            if (tra > td) {
+                const float r0[3] = {ro[0] + rd[0] * tra, ro[1] + rd[1] * tra, ro[2] + rd[2] * tra};
+                skip = sample_voxel_space(r0, sbrick, ce) > 0.0f;
+                ++cnt.density_lookups;
+            }
+            if (skip) {
+                td = tra;
+                s0 = tr0;
+            } else {
+                s0 = 0.0f;
+            }
+        } else if (tra > td) {
+            // src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
+            // fog leaves, so the masked selects are bitwise blends: past the leaf
+            // entry, td keeps all but its lowest bit and s0 becomes the lowest bit
+            // of tr0 (0 or the smallest denormal).
             td = tra;
             s0 = tr0;
         } else {
@@ -1051,16 +1077,28 @@ __device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, co
                 break;
             }
             bool rm = sc > tr0;
-            float rho = -1.0f;
+            float rho = -1.0f, dist = 1.0f;
+            bool fog_decides = rm;  // the decision depends on the fog density (what the visitor differentiates)
             if (rm) {
                 const float rc[3] = {ro[0] + rd[0] * td, ro[1] + rd[1] * td, ro[2] + rd[2] * td};
-                rho = sample_voxel_space(rc, brick, ce);
-                ++cnt.density_lookups;
+                if (SDF && sbrick) {
+                    // src/kernel.cpp:287-300: inside the surface (dist <= 0) always
+                    // collides; outside, the fog brick (if any) decides
+                    dist = sample_voxel_space(rc, sbrick, ce);
+                    ++cnt.density_lookups;
+                    fog_decides = dist > 0.0f && fogx != kNone;
+                    if (fog_decides) {
+                        rho = sample_voxel_space(rc, brick, ce);
+                        ++cnt.density_lookups;
+                    }
+                } else {
+                    rho = sample_voxel_space(rc, brick, ce);
+                    ++cnt.density_lookups;
+                }
             }
             const float q = g.uniform();
-            const bool looked = rm;
-            rm = rm && (rho / smax < q);
-            if (looked) {
+            rm = rm && (rho / smax < q) && (dist > 0.0f);
+            if (fog_decides) {
                 const float rc[3] = {ro[0] + rd[0] * td, ro[1] + rd[1] * td, ro[2] + rd[2] * td};
                 visit(brick, ce, rc, rho, smax, !rm);
             }
@@ -1116,7 +1154,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
     const float depth0 = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)py * P.w + px]) : 3.402823466e+38f;
     for (uint32_t r = 0;; ++r) {
         float td;
-        const uint32_t res = track(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+        const uint32_t res = track<(FEAT & kFeatSdf) != 0>(S, P, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
         if (r == 0) sun_acc.w = sky_acc.w = first_alpha(P, res);
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
@@ -1151,7 +1189,7 @@ __device__ __forceinline__ void path_sample(const DevScene &S, const DevParams &
 #pragma unroll
         for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
         float tds;
-        if (track(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped &&
+        if (track<(FEAT & kFeatSdf) != 0>(S, P, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt) == kTrackEscaped &&
             !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd))) {
             const bool hit = sun_hit(P, lrd);
             const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,

@@ -84,19 +84,21 @@ int prepare_scene(const dr_scene_desc *s, HostScene &out) {
     leaf.assign((size_t)s->n_nodes * 2, make_float4(0.f, 0.f, 0.f, 0.f));
     for (uint32_t i = 0; i < s->n_nodes; ++i) {
         const dr_node &o = N[i];
-        if (o.volx[0] != DR_NONE)
-            return need(false, DR_ERR_INVALID, "dr_upload_scene: surface (SDF) leaves are not supported");
         if (is_leaf(i)) {
-            if (o.volx[1] >= s->n_leaves)
+            const bool sdf = o.volx[0] != DR_NONE, fog = o.volx[1] != DR_NONE;
+            if (sdf && (!s->sdf_bricks || o.volx[0] >= s->n_sdf_leaves))
+                return need(false, DR_ERR_INVALID, "dr_upload_scene: SDF brick index out of range (or no SDF pool)");
+            if (fog && o.volx[1] >= s->n_leaves)
                 return need(false, DR_ERR_INVALID, "dr_upload_scene: brick index out of range");
-            if (!(o.ce[3] > 0.0f) || !std::isfinite(o.ce[3]) || !(o.qval[1] >= 0.0f) || !std::isfinite(o.qval[1]))
+            if (!(o.ce[3] > 0.0f) || !std::isfinite(o.ce[3]) ||
+                (!sdf && (!(o.qval[1] >= 0.0f) || !std::isfinite(o.qval[1]))))
                 return need(false, DR_ERR_INVALID, "dr_upload_scene: leaf with bad extent or majorant");
-            uint32_t bits;
-            std::memcpy(&bits, &o.volx[1], 4);
-            float fb;
-            std::memcpy(&fb, &bits, 4);
+            float fb, sb;
+            std::memcpy(&fb, &o.volx[1], 4);  // index bits (kNone when absent)
+            std::memcpy(&sb, &o.volx[0], 4);
             leaf[2 * (size_t)i] = make_float4(o.ce[0], o.ce[1], o.ce[2], o.ce[3]);
-            leaf[2 * (size_t)i + 1] = make_float4(o.qval[1], fb, 0.0f, 0.0f);
+            // src/kernel.cpp:245-251: an SDF leaf's majorant is 1, a fog leaf's qval[FOG]
+            leaf[2 * (size_t)i + 1] = make_float4(sdf ? 1.0f : o.qval[1], fb, sb, 0.0f);
         } else {
             leaf[2 * (size_t)i] = make_float4(o.ce[0], o.ce[1], o.ce[2], o.ce[3]);
             leaf[2 * (size_t)i + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -168,6 +170,10 @@ int prepare_scene(const dr_scene_desc *s, HostScene &out) {
     out.leaf_flag.assign(s->n_nodes, 0);
     for (uint32_t i = 0; i < s->n_nodes; ++i) out.leaf_flag[i] = is_leaf(i) ? 1 : 0;
     out.bricks = s->bricks;
+    out.sdf = s->sdf_bricks;
+    out.n_sdf = s->sdf_bricks ? s->n_sdf_leaves : 0u;
+    for (uint32_t i = 0; i < s->n_nodes; ++i)
+        if (is_leaf(i)) out.leaf_flag[i] = (uint8_t)(1u | (N[i].volx[1] != DR_NONE ? 2u : 0u) | (N[i].volx[0] != DR_NONE ? 4u : 0u));
     return DR_OK;
 }
 
@@ -190,10 +196,16 @@ int upload_scene(const HostScene &h, SceneBufs &b, bool use_grid, cudaStream_t s
     if (nb)
         DR_CUDA(cudaMemcpyAsync(b.bricks.p, h.bricks, nb * 4, cudaMemcpyHostToDevice, st),
                 "dr_upload_scene: copy bricks");
+    const size_t ns = (size_t)h.n_sdf * kBrick;
+    if (ns) {
+        DR_CUDA(b.sdf.reserve(ns), "dr_upload_scene: alloc SDF bricks");
+        DR_CUDA(cudaMemcpyAsync(b.sdf.p, h.sdf, ns * 4, cudaMemcpyHostToDevice, st), "dr_upload_scene: copy SDF bricks");
+    }
     DR_CUDA(cudaStreamSynchronize(st), "dr_upload_scene: sync");
     S.child = b.child.p;
     S.leaf = b.leaf.p;
     S.bricks = b.bricks.p;
+    S.sdf_bricks = ns ? b.sdf.p : nullptr;
     for (int k = 0; k < 4; ++k) S.root_ce[k] = h.root_ce[k];
     S.n_nodes = h.n_nodes;
     S.n_leaves = h.n_leaves;

@@ -65,6 +65,8 @@ struct HostScene {
     uint32_t n_nodes = 0, n_leaves = 0;
     float root_ce[4] = {0, 0, 0, 0};
     const float *bricks = nullptr;  // the caller's brick pool (n_leaves * 512 floats)
+    const float *sdf = nullptr;     // the caller's SDF pool (n_sdf * 512 floats) or null
+    uint32_t n_sdf = 0;
 };
 
 // Device buffers of one uploaded scene.
@@ -72,11 +74,13 @@ struct SceneBufs {
     DevBuf<uint4> child;
     DevBuf<float4> leaf;
     DevBuf<float> bricks;
+    DevBuf<float> sdf;
     DevBuf<uint32_t> macro, cells;
     void release() {
         child.release();
         leaf.release();
         bricks.release();
+        sdf.release();
         macro.release();
         cells.release();
     }

@@ -24,11 +24,13 @@ constexpr uint32_t kStepBudget = 1u << 24;  // tracking steps per segment before
 //   child[2*id], child[2*id+1]: the eight child entries of node id, remapped:
 //       0 = no child, kLeafBit|c = leaf node c, c = internal node c
 //   leaf[2*id]   = (center.xyz, half extent)
-//   leaf[2*id+1] = (majorant, brick index bits, 0, 0)
+//   leaf[2*id+1] = (majorant, FOG brick index bits, SDF brick index bits, 0);
+//                  an index kNone = no such brick; SDF leaves have majorant 1
 struct DevScene {
     const uint4 *child;
     const float4 *leaf;
     const float *bricks;
+    const float *sdf_bricks;   // SDF pool, or null when no leaf has a surface brick
     float root_ce[4];
     uint32_t n_nodes;
     uint32_t n_leaves;

@@ -212,6 +212,7 @@ struct PathLane {
     float lo, tr0, tr1, trb, s0, sr, smax, denom;
     float4 ce;
     const float *brick;
+    const float *sdf;  // surface brick of an SDF leaf (kFeatSdf instantiations), else null
 };
 
 // Stack traversal for the rare segments the cell walk does not take (a zero
@@ -275,7 +276,7 @@ __device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &
 // One traversal step.  Returns 0 after moving to another cell (call again), 1
 // when a leaf was entered and its free flight prepared, 2 when the segment has
 // no further leaf (or the depth mask stops it): the segment escaped.
-template <bool WALK>
+template <bool WALK, uint32_t FEAT>
 __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
                                               uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits,
                                               float (*tstack)[6]) {
@@ -309,7 +310,28 @@ __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene 
     L.tr0 = tra - L.td;
     L.tr1 = trb - L.td;
     L.trb = trb;
-    if (tra > L.td) {
+    bool sdf_leaf = false;
+    if constexpr ((FEAT & kFeatSdf) != 0) {
+        const uint32_t sdfx = __float_as_uint(meta.z);
+        sdf_leaf = sdfx != kNone;
+        L.sdf = sdf_leaf ? S.sdf_bricks + (size_t)sdfx * kBrick : nullptr;
+        if (__float_as_uint(meta.y) == kNone) L.brick = nullptr;  // a surface leaf without fog
+    }
+    if (sdf_leaf) {
+        // src/kernel.cpp:253-263: entered only when before it and outside the surface there
+        bool skip = false;
+        if (tra > L.td) {
+            const float r0[3] = {L.ro[0] + L.rd[0] * tra, L.ro[1] + L.rd[1] * tra, L.ro[2] + L.rd[2] * tra};
+            skip = sample_voxel_space(r0, L.sdf, L.ce) > 0.0f;
+            ++cnt.density_lookups;
+        }
+        if (skip) {
+            L.td = tra;
+            L.s0 = L.tr0;
+        } else {
+            L.s0 = 0.0f;
+        }
+    } else if (tra > L.td) {
         L.td = tra;
         L.s0 = L.tr0;
     } else {
@@ -323,7 +345,7 @@ __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene 
 
 // One delta-tracking step.  Returns 0 = continue in this leaf, 1 = leaf left,
 // 2 = segment ended (collision, or the step budget ran out).
-template <bool WALK>
+template <bool WALK, uint32_t FEAT>
 __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
     const float sc = L.s0 + L.sr;
     L.td = L.lo + sc;
@@ -332,14 +354,24 @@ __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
         return 1;
     }
     bool rm = sc > L.tr0;
-    float rho = -1.0f;
+    float rho = -1.0f, dist = 1.0f;
     if (rm) {
         const float rc[3] = {L.ro[0] + L.rd[0] * L.td, L.ro[1] + L.rd[1] * L.td, L.ro[2] + L.rd[2] * L.td};
-        rho = sample_voxel_space(rc, L.brick, L.ce);
-        ++cnt.density_lookups;
+        if ((FEAT & kFeatSdf) && L.sdf) {
+            // src/kernel.cpp:287-300: inside the surface always collides
+            dist = sample_voxel_space(rc, L.sdf, L.ce);
+            ++cnt.density_lookups;
+            if (dist > 0.0f && L.brick) {
+                rho = sample_voxel_space(rc, L.brick, L.ce);
+                ++cnt.density_lookups;
+            }
+        } else {
+            rho = sample_voxel_space(rc, L.brick, L.ce);
+            ++cnt.density_lookups;
+        }
     }
     const float q = L.g.uniform();
-    rm = rm && (rho / L.smax < q);
+    rm = rm && (rho / L.smax < q) && (dist > 0.0f);
     if (!rm) {
         L.esc = L.td < L.depth ? kTrackCollided : kTrackCut;
         return 2;
@@ -479,7 +511,7 @@ __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const 
         return;
     }
     if (state == kTrav) {
-        const uint32_t r = trav_step(L, S, P, nstack, slow, cnt, visits, tstack);
+        const uint32_t r = trav_step<WALK, FEAT>(L, S, P, nstack, slow, cnt, visits, tstack);
         if (r == 1u) {
             state = kStep;
         } else if (r == 2u) {
@@ -489,7 +521,7 @@ __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const 
     }
     // up to `steps` free-flight steps while the lane stays in its leaf
     for (uint32_t k = 0; k < steps && state == kStep; ++k) {
-        const uint32_t rs = track_step(L, cnt);
+        const uint32_t rs = track_step<WALK, FEAT>(L, cnt);
         if (rs == 1) state = kTrav;
         else if (rs == 2) state = kEvent;
     }
@@ -798,16 +830,18 @@ struct ScatterVisit {
 
 // One copy of the tracking loop per visitor for the whole adjoint (each call
 // site inlining it would multiply the code the warps fetch).
+template <bool SDF>
 __device__ __noinline__ uint32_t track_plain(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
                                              float depth, float &td, uint32_t *nstack, Count &cnt) {
     const NoVisit nv;
-    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, nv);
+    return track_v<NoVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, nv);
 }
 
+template <bool SDF>
 __device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, const float *ro, const float *rd,
                                                Rng &g, float depth, float &td, uint32_t *nstack, Count &cnt,
                                                const ScatterVisit &sv) {
-    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, sv);
+    return track_v<ScatterVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, sv);
 }
 
 constexpr uint32_t kEscBits = 64;  // shadow segments whose outcome pass 1 records
@@ -835,10 +869,11 @@ struct RatioVisit {
     }
 };
 
+template <bool SDF>
 __device__ __noinline__ uint32_t track_ratio(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
                                              float depth, float &td, uint32_t *nstack, Count &cnt,
                                              const RatioVisit &rv) {
-    return track_v(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, rv);
+    return track_v<RatioVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, rv);
 }
 
 struct PathTotals {
@@ -883,17 +918,17 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         uint32_t res;
         if constexpr (SCATTER) {
             vis.w = tot.w - (dot3f(dsun, acc_sun) + dot3f(dsky, acc_sky));
-            res = track_scatter(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
+            res = track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
         } else if constexpr (RATIO) {
             // the segment's ratios scale everything the path adds from here on
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
-            res = track_ratio(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, rv);
+            res = track_ratio<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, rv);
             T0 = T0 * ws;
             T1 = T1 * ws;
             T2 = T2 * ws;
         } else {
-            res = track_plain(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+            res = track_plain<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
         }
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
@@ -935,7 +970,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
             const bool known = r < kEscBits;
             const Rng g0 = g;
             ScatterVisit sv{(known && ((tot.esc >> r) & 1ull)) ? dot3f(dsun, cn) : 0.0f, grad, S.bricks};
-            const uint32_t sres = track_scatter(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
+            const uint32_t sres = track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
             if (known) {
                 lit = (tot.esc >> r) & 1ull;
             } else {
@@ -944,17 +979,17 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
                 if (lit && sv.w != 0.0f) {
                     Rng g1 = g0;  // the same draws again: ends in the state g already holds
                     float t2;
-                    (void)track_scatter(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
+                    (void)track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
                 }
             }
         } else if constexpr (RATIO) {
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
-            const uint32_t sres = track_ratio(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
+            const uint32_t sres = track_ratio<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
             lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             cn = f3(cn.x * ws, cn.y * ws, cn.z * ws);
         } else {
-            const uint32_t sres = track_plain(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
+            const uint32_t sres = track_plain<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
             lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             if (lit && r < kEscBits) tot.esc |= 1ull << r;
         }
@@ -1175,10 +1210,10 @@ __global__ void adjoint_transmittance_kernel(DevScene S, DevParams P, const floa
         Rng g = rng_seed(seed, r, s);
         const Rng g0 = g;
         float td;
-        if (track_plain(S, P.sigma_e, o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped) {
+        if (track_plain<true>(S, P.sigma_e, o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped) {
             ++esc;
             Rng g1 = g0;
-            (void)track_scatter(S, P.sigma_e, o, d, g1, 3.402823466e+38f, td, nstack, cnt, sv);
+            (void)track_scatter<true>(S, P.sigma_e, o, d, g1, 3.402823466e+38f, td, nstack, cnt, sv);
         }
     }
     atomicAdd(&escapes[r], (unsigned long long)esc);
@@ -1268,7 +1303,7 @@ static size_t mie_smem(const DevParams &P) {
 // Feature bits a frame needs.
 static uint32_t frame_features(const DevScene &S, const DevParams &P) {
     return ((S.occ_nodes && P.embree) ? kFeatOcc : 0u) |
-           ((P.phase_mode == kPhaseHG || P.env_mode != kEnvHosek) ? kFeatExt : 0u);
+           ((P.phase_mode == kPhaseHG || P.env_mode != kEnvHosek) ? kFeatExt : 0u) | (S.sdf_bricks ? kFeatSdf : 0u);
 }
 
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
@@ -1321,16 +1356,14 @@ static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
     }
 }
 
-// Batches carry no occluders (their scenes come from dr_scene_desc records).
+// Frames that use any feature (occluders, HG phase / environment maps, surface
+// leaves) take the instantiation with all of them.  Batches carry no occluders
+// (their scenes come from dr_scene_desc records), so the flag stays off there.
 static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool batch, uint32_t feat = 0) {
-    if (batch) return (feat & kFeatExt) ? persistent_variant_of<true, kFeatExt>(minb, traversal)
-                                        : persistent_variant_of<true, 0>(minb, traversal);
-    switch (feat & (kFeatOcc | kFeatExt)) {
-    case kFeatOcc: return persistent_variant_of<false, kFeatOcc>(minb, traversal);
-    case kFeatExt: return persistent_variant_of<false, kFeatExt>(minb, traversal);
-    case kFeatOcc | kFeatExt: return persistent_variant_of<false, kFeatOcc | kFeatExt>(minb, traversal);
-    default: return persistent_variant_of<false, 0>(minb, traversal);
-    }
+    if (batch) return feat ? persistent_variant_of<true, kFeatAll>(minb, traversal)
+                           : persistent_variant_of<true, 0>(minb, traversal);
+    return feat ? persistent_variant_of<false, kFeatAll>(minb, traversal)
+                : persistent_variant_of<false, 0>(minb, traversal);
 }
 
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
@@ -1384,7 +1417,7 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatExt : 0u, fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatAll : 0u, fn, blocks, batch);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;

@@ -76,6 +76,8 @@ class DrSceneDesc(C.Structure):
         ("bricks", C.c_void_p),
         ("n_leaves", C.c_uint32),
         ("lvoxc", C.c_uint32),
+        ("sdf_bricks", C.c_void_p),
+        ("n_sdf_leaves", C.c_uint32),
     ]
 
 

@@ -170,6 +170,10 @@ class Renderer:
         nodes = np.ascontiguousarray(oc.nodes)
         bricks = np.ascontiguousarray(oc.bricks, np.float32)
         d = N.DrSceneDesc(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+        sdf = getattr(oc, "sdf_bricks", None)
+        if sdf is not None:
+            sdf = np.ascontiguousarray(sdf, np.float32).reshape(-1, 512)
+            d.sdf_bricks, d.n_sdf_leaves = sdf.ctypes.data, len(sdf)
         N.check(N.lib().dr_upload_scene(self._ctx, C.byref(d)))
 
     def set_occluders(self, surfaces, mode: int = OCCLUDE_ALL_SURFACES):
@@ -366,6 +370,11 @@ class Batch:
             bricks = np.ascontiguousarray(oc.bricks, np.float32)
             self._keep += [nodes, bricks]
             descs[i] = N.DrSceneDesc(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
+            sdf = getattr(oc, "sdf_bricks", None)
+            if sdf is not None:
+                sdf = np.ascontiguousarray(sdf, np.float32).reshape(-1, 512)
+                self._keep.append(sdf)
+                descs[i].sdf_bricks, descs[i].n_sdf_leaves = sdf.ctypes.data, len(sdf)
         bv = (N.DrBatchView * len(views))()
         params = []
         self.views = list(views)

@@ -23,6 +23,7 @@ class Octree:
     nodes: np.ndarray     # NODE_DTYPE records
     bricks: np.ndarray    # (n_leaves, 512) float32
     mlevel: int
+    sdf_bricks: np.ndarray | None = None  # (n_sdf, 512) float32 surface bricks of leaves with volx[0] set
 
     @property
     def n_nodes(self) -> int:

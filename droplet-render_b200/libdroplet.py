@@ -33,6 +33,12 @@ Inputs the reference takes from places outside the rendering path:
     header), or SetSkyState(configs, radiances).  Turbidity and ground albedo
     are read from world.droplet.turbidity / ground_albedo when present, else
     the reference's fixed 7 and 0.15 (src/kernel.cpp:525);
+  * the phase function: blcloudsampling.phasef 'M' (Mie) or 'H' (Henyey-
+    Greenstein with phasea), as src/main.cpp:522-536;
+  * the environment: by default escaping rays take the Hosek sky (the
+    reference built with USE_ARHOSEK_SKYMODEL); SetSkyModel("environment")
+    selects its default build, whose light is the world.droplet.envtex image
+    (MapEnv) or none (NullEnv);
   * occlusion geometry: with world.droplet.occlusion set, the reference (built
     with Embree) occludes with the triangle meshes its node trees produce
     (SceneData::Surface, src/main.cpp:406-419, src/SceneOcclusion.cpp:19-56).
@@ -70,6 +76,7 @@ _phase = None
 _sky_dataset = None
 _sky_state = None
 _holdout_only = False     # occluders: every surface (the reference) or holdout meshes only
+_sky_model = "hosek"      # "hosek": the reference built with USE_ARHOSEK_SKYMODEL; "environment": its default build
 _device = int(os.environ.get("DROPLET_DEVICE", "0"))
 
 
@@ -95,6 +102,17 @@ def SetSkyState(configs, radiances):
     from droplet_b200.sky import SkyState
 
     _sky_state = SkyState(np.asarray(configs, np.float64).reshape(3, 9), np.asarray(radiances, np.float64).reshape(3))
+
+
+def SetSkyModel(model: str):
+    """"hosek" (default): escaping rays take the Hosek-Wilkie sky, as the
+    reference built with USE_ARHOSEK_SKYMODEL; "environment": its default
+    build, where they take pow(world.droplet.envtex, 2.2) (MapEnv) or nothing
+    (NullEnv) when no texture is set (src/kernel.cpp:329-364)."""
+    global _sky_model
+    if model not in ("hosek", "environment"):
+        _fail("sky model must be 'hosek' or 'environment'")
+    _sky_model = model
 
 
 def SetOccluderMode(holdout_only: bool):
@@ -152,8 +170,13 @@ def _parse(scene, data, tilex, tiley, w, h):
 
     sam = scene.blcloudsampling
     phasef = str(sam.phasef)
-    if not phasef.upper().startswith("M"):
-        _fail("only the Mie phase function is implemented on the GPU path")
+    # src/main.cpp:522-536: 'H' = HGPhase with g1 = phasea, 'M' = MiePhase
+    if phasef[:1] == "H":
+        phase = ("hg", float(sam.phasea))
+    elif phasef[:1] == "M":
+        phase = ("mie", 0.0)
+    else:
+        _fail(f"unknown phase function {phasef!r}")
     grid = scene.blcloudgrid
     world = scene.world.droplet
     vol = getattr(scene, "droplet_volume", None)
@@ -166,6 +189,15 @@ def _parse(scene, data, tilex, tiley, w, h):
         depth = np.ascontiguousarray(scene.droplet_depth, np.float32).reshape(h, w)
     depthcomp = bool(getattr(world, "depthcomp", False))
     occlusion = bool(getattr(world, "occlusion", False))
+    # environment texture (src/main.cpp:552-587): read by the reference's default
+    # build only (without USE_ARHOSEK_SKYMODEL); see SetSkyModel
+    env = None
+    envtex = str(getattr(world, "envtex", "(droplet.nan)"))
+    if _sky_model == "environment" and envtex != "(droplet.nan)":
+        img = data.images[envtex] if data is not None and hasattr(data, "images") else None
+        if img is not None:
+            ew, eh = int(img.size[0]), int(img.size[1])
+            env = np.asarray(list(img.pixels), np.float32).reshape(eh, ew, 4)
     surfaces = []
     if occlusion:
         for srf in getattr(scene, "droplet_surfaces", None) or []:
@@ -173,6 +205,7 @@ def _parse(scene, data, tilex, tiley, w, h):
                              np.ascontiguousarray(srf["indices"], np.uint32).reshape(-1, 3),
                              0x2 if srf.get("holdout") else 0x0))
     return {
+        "phase": phase, "env": env,
         "occlusion": occlusion, "surfaces": surfaces,
         "viewi": viewi, "proji": proji, "w": int(w), "h": int(h), "tilex": int(tilex), "tiley": int(tiley),
         "sun": suns[0], "scattevs": int(sam.scatterevs), "sigma_s": float(sam.msigmas), "sigma_a": float(sam.msigmaa),
@@ -219,10 +252,23 @@ def _build(job):
             oc = build_octree(vol["block_origin"], vol["block_values"], float(vol["voxel_size"]), job["maxdepth"])
         pdf, cdf = _phase_table()
         sd, sc, sa = job["sun"]
+        from droplet_b200 import _native as N
+
+        kind, g = job["phase"]
+        hosek = _sky_model == "hosek"
+        if hosek:
+            sky_state = _sky(sd, job["turbidity"], job["ground_albedo"])
+        else:
+            from droplet_b200.sky import SkyState
+
+            sky_state = SkyState(np.zeros((3, 9)), np.zeros(3))  # unused without the Hosek model
+        env_mode = N.DR_ENV_HOSEK if hosek else (N.DR_ENV_MAP if job["env"] is not None else N.DR_ENV_NONE)
         st = RenderSettings(sigma_s=job["sigma_s"], sigma_a=job["sigma_a"], scattevs=job["scattevs"], sun_dir=sd,
-                            sun_color=sc, sun_angle=sa, sky=_sky(sd, job["turbidity"], job["ground_albedo"]),
-                            phase=PhaseTable(pdf, cdf), viewi=job["viewi"], proji=job["proji"], w=job["w"],
-                            h=job["h"], depth=job["depth"], depthcomp=job["depthcomp"], embree=job["occlusion"])
+                            sun_color=sc, sun_angle=sa, sky=sky_state, phase=PhaseTable(pdf, cdf),
+                            viewi=job["viewi"], proji=job["proji"], w=job["w"], h=job["h"], depth=job["depth"],
+                            depthcomp=job["depthcomp"], embree=job["occlusion"],
+                            phase_mode=N.DR_PHASE_HG if kind == "hg" else N.DR_PHASE_MIE_REFERENCE, hg_g=g,
+                            env_mode=env_mode, env_map=job["env"])
         r = Renderer(_device)
         if job["occlusion"]:
             r.set_occluders(job["surfaces"], 1 if _holdout_only else 0)

@@ -53,13 +53,18 @@ typedef struct {
     uint32_t mlevel;    /* octree depth; leaves sit at level mlevel-1 */
 } dr_octree;
 
-/* Scene description handed to dr_upload_scene (same fields as dr_octree). */
+/* Scene description handed to dr_upload_scene (the fields of dr_octree, plus
+ * the surface pool Scene::pvol[VOLUME_BUFFER_SDF]).  A leaf carries a FOG brick
+ * (volx[1]), an SDF brick (volx[0]: signed distance samples, same layout), or
+ * both; SDF leaves take majorant 1 (src/kernel.cpp:245-251). */
 typedef struct {
     const dr_node *nodes;
     uint32_t n_nodes;
-    const float *bricks;
+    const float *bricks;        /* FOG pool: n_leaves bricks */
     uint32_t n_leaves;
     uint32_t lvoxc;
+    const float *sdf_bricks;    /* SDF pool: n_sdf_leaves bricks, or NULL when no leaf has one */
+    uint32_t n_sdf_leaves;
 } dr_scene_desc;
 
 #define DR_PHASE_MIE_REFERENCE 0u  /* the reference's tabulated sampler (src/KernelSampler.cpp:257-285) */

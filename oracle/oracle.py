@@ -42,7 +42,7 @@ class OrcParams(C.Structure):
 
 class OrcScene(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("n_nodes", C.c_uint32), ("bricks", C.c_void_p), ("n_leaves", C.c_uint32),
-                ("lvoxc", C.c_uint32), ("occ_tris", C.c_void_p), ("occ_n", C.c_uint32)]
+                ("lvoxc", C.c_uint32), ("occ_tris", C.c_void_p), ("occ_n", C.c_uint32), ("sdf_bricks", C.c_void_p)]
 
 
 class OrcCounters(C.Structure):
@@ -135,12 +135,16 @@ class Port:
         return nodes, bricks.reshape(nl.value, lv.value ** 3), int(ml.value)
 
     @staticmethod
-    def scene(nodes: np.ndarray, bricks: np.ndarray, occ: np.ndarray = None) -> OrcScene:
-        """occ: occluder triangles from occluder_triangles() (kept alive by the caller)."""
+    def scene(nodes: np.ndarray, bricks: np.ndarray, occ: np.ndarray = None, sdf: np.ndarray = None) -> OrcScene:
+        """occ: occluder triangles from occluder_triangles(); sdf: the surface brick
+        pool (float32, 512 per brick); both kept alive by the caller."""
         S = OrcScene(nodes.ctypes.data, len(nodes), bricks.ctypes.data, len(bricks), 8)
         if occ is not None and len(occ):
             assert occ.dtype == np.float32 and occ.flags.c_contiguous and occ.shape[1] == 12
             S.occ_tris, S.occ_n = occ.ctypes.data, len(occ)
+        if sdf is not None:
+            assert sdf.dtype == np.float32 and sdf.flags.c_contiguous
+            S.sdf_bricks = sdf.ctypes.data
         return S
 
     @staticmethod
@@ -385,6 +389,8 @@ class Reference:
         L.ref_scene_create.argtypes = [vp, u32, vp, u32, u32]
         L.ref_scene_create.restype = vp
         L.ref_scene_destroy.argtypes = [vp]
+        L.ref_scene_create_sdf.argtypes = [vp, u32, vp, u32, vp, u32, u32]
+        L.ref_scene_create_sdf.restype = vp
         L.ref_leaf_sequence.argtypes = [vp, C.c_int, vp, vp, u32, vp, vp, vp]
         L.ref_leaf_sequence.restype = u32
         L.ref_sky_state.argtypes = [f64, f64, f64, vp, vp]
@@ -444,10 +450,14 @@ class Reference:
     def set_threads(self, n: int):
         self.L.ref_set_threads(int(n))
 
-    def scene(self, nodes: np.ndarray, bricks: np.ndarray):
+    def scene(self, nodes: np.ndarray, bricks: np.ndarray, sdf: np.ndarray = None):
         nodes = np.ascontiguousarray(nodes)
         bricks = np.ascontiguousarray(bricks, np.float32)
-        return _RefScene(self, self.L.ref_scene_create(_p(nodes), len(nodes), _p(bricks), len(bricks), 8))
+        if sdf is None:
+            return _RefScene(self, self.L.ref_scene_create(_p(nodes), len(nodes), _p(bricks), len(bricks), 8))
+        sdf = np.ascontiguousarray(sdf, np.float32).reshape(-1, 512)
+        return _RefScene(self, self.L.ref_scene_create_sdf(_p(nodes), len(nodes), _p(bricks), len(bricks), _p(sdf),
+                                                           len(sdf), 8))
 
     def mie_tables(self):
         n = self.L.ref_mie_table_size()

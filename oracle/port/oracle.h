@@ -40,6 +40,8 @@ typedef struct {
      * 12 floats each: v0 xyz, 0, e1 = v1 - v0 xyz, 0, e2 = v2 - v0 xyz, 0; tested one by one */
     const float *occ_tris;
     uint32_t occ_n;
+    /* surface bricks (Scene::pvol[VOLUME_BUFFER_SDF]) of leaves with volx[ORC_SDF] set, or NULL */
+    const float *sdf_bricks;
 } orc_scene;
 
 typedef struct {

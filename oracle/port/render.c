@@ -60,20 +60,39 @@ static int track_depth_v(const orc_scene *S, const orc_params *P, const float ro
         const orc_node *o = &S->nodes[node];
         const float lo = td;
         const float tr0 = tra - td, tr1 = trb - td;
-        const float smax = o->qval[ORC_FOG];
-        /* src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
-         * fog leaves, so the masked selects below are bitwise blends: past the
-         * leaf entry, td keeps all but its lowest bit and s0 becomes the lowest
-         * bit of tr0 (0 or the smallest denormal). */
+        /* src/kernel.cpp:245-251: a leaf with a surface brick takes majorant 1 */
+        const int sdf = o->volx[ORC_SDF] != ORC_NONE && S->sdf_bricks, fog = o->volx[ORC_FOG] != ORC_NONE;
+        const float *sbrick = sdf ? S->sdf_bricks + (size_t)o->volx[ORC_SDF] * lv3 : 0;
+        const float smax = sdf ? 1.0f : o->qval[ORC_FOG];
         float s0;
-        if (tra > td) {
+        if (sdf) {
+            /* src/kernel.cpp:253-263: sm = (tra > td) & (d0 > 0) with d0 the
+             * distance at the leaf entry (a full mask: VM is 0) */
+            int skip = 0;
+            if (tra > td) {
+                float r0[3];
+                for (int k = 0; k < 3; ++k) r0[k] = ro[k] + rd[k] * tra;
+                skip = orc_sample_voxel_space(r0, sbrick, o->ce, N) > 0.0f;
+                if (cnt) cnt->density_lookups++;
+            }
+            if (skip) {
+                td = tra;
+                s0 = tr0;
+            } else {
+                s0 = 0.0f;
+            }
+        } else if (tra > td) {
+            /* src/kernel.cpp:241-265: sm = (tra > td) | VM with VM the integer 1 for
+             * fog leaves, so the masked selects below are bitwise blends: past the
+             * leaf entry, td keeps all but its lowest bit and s0 becomes the lowest
+             * bit of tr0 (0 or the smallest denormal). */
             td = tra;
             s0 = tr0;
         } else {
             td = orc_u2f((orc_f2u(td) & ~1u) | (orc_f2u(tra) & 1u));
             s0 = orc_u2f(orc_f2u(tr0) & 1u);
         }
-        const float *brick = S->bricks + (size_t)o->volx[ORC_FOG] * lv3;
+        const float *brick = fog ? S->bricks + (size_t)o->volx[ORC_FOG] * lv3 : 0;
         const float denom = sigma_e * smax;
         float sr = -orc_log(orc_rng_uniform(g)) / denom;
         for (;;) {
@@ -84,17 +103,29 @@ static int track_depth_v(const orc_scene *S, const orc_params *P, const float ro
                 break;
             }
             int rm = sc > tr0;
-            float rho = -1.0f;
+            float rho = -1.0f, dist = 1.0f;
+            int fog_decides = rm;
             if (rm) {
                 float rc[3];
                 for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
-                rho = orc_sample_voxel_space(rc, brick, o->ce, N);
-                if (cnt) cnt->density_lookups++;
+                if (sdf) {
+                    /* src/kernel.cpp:287-300: inside the surface (dist <= 0) always
+                     * collides; outside, the fog brick (if any) decides */
+                    dist = orc_sample_voxel_space(rc, sbrick, o->ce, N);
+                    if (cnt) cnt->density_lookups++;
+                    fog_decides = dist > 0.0f && fog;
+                    if (fog_decides) {
+                        rho = orc_sample_voxel_space(rc, brick, o->ce, N);
+                        if (cnt) cnt->density_lookups++;
+                    }
+                } else {
+                    rho = orc_sample_voxel_space(rc, brick, o->ce, N);
+                    if (cnt) cnt->density_lookups++;
+                }
             }
             const float q = orc_rng_uniform(g);
-            const int looked = rm;
-            rm = rm && (rho / smax < q);
-            if (looked && visit) {
+            rm = rm && (rho / smax < q) && (dist > 0.0f);
+            if (fog_decides && visit) {
                 float rc[3];
                 for (int k = 0; k < 3; ++k) rc[k] = ro[k] + rd[k] * td;
                 visit(vctx, brick, o->ce, rc, rho, smax, !rm);

@@ -67,6 +67,19 @@ extern "C" void *ref_scene_create(const void *nodes, unsigned n_nodes, const flo
     return s;
 }
 
+/* As ref_scene_create, with the surface pool Scene::pvol[VOLUME_BUFFER_SDF]
+ * (n_sdf_leaves bricks) for nodes whose volx[VOLUME_BUFFER_SDF] is set. */
+extern "C" void *ref_scene_create_sdf(const void *nodes, unsigned n_nodes, const float *fog_bricks,
+                                      unsigned n_fog_leaves, const float *sdf_bricks, unsigned n_sdf_leaves,
+                                      unsigned lvoxc) {
+    Scene *s = (Scene *)ref_scene_create(nodes, n_nodes, fog_bricks, n_fog_leaves, lvoxc);
+    delete[] s->pvol[VOLUME_BUFFER_SDF];
+    s->leafx[VOLUME_BUFFER_SDF] = n_sdf_leaves;
+    s->pvol[VOLUME_BUFFER_SDF] = new float[(size_t)n_sdf_leaves * s->lvoxc3 + 1];
+    std::memcpy(s->pvol[VOLUME_BUFFER_SDF], sdf_bricks, (size_t)n_sdf_leaves * s->lvoxc3 * sizeof(float));
+    return s;
+}
+
 extern "C" void ref_scene_destroy(void *p) {
     Scene *s = (Scene *)p;
     delete[] s->pvol[0];

@@ -186,3 +186,39 @@ def occluder_surfaces():
     v = (base[:, None, :] + rng.normal(scale=0.05, size=(200, 3, 3))).reshape(-1, 3).astype(np.float32)
     small = (v, np.arange(600, dtype=np.uint32).reshape(-1, 3), 0x2)
     return [sphere, ground, small]
+
+
+def sdf_scene(radius: float = 0.18):
+    """The config-0 octree with an opaque sphere (centre (0.5, 0.5, 0.5)):
+    leaves within 1.5 leaf diagonals of its surface get an SDF brick (signed
+    distance at the brick's sample positions, the resampling of
+    src/scene.cpp:880-886), every third of those loses its fog brick, and
+    fog leaves wholly inside the sphere are removed as the reference's builder
+    removes them (src/scene.cpp:875-883).  Returns (nodes, bricks, sdf_bricks,
+    mlevel)."""
+    from oracle.oracle import NODE_DTYPE
+
+    nodes, bricks, mlevel = golden_octree()
+    nodes = nodes.copy()
+    c = np.array(W.CENTER, np.float64)
+    vol = nodes["volx"]
+    leaves = np.flatnonzero((vol[:, 0] != 0xFFFFFFFF) | (vol[:, 1] != 0xFFFFFFFF))
+    sdf = []
+    t = (8.0 - 2.0 * np.arange(8) - 1.0) / 7.0
+    for k, i in enumerate(leaves):
+        ce = nodes["ce"][i].astype(np.float64)
+        d = np.linalg.norm(ce[:3] - c) - radius
+        diag = np.sqrt(3.0) * ce[3]
+        if d < -1.5 * diag:
+            nodes["volx"][i, 1] = 0xFFFFFFFF  # inside the surface: no fog leaf
+            continue
+        if abs(d) > 1.5 * diag:
+            continue
+        z, y, x = np.meshgrid(t, t, t, indexing="ij")  # brick order: x fastest
+        p = np.stack([ce[0] - ce[3] * x, ce[1] - ce[3] * y, ce[2] - ce[3] * z], -1).reshape(-1, 3)
+        sdf.append((np.linalg.norm(p - c, axis=1) - radius).astype(np.float32))
+        nodes["volx"][i, 0] = len(sdf) - 1
+        if len(sdf) % 3 == 0:
+            nodes["volx"][i, 1] = 0xFFFFFFFF  # surface leaf without fog
+    assert nodes.dtype == NODE_DTYPE
+    return nodes, bricks, np.ascontiguousarray(np.stack(sdf)), mlevel

@@ -225,3 +225,26 @@ def test_addon_flow_with_occluders_matches_renderer(lib):
         plain, _ = r.render_tile(16, 16, 32, 32, 16, sample_base=0)
     assert np.allclose(sun, ref, rtol=1e-3, atol=1e-5 * np.abs(ref).max())
     assert sun[..., :3].sum() < 0.97 * plain[..., :3].sum()
+
+
+def test_begin_render_reads_phase_and_environment(lib):
+    from test_phase_env import env_map
+
+    scene = fake_scene()
+    scene.blcloudsampling.phasef = "H"
+    scene.blcloudsampling.phasea = 0.6
+    em = env_map()
+    scene.world.droplet.envtex = "sky.exr"
+    data = NS(images={"sky.exr": NS(size=(em.shape[1], em.shape[0]), pixels=em.reshape(-1).tolist())})
+    lib.BeginRender(scene, data, 32, 32, 64, 64, 1)
+    job = lib._job
+    assert job["phase"] == ("hg", 0.6)
+    assert job["env"] is None  # the Hosek build reads no environment texture
+    wait_ready(lib)
+    lib.EndRender()
+    lib.SetSkyModel("environment")
+    lib.BeginRender(scene, data, 32, 32, 64, 64, 1)
+    assert np.array_equal(lib._job["env"], em)
+    wait_ready(lib)
+    with pytest.raises(SystemError):
+        lib.SetSkyModel("other")
