@@ -719,6 +719,7 @@ def run_b200(args):
     import torch
     import torch.distributed as dist
 
+    from droplet_b200 import ranks
     from droplet_b200.renderer import PhaseTable, Renderer, RenderSettings
     from droplet_b200.scene import Octree
     from droplet_b200.sky import SkyState
@@ -748,7 +749,7 @@ def run_b200(args):
         X0, Y0, TW, TH = 0, 0, W_IMG, H_IMG
     sun = torch.empty((TH, TW, 4), dtype=torch.float32, device="cuda")
     sky = torch.empty_like(sun)
-    seed = 1000 + rank
+    seed = ranks.frame_seed(1000, rank)
     tuning = {"kernel": "persistent", "choice": list(r.get_tuning()), "tuned": False}
     if args.tuning:
         r.set_tuning(*[int(v) for v in args.tuning.split(",")])
@@ -792,14 +793,7 @@ def run_b200(args):
     t_local = sum(kernel_ms) / 1e3
     cnt = r.counters()
     verts_local = cnt["vertices"]
-    if world > 1:
-        t = torch.tensor([t_local], dtype=torch.float64, device="cuda")
-        v = torch.tensor([float(verts_local)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(v, op=dist.ReduceOp.SUM)
-        t_max, verts = float(t.item()), float(v.item())
-    else:
-        t_max, verts = t_local, float(verts_local)
+    t_max, verts = ranks.slowest_and_total(t_local, float(verts_local), device="cuda")
     value = verts / t_max
 
     # end to end through the public blocking API with host buffers (params upload
@@ -818,10 +812,7 @@ def run_b200(args):
         r.set_params(settings)
         r.render_tile(X0, Y0, TW, TH, SPP, seed=seed, sample_base=(args.warmup + k) * SPP, out=frame)
     t_e2e = (time.perf_counter() - t0)
-    if world > 1:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = ranks.slowest(t_e2e, device="cuda")
     e2e_value = (verts / args.steps) * e2e_steps / t_e2e  # same work per frame
     d2h = 2 * TH * TW * 16
 

@@ -14,6 +14,11 @@ reference's sky 0/0 for rd.y == 0, adds nothing), and the adjoint leaves such
 paths out the same way.  The leaf majorants
 are recomputed from the bricks on each forward (majorant_scale x maximum,
 floor 0.01) and held fixed through the backward pass.
+
+Several GPUs (one process each): every rank renders its share of the views
+(ranks.my_views), computes its part of the loss and calls backward, then
+ranks.sum_gradients(bricks.grad, albedo.grad) sums the gradients over the ranks
+before the optimizer step: the gradient of the loss summed over all views.
 """
 from __future__ import annotations
 
