@@ -290,6 +290,23 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def profiled_l2():
+    """L2 figures of the render kernel from the committed ncu summary
+    (profiles/render_persistent_kernel_c1.md, lines "l2_throughput_pct: X" and
+    "lts_hit_rate: X")."""
+    p = os.path.join(ROOT, "profiles", "render_persistent_kernel_c1.md")
+    out = {}
+    try:
+        with open(p) as f:
+            for line in f:
+                for key in ("l2_throughput_pct", "lts_hit_rate"):
+                    if line.startswith(key + ":"):
+                        out[key] = float(line.split(":")[1])
+    except Exception:
+        pass
+    return out or None
+
+
 def profiled_traffic():
     """DRAM bytes per vertex of the render kernel from the committed ncu summary
     (profiles/render_persistent_kernel_c1.md, line "dram_bytes_per_vertex: X")."""
@@ -840,6 +857,14 @@ def run_b200(args):
                                   "by this frame's vertices (profiles/render_persistent_kernel_c1.md)",
                 "algorithmic_bytes_per_vertex": b_v,
                 "calibration": "B_v from a 16-spp frame (seed 4242) with the octree stack traversal"}
+    # the scene (23 MB of bricks) is L2-resident: the L2's own throughput as a
+    # fraction of its peak and its hit rate, from the committed ncu capture
+    l2 = profiled_l2()
+    if l2:
+        roofline["l2"] = {"frac": l2.get("l2_throughput_pct", float("nan")) / 100.0,
+                          "lts_hit_rate": l2.get("lts_hit_rate"),
+                          "source": "ncu L2 throughput (% of peak) and lts__t_sector_hit_rate.pct on a 512^2 crop "
+                                    "launch (profiles/render_persistent_kernel_c1.md)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
