@@ -595,6 +595,14 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
             ms.append(a.elapsed_time(b))
     cnt = r.counters()
     plain = cnt["vertices"] / (sum(ms) / 1e3)
+    # the bricks (184 MB) exceed L2: algorithmic bytes per vertex from the
+    # timed frames' own counters (stack traversal: the reference's node visits)
+    b_v = (64.0 * cnt["node_visits"] + 32.0 * cnt["density_lookups"] + 24.0 * cnt["mie_evals"]) / cnt["vertices"]
+    peak, peak_kind = measured_peak()
+    achieved = b_v * plain / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_vertex": b_v,
+                "calibration": "counters of the timed frames" + ("" if best[3] == 0 else " (cell walk: grid cells)")}
     bt = Batch(r, [oc], [BatchView(0, big, spp, 11, (x0, y0, 1920, 1080)) for (x0, y0) in tiles])
     bt.set_tuning(*best)
     for _ in range(warmup):
@@ -644,7 +652,8 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
         "bricks_mb": oc.bricks.nbytes / 1e6, "field_s": round(t_field, 1), "build_s": round(t_build, 1),
         "tuning": list(best),
         "plain": {"value": plain, "unit": "vertices/s", "ms_per_frame": float(np.mean(ms)), "launch_ms": ms,
-                  "vertices_per_frame": cnt["vertices"] / steps, "paths_per_frame": cnt["paths"] / steps},
+                  "vertices_per_frame": cnt["vertices"] / steps, "paths_per_frame": cnt["paths"] / steps,
+                  "roofline": roofline},
         "batched": {"value": batched, "unit": "vertices/s", "ms_per_frame": float(np.mean(bms)), "launch_ms": bms},
         "adjoint_512": {"forward_ms": times[-1][0], "adjoint_ms": times[-1][1],
                         "ratio": times[-1][1] / times[-1][0], "spp": 32,
