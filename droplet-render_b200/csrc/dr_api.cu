@@ -29,7 +29,7 @@ using namespace dr;
 
 extern "C" {
 
-int dr_version(void) { return 100; }
+int dr_version(void) { return DR_VERSION; }
 
 const char *dr_last_error(void) { return last_error(); }
 

@@ -28,6 +28,7 @@ DR_PHASE_HG = 2
 DR_ENV_HOSEK = 0
 DR_ENV_NONE = 1
 DR_ENV_MAP = 2
+DR_VERSION = 200  # include/droplet_b200.h: the struct layouts below
 DR_KERNEL_DEPTHCOMP = 0x1
 DR_KERNEL_FINITE_PATHS = 0x2
 DR_KERNEL_EMBREE = 0x4
@@ -251,6 +252,9 @@ def lib() -> C.CDLL:
                 fn = getattr(L, name)
                 fn.restype = res
                 fn.argtypes = args
+            if L.dr_version() != DR_VERSION:
+                raise ImportError(f"{LIB_PATH} has interface version {L.dr_version()}, this binding expects "
+                                  f"{DR_VERSION}: rebuild the library")
             _lib = L
     return _lib
 

@@ -121,6 +121,11 @@ typedef struct {
 typedef struct dr_ctx dr_ctx;
 
 /* ---- library ------------------------------------------------------------- */
+/* Version of the interface in this header.  dr_version() returns the version
+ * the library was built with; a caller built against another header must not
+ * pass it structs (200: dr_scene_desc gained the SDF pool, dr_render_params the
+ * phase and environment fields). */
+#define DR_VERSION 200
 int dr_version(void);
 const char *dr_last_error(void);
 int dr_device_count(int *count);

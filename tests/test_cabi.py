@@ -35,7 +35,7 @@ def test_binding_covers_the_header():
 
 def test_version_and_errors():
     L = N.lib()
-    assert L.dr_version() >= 100
+    assert L.dr_version() == N.DR_VERSION == 200
     rc = L.dr_create(0, None)
     assert rc == N.DR_ERR_INVALID
     assert b"null" in L.dr_last_error()
