@@ -529,18 +529,10 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
     }
 
 
-def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp: int = 256):
-    """The large sparse scene (config 4): 24 puffs (workloads.slab_recipe) on a
-    2048^3 grid, sigma_t = 100, albedo 0.99, 128 scattering events, 3840x2160 at
-    256 spp rendered as 4 camera tiles of 1920x1080: plain (one launch per tile)
-    and batched (one graph launch of the 4 tiles), both timed with CUDA events;
-    then one adjoint step at 512x512 (32 spp, L2 loss against a 128-spp render of
-    the scene, starting from its bricks scaled by 0.9)."""
-    import torch
-
-    from droplet_b200 import adjoint as AD
-    from droplet_b200 import autotune
-    from droplet_b200.renderer import Batch, BatchView, PhaseTable, RenderSettings
+def build_large(pdf, cdf, cfgs, rads):
+    """The config-4 scene and a settings(w, h) factory for its camera:
+    (octree, settings, non-zero voxels, field seconds, build seconds, blocks)."""
+    from droplet_b200.renderer import PhaseTable, RenderSettings
     from droplet_b200.scene import build_octree
     from droplet_b200.sky import SkyState
 
@@ -552,6 +544,7 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
     t = time.time()
     oc = build_octree(org, vals, rec.voxel_size, 12)
     t_build = time.time() - t
+    n_blocks = int(len(org))
     del vals
     ss, sa, ev = W.medium("c4")
 
@@ -564,6 +557,50 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
                               sky=SkyState(cfgs, rads), phase=PhaseTable(pdf, cdf), viewi=viewi, proji=proji, w=w,
                               h=h)
 
+    return oc, settings, nonzero, t_field, t_build, n_blocks
+
+
+def profile_large(crop: int, launches: int = 3, spp: int = 256):
+    """Capture case for ncu: the config-4 scene, an crop x crop centre crop of
+    its 3840x2160 frame at 256 spp, the tuned launch shape of the full frame
+    ([0, 8, 16, 0, 0, 4, 4]), `launches` launches; prints one line of counters."""
+    import torch
+
+    from droplet_b200.renderer import Renderer
+
+    pdf, cdf, cfgs, rads = load_inputs()
+    oc, settings, _, _, _, _ = build_large(pdf, cdf, cfgs, rads)
+    r = Renderer(0)
+    r.upload(oc)
+    r.set_params(settings(3840, 2160))
+    r.set_tuning(0, 8, 16, 0, 0, 4, 4)
+    x0, y0 = (3840 - crop) // 2, (2160 - crop) // 2
+    sun = torch.empty((crop, crop, 4), device="cuda")
+    sky = torch.empty_like(sun)
+    r.reset_counters()
+    for k in range(launches):
+        r.render_tile_async(x0, y0, crop, crop, spp, 11, k * spp, sun.data_ptr(), sky.data_ptr())
+    torch.cuda.synchronize()
+    cnt = r.counters()
+    print(json.dumps({"profile_large": {"crop": crop, "spp": spp, "launches": launches, "counters": cnt,
+                                        "bricks_mb": oc.bricks.nbytes / 1e6}}))
+    r.close()
+
+
+def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp: int = 256):
+    """The large sparse scene (config 4): 24 puffs (workloads.slab_recipe) on a
+    2048^3 grid, sigma_t = 100, albedo 0.99, 128 scattering events, 3840x2160 at
+    256 spp rendered as 4 camera tiles of 1920x1080: plain (one launch per tile)
+    and batched (one graph launch of the 4 tiles), both timed with CUDA events;
+    then one adjoint step at 512x512 (32 spp, L2 loss against a 128-spp render of
+    the scene, starting from its bricks scaled by 0.9)."""
+    import torch
+
+    from droplet_b200 import adjoint as AD
+    from droplet_b200 import autotune
+    from droplet_b200.renderer import Batch, BatchView
+
+    oc, settings, nonzero, t_field, t_build, n_blocks = build_large(pdf, cdf, cfgs, rads)
     saved = r.get_tuning()
     r.upload(oc)
     big = settings(3840, 2160)
@@ -647,7 +684,7 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
     return {
         "workload": "24 puffs (seeds 20-43, radii U[0.02,0.12], default_rng(2044)) in a 1x1x0.3 slab on a 2048^3 grid, "
                     "sigma_t 100, albedo 0.99, 128 events, 3840x2160 at 256 spp as 4 tiles of 1920x1080",
-        "nonzero_voxels": nonzero, "occupancy": nonzero / 2048 ** 3, "blocks": int(len(org)),
+        "nonzero_voxels": nonzero, "occupancy": nonzero / 2048 ** 3, "blocks": n_blocks,
         "nodes": int(oc.n_nodes), "leaves": int(oc.n_leaves), "octree_depth": int(oc.mlevel),
         "bricks_mb": oc.bricks.nbytes / 1e6, "field_s": round(t_field, 1), "build_s": round(t_build, 1),
         "tuning": list(best),
@@ -964,6 +1001,8 @@ def main():
     ap.add_argument("--no-rmse", action="store_true", help="skip the seconds-to-1%%-RMSE measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the inverse-rendering (adjoint) measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the large sparse scene (config 4)")
+    ap.add_argument("--profile-large", type=int, default=0,
+                    help="profiling case only: an NxN centre crop of the config-4 frame, 3 launches")
     ap.add_argument("--fd-groups", type=int, default=8, help="seed groups of the finite-difference check")
     ap.add_argument("--fd-spp", type=int, default=32, help="spp per view of the finite-difference check")
     ap.add_argument("--fd-eps", type=float, default=1e-3, help="brick-sample step of the finite-difference check")
@@ -971,6 +1010,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_large:
+        return profile_large(args.profile_large)
     return run_b200(args)
 
 
