@@ -272,3 +272,32 @@ def test_reweighted_loss_equals_restatement_and_differences_match_adjoint(adj, p
     ad = float((g * u).sum())
     assert abs(ad) > 0
     assert abs(fd - ad) <= 1e-3 * abs(ad), (fd, ad)
+
+
+def test_adjoint_across_path_chunks_equals_two_halves(adj):
+    """A 512x512 tile at 40 spp has 10.5 M paths, more than one chunk of the
+    totals/scatter passes (2^23 paths): its gradient equals the sum of the two
+    20-spp halves (sample_base 0 and 20), each within one chunk, up to the
+    order of the float atomics."""
+    import torch
+
+    r, nodes, bricks = adj
+    cfg = c0_cfg(512, 512)
+    r.set_params(settings_from_cfg(cfg))
+    rng = np.random.default_rng(13)
+    d = torch.as_tensor(rng.normal(size=(512, 512, 4)).astype(np.float32) * 1e-3, device="cuda").contiguous()
+
+    def grad(spp, base):
+        g = torch.zeros((len(bricks), 512), dtype=torch.float32, device="cuda")
+        ga = torch.zeros(1, dtype=torch.float64, device="cuda")
+        r.adjoint_tile_async(0, 0, 512, 512, spp, 31, base, d.data_ptr(), d.data_ptr(), g.data_ptr(), ga.data_ptr())
+        torch.cuda.synchronize()
+        return g.double().cpu().numpy(), float(ga.item())
+
+    g_full, a_full = grad(40, 0)
+    g_a, a_a = grad(20, 0)
+    g_b, a_b = grad(20, 20)
+    scale = np.abs(g_full).max()
+    assert scale > 0
+    assert np.allclose(g_full, g_a + g_b, rtol=1e-4, atol=1e-5 * scale)
+    assert abs(a_full - (a_a + a_b)) <= 1e-5 * abs(a_full)
