@@ -339,14 +339,21 @@ __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene 
         L.s0 = __uint_as_float(__float_as_uint(L.tr0) & 1u);
     }
     L.denom = P.sigma_e * L.smax;
-    L.sr = -dlog(L.g.uniform()) / L.denom;
+    // the first free-flight distance is drawn by the first track_step:
+    // 0 - l/d equals -l/d here (l < 0), and the draw order is unchanged
+    L.sr = 0.0f;
     return 1u;
 }
 
-// One delta-tracking step.  Returns 0 = continue in this leaf, 1 = leaf left,
-// 2 = segment ended (collision, or the step budget ran out).
+// One delta-tracking step: draws the next free-flight distance, then tests
+// it.  Returns 0 = continue in this leaf, 1 = leaf left, 2 = segment ended
+// (collision, or the step budget ran out).  Drawing at the start of a step
+// rather than at the end of the previous one (or at leaf entry) consumes the
+// same stream in the same order, and lets lanes that just entered a leaf draw
+// together with lanes already tracking.
 template <bool WALK, uint32_t FEAT>
 __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
+    L.sr = L.sr - dlog(L.g.uniform()) / L.denom;
     const float sc = L.s0 + L.sr;
     L.td = L.lo + sc;
     if (!(sc < L.tr1)) {
@@ -381,35 +388,17 @@ __device__ __forceinline__ uint32_t track_step(PathLane<WALK> &L, Count &cnt) {
         L.esc = kTrackEscaped;
         return 2;
     }
-    L.sr = L.sr - dlog(L.g.uniform()) / L.denom;
     return 0;
 }
 
-// Segment end: the body of path_sample() between two track() calls.
+// The end of a main segment: light gathered on escape, the path finished at a
+// cut or the event limit (state becomes kFetch), or a scattering event that
+// sets up the shadow segment and the pending continuation.
 template <bool WALK, uint32_t FEAT>
-__device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
-                                        const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
-                                        uint32_t &state, Trav *slow) {
+__device__ __forceinline__ void scatter_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
+                                              const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
+                                              Count &cnt, uint32_t &state) {
     const float f = P.albedo;
-    if (L.seg == kSegShadow) {
-        if (L.esc == kTrackEscaped && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
-            const bool hit = sun_hit(P, L.rd);
-            const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
-                        s2 = hit ? P.sun_color[2] : 0.0f;
-            L.sun.x = L.sun.x + L.sw[0] * s0;
-            L.sun.y = L.sun.y + L.sw[1] * s1;
-            L.sun.z = L.sun.z + L.sw[2] * s2;
-        }
-        for (int k = 0; k < 3; ++k) {
-            L.T[k] = L.tn[k];
-            L.rd[k] = L.srd[k];
-        }
-        L.r += 1;
-        L.seg = kSegMain;
-        L.depth = 3.402823466e+38f;
-        begin_segment(L, S, cnt, state, slow);
-        return;
-    }
     if (L.r == 0) L.sun.w = L.sky.w = first_alpha(P, L.esc);
     if (L.esc == kTrackEscaped) {
         if (L.r > 0 && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
@@ -427,11 +416,9 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
             L.sky.y = L.sky.y + L.T[1] * sky.y;
             L.sky.z = L.sky.z + L.T[2] * sky.z;
         }
-        finish_path(L, P, A, sun_out, sky_out);
-        state = kFetch;
-        return;
     }
-    if (L.esc == kTrackCut || L.r >= P.scattevs) {
+    // one store for escaped, cut and last-event paths alike
+    if (L.esc == kTrackEscaped || L.esc == kTrackCut || L.r >= P.scattevs) {
         finish_path(L, P, A, sun_out, sky_out);
         state = kFetch;
         return;
@@ -458,6 +445,34 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
         L.rd[k] = lrd[k];
     }
     L.seg = kSegShadow;
+}
+
+// Segment end: the body of path_sample() between two track() calls.
+template <bool WALK, uint32_t FEAT>
+__device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
+                                        const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
+                                        uint32_t &state, Trav *slow) {
+    if (L.seg == kSegShadow) {
+        if (L.esc == kTrackEscaped && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
+            const bool hit = sun_hit(P, L.rd);
+            const float s0 = hit ? P.sun_color[0] : 0.0f, s1 = hit ? P.sun_color[1] : 0.0f,
+                        s2 = hit ? P.sun_color[2] : 0.0f;
+            L.sun.x = L.sun.x + L.sw[0] * s0;
+            L.sun.y = L.sun.y + L.sw[1] * s1;
+            L.sun.z = L.sun.z + L.sw[2] * s2;
+        }
+        for (int k = 0; k < 3; ++k) {
+            L.T[k] = L.tn[k];
+            L.rd[k] = L.srd[k];
+        }
+        L.r += 1;
+        L.seg = kSegMain;
+    } else {
+        scatter_event<WALK, FEAT>(L, S, P, M, A, sun_out, sky_out, cnt, state);
+        if (state == kFetch) return;
+    }
+    // one segment start for both kinds of event, so that lanes of a batch that
+    // ended a shadow segment and lanes that scattered run it together
     L.depth = 3.402823466e+38f;
     begin_segment(L, S, cnt, state, slow);
 }
