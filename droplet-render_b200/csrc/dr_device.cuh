@@ -261,10 +261,12 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
     }
 }
 
-// Up to `budget` loop iterations (child examinations or pops) towards the next
-// leaf: returns kTravLeaf with (leaf, tra, trb), kTravDone when the ray has no
-// further leaf, or kTravMore when the budget ran out first (call again: the
-// state is complete after every iteration).
+// Up to `budget` loop iterations towards the next leaf, each one child
+// examination preceded by the pops of exhausted nodes (at most one per level,
+// so that lanes that pop examine in the same iteration as lanes that do not):
+// returns kTravLeaf with (leaf, tra, trb), kTravDone when the ray has no further
+// leaf, or kTravMore when the budget ran out first (call again: the state is
+// complete after every iteration).
 // tstack (optional, kMaxDepth x 6 floats): the ancestors' intervals are saved
 // at each descent and read back on a pop; without it a pop rebuilds the
 // interval from the root by replaying the 3-bit child slots (the same floats).
@@ -275,7 +277,7 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
     if (!T.active) return kTravDone;
     for (uint32_t it = 0;; ++it) {
         if (it == budget) return kTravMore;
-        if (T.tn >= 8) {
+        while (T.tn >= 8) {  // T.l falls by one per pop: at most kMaxDepth pops
             if (T.l == 0) {
                 T.active = false;
                 return kTravDone;
