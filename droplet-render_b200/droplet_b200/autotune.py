@@ -36,7 +36,7 @@ def stage2(best):
     k, bps, batch = best[:3]
     out = [(k, bps, batch, trav, tile, 0, 0) for trav in (0, 1) for tile in (0, 8, 16)]
     out += [(k, bps, b2, 0, 0, 0, 0) for b2 in (12, 20, 28, 32) if b2 != batch]
-    out += [(k, bps, batch, 0, 0, v, st) for v in (2, 4, 8) for st in (1, 2, 4)]
+    out += [(k, bps, batch, 0, 0, v, st) for v in (2, 3, 4, 8) for st in (1, 2, 4)]
     return out
 
 
