@@ -275,7 +275,7 @@ int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
     if (!c || !t) return need(false, DR_ERR_INVALID, "dr_set_tuning: null argument");
     if (!valid_tuning(t))
         return need(false, DR_ERR_INVALID,
-                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1, tile <= 64, "
+                    "dr_set_tuning: kernel 0/1, event_batch <= 32, blocks_per_sm <= 64, traversal 0/1/2, tile <= 64, "
                     "visits <= 255, steps <= 255");
     c->tuning.kernel = t->kernel;
     c->tuning.block = kPersistentBlock;

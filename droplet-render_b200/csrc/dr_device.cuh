@@ -267,13 +267,46 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
 // returns kTravLeaf with (leaf, tra, trb), kTravDone when the ray has no further
 // leaf, or kTravMore when the budget ran out first (call again: the state is
 // complete after every iteration).
-// tstack (optional, kMaxDepth x 6 floats): the ancestors' intervals are saved
-// at each descent and read back on a pop; without it a pop rebuilds the
-// interval from the root by replaying the 3-bit child slots (the same floats).
+// The stack (see LocalStack / SharedStack) saves the ancestors' node ids and,
+// when it has room for them, their intervals at each descent, read back on a
+// pop; without intervals a pop rebuilds the interval from the root by replaying
+// the 3-bit child slots (the same floats).
 enum : uint32_t { kTravMore = 0, kTravLeaf = 1, kTravDone = 2 };
-__device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
-                                                float &tra, float &trb, Count &cnt, uint32_t budget,
-                                                float (*tstack)[6] = nullptr) {
+
+// Where the traversal keeps its ancestors.  LocalStack: node ids and intervals
+// in the lane's own arrays (local memory); without `iv` a pop replays the
+// interval from the root.  SharedStack: level l of this lane at col[(7l + k) *
+// STRIDE] (k = 0..5 the interval t0.xyz, t1.xyz, k = 6 the node id), one
+// column per lane of the block, so the lanes of a warp touch 32 consecutive
+// words whatever their levels (no bank conflicts); `levels` entries fit, and a
+// descent that would need more gives up like the reference's depth limit (the
+// host sizes the stack from the octree's depth, so that never happens).
+struct LocalStack {
+    uint32_t *nodes;
+    float (*iv)[6];
+    __device__ __forceinline__ uint32_t node(int l) const { return nodes[l]; }
+    __device__ __forceinline__ void set_node(int l, uint32_t v) const { nodes[l] = v; }
+    __device__ __forceinline__ bool has_iv() const { return iv != nullptr; }
+    __device__ __forceinline__ float get(int l, int k) const { return iv[l][k]; }
+    __device__ __forceinline__ void put(int l, int k, float v) const { iv[l][k] = v; }
+    __device__ __forceinline__ bool full(int l) const { return l + 1 >= kMaxDepth - 1; }
+};
+
+template <int STRIDE>
+struct SharedStack {
+    float *col;
+    int levels;
+    __device__ __forceinline__ uint32_t node(int l) const { return __float_as_uint(col[(7 * l + 6) * STRIDE]); }
+    __device__ __forceinline__ void set_node(int l, uint32_t v) const { col[(7 * l + 6) * STRIDE] = __uint_as_float(v); }
+    __device__ __forceinline__ bool has_iv() const { return true; }
+    __device__ __forceinline__ float get(int l, int k) const { return col[(7 * l + k) * STRIDE]; }
+    __device__ __forceinline__ void put(int l, int k, float v) const { col[(7 * l + k) * STRIDE] = v; }
+    __device__ __forceinline__ bool full(int l) const { return l + 1 >= kMaxDepth - 1 || l >= levels; }
+};
+
+template <class ST>
+__device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, const ST &stk, uint32_t &leaf,
+                                                float &tra, float &trb, Count &cnt, uint32_t budget) {
     if (!T.active) return kTravDone;
     for (uint32_t it = 0;; ++it) {
         if (it == budget) return kTravMore;
@@ -284,13 +317,13 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
             }
             const int l = T.l - 1;
             T.l = l;
-            T.node = nstack[l];
+            T.node = stk.node(l);
             T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
-            if (tstack) {
+            if (stk.has_iv()) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    T.t0[k] = tstack[l][k];
-                    T.t1[k] = tstack[l][3 + k];
+                    T.t0[k] = stk.get(l, k);
+                    T.t1[k] = stk.get(l, 3 + k);
                 }
                 continue;
             }
@@ -329,21 +362,21 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
             return kTravLeaf;
         }
         const int l = T.l;
-        if (l + 1 >= kMaxDepth - 1) {  // an internal node at level 15 has no stack room (reference limit)
+        if (stk.full(l)) {  // an internal node at level 15 has no stack room (reference limit)
             T.active = false;
             ++cnt.gave_up;
             return kTravDone;
         }
-        nstack[l] = T.node;
-        if (tstack) {
+        stk.set_node(l, T.node);
+        if (stk.has_iv()) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                tstack[l][k] = T.t0[k];
-                tstack[l][3 + k] = T.t1[k];
+                stk.put(l, k, T.t0[k]);
+                stk.put(l, 3 + k, T.t1[k]);
             }
         }
         T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
-        if (!tstack) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));  // replay path only
+        if (!stk.has_iv()) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));  // replay path only
         T.l = l + 1;
         T.node = child;
         for (int k = 0; k < 3; ++k) {
@@ -353,6 +386,12 @@ __device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint
         }
         T.tn = first_node(T.t0, tm);
     }
+}
+
+__device__ __forceinline__ uint32_t trav_next_k(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,
+                                                float &tra, float &trb, Count &cnt, uint32_t budget,
+                                                float (*tstack)[6] = nullptr) {
+    return trav_next_s(T, S, LocalStack{nstack, tstack}, leaf, tra, trb, cnt, budget);
 }
 
 __device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *nstack, uint32_t &leaf,

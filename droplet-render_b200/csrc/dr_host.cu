@@ -162,6 +162,8 @@ int prepare_scene(const dr_scene_desc *s, HostScene &out) {
         if (cells.empty()) cells.assign(512, kNone);
     }
     out.levels = levels;
+    // a tree with every leaf at depth d pushes at most d - 1 ancestors
+    out.stack_levels = levels >= 2 ? levels - 1 : 0u;
     out.n = n;
     out.mdim = mdim;
     out.n_nodes = s->n_nodes;
@@ -214,6 +216,7 @@ int upload_scene(const HostScene &h, SceneBufs &b, bool use_grid, cudaStream_t s
     S.levels = use_grid ? h.levels : 0u;
     S.n = h.n;
     S.mdim = h.mdim;
+    S.stack_levels = h.stack_levels;
     S.occ_nodes = nullptr;
     S.occ_tris = nullptr;
     S.occ_n_nodes = 0;
@@ -339,7 +342,7 @@ int make_tile_args(uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t 
 
 bool valid_tuning(const dr_tuning *t) {
     return t && t->kernel <= DR_KERNEL_PER_PATH && t->event_batch <= 32 && t->blocks_per_sm <= 64 &&
-           t->traversal <= 1 && t->tile <= 64 && t->visits <= 255 && t->steps <= 255;
+           t->traversal <= 2 && t->tile <= 64 && t->visits <= 255 && t->steps <= 255;
 }
 
 }  // namespace dr

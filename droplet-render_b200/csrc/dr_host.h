@@ -62,6 +62,7 @@ struct HostScene {
     std::vector<uint32_t> macro, cells;
     std::vector<uint8_t> leaf_flag;
     uint32_t levels = 0, n = 0, mdim = 0;
+    uint32_t stack_levels = 0;  // traversal stack entries a ray can need (0: unknown, local stack only)
     uint32_t n_nodes = 0, n_leaves = 0;
     float root_ce[4] = {0, 0, 0, 0};
     const float *bricks = nullptr;  // the caller's brick pool (n_leaves * 512 floats)

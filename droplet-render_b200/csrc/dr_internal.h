@@ -43,6 +43,10 @@ struct DevScene {
     uint32_t levels;     // leaf depth below the root (0 = no grid; stack traversal only)
     uint32_t n;          // leaf cells per axis
     uint32_t mdim;       // macro cells per axis
+    // Entries the stack traversal can push on any ray: internal nodes below the
+    // root on the deepest root-to-leaf path (0: unknown, e.g. leaves at mixed
+    // depths or a DAG; then only the local-memory stack is used).
+    uint32_t stack_levels;
     // Occluder BVH (null: no occluders).  Node i = occ_nodes[4i .. 4i+3]: left
     // box (min xyz, max x), (max yz, right min xy), (right min z, right max
     // xyz), then (left ref, right ref, left count, right count) as uint32

@@ -276,18 +276,24 @@ __device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &
 // One traversal step.  Returns 0 after moving to another cell (call again), 1
 // when a leaf was entered and its free flight prepared, 2 when the segment has
 // no further leaf (or the depth mask stops it): the segment escaped.
-template <bool WALK, uint32_t FEAT>
+// SHS: the traversal stack lives in shared memory (column shcol, shlevels
+// entries) instead of the lane's local arrays nstack / tstack.
+template <bool WALK, uint32_t FEAT, bool SHS>
 __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
                                               uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits,
-                                              float (*tstack)[6]) {
+                                              float (*tstack)[6], float *shcol, int shlevels) {
     uint32_t leaf = 0;
     float tra = 0.0f, trb = 0.0f;
     uint32_t r;
     if constexpr (!WALK) {
         // at most `visits` examinations per loop iteration (0: up to the next leaf)
-        r = L.wmode == 3u ? trav_next_k(L.st.t, S, nstack, leaf, tra, trb, cnt, visits ? visits : 0xffffffffu,
-                                        tstack)
-                          : kTravDone;
+        const uint32_t budget = visits ? visits : 0xffffffffu;
+        if constexpr (SHS)
+            r = L.wmode == 3u ? trav_next_s(L.st.t, S, SharedStack<kPersistentBlock>{shcol, shlevels}, leaf, tra,
+                                            trb, cnt, budget)
+                              : kTravDone;
+        else
+            r = L.wmode == 3u ? trav_next_k(L.st.t, S, nstack, leaf, tra, trb, cnt, budget, tstack) : kTravDone;
     } else if (L.wmode == 1u) {
         r = walk_step(L.st.w, S, leaf, tra, trb, cnt);
     } else if (L.wmode == 2u) {
@@ -516,17 +522,17 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
 }
 
 // One loop iteration of a lane that holds a path (see render_persistent_kernel).
-template <bool WALK, uint32_t FEAT>
+template <bool WALK, uint32_t FEAT, bool SHS>
 __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const DevScene &S, const DevParams &P,
                                           const MieSmem &M, const TileArgs &A, float4 *sun_out, float4 *sky_out,
                                           Count &cnt, uint32_t &state, uint32_t *nstack, Trav *slow, uint32_t visits,
-                                          uint32_t steps, float (*tstack)[6]) {
+                                          uint32_t steps, float (*tstack)[6], float *shcol, int shlevels) {
     if (events) {
         if (state == kEvent) path_event<WALK, FEAT>(L, S, P, M, A, sun_out, sky_out, cnt, state, slow);
         return;
     }
     if (state == kTrav) {
-        const uint32_t r = trav_step<WALK, FEAT>(L, S, P, nstack, slow, cnt, visits, tstack);
+        const uint32_t r = trav_step<WALK, FEAT, SHS>(L, S, P, nstack, slow, cnt, visits, tstack, shcol, shlevels);
         if (r == 1u) {
             state = kStep;
         } else if (r == 2u) {
@@ -556,7 +562,10 @@ __device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
 // BATCH: the paths of many views (each with its own scene, parameters, tile
 // and output) share one work queue; a lane looks its view up when it fetches
 // a path and reads that view's records from global memory (L1-resident).
-template <int MINB, bool WALK, bool BATCH, uint32_t FEAT>
+// SHS (stack traversal only): the traversal stack of each lane lives in
+// dynamic shared memory after the phase tables, `knobs` bits 24-31 entries
+// deep (7 words per entry and lane), instead of local memory.
+template <int MINB, bool WALK, bool BATCH, uint32_t FEAT, bool SHS = false>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
                                                                             float4 *sky_out, DevCounters *C,
@@ -566,6 +575,8 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     // iteration (0: to the next leaf), bits 16-23 the tracking steps per iteration
     const uint32_t event_batch = knobs & 0xffu, visits = (knobs >> 8) & 0xffu;
     const uint32_t steps = ((knobs >> 16) & 0xffu) ? ((knobs >> 16) & 0xffu) : 1u;
+    const int shlevels = (int)(knobs >> 24);
+    static_assert(!(SHS && WALK), "the shared-memory stack serves the stack traversal");
     float ts[kMaxDepth][6];  // ancestors' intervals of the stack traversal (local memory)
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
@@ -583,6 +594,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         n_total = A.n_paths;
     }
     const bool staged = stage_mie(mie_pack, mb, smem, &mbar);
+    float *const shcol = reinterpret_cast<float *>(smem + ((mb + 15u) & ~15u)) + threadIdx.x;
     Count cnt;
     cnt.zero();
     uint32_t paths = 0;
@@ -626,11 +638,11 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work<WALK, FEAT>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack, slow,
-                                 visits, steps, ts);
+            lane_work<WALK, FEAT, SHS>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack,
+                                      slow, visits, steps, ts, shcol, shlevels);
         } else {
-            lane_work<WALK, FEAT>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits, steps,
-                                 ts);
+            lane_work<WALK, FEAT, SHS>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits,
+                                      steps, ts, shcol, shlevels);
         }
     }
     warp_sum_counts(cnt, C, paths);
@@ -1358,6 +1370,12 @@ static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
                                               : render_persistent_kernel<5, true, BATCH, FEAT>;
         return minb >= 7 ? render_persistent_kernel<8, false, BATCH, FEAT> : render_persistent_kernel<5, false, BATCH, FEAT>;
     } else {
+        if (traversal == 2u && !BATCH) {
+            if (minb >= 8) return render_persistent_kernel<8, false, false, 0, true>;
+            if (minb >= 6) return render_persistent_kernel<6, false, false, 0, true>;
+            if (minb >= 5) return render_persistent_kernel<5, false, false, 0, true>;
+            return render_persistent_kernel<4, false, false, 0, true>;
+        }
         if (traversal == 1u) {
             if (minb >= 8) return render_persistent_kernel<8, true, BATCH, 0>;
             if (minb >= 6) return render_persistent_kernel<6, true, BATCH, 0>;
@@ -1409,16 +1427,34 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
     return cudaSuccess;
 }
 
+// Largest octree depth whose traversal stack goes to shared memory: 7 entries
+// x 28 B x 128 lanes = 25 KB per block besides the phase tables.
+constexpr uint32_t kShStackMax = 7;
+
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
-                                     const Tuning &tune, int device, cudaStream_t st) {
+                                     const Tuning &tune_in, int device, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
-    const size_t smem = mie_smem(P);
+    size_t smem = mie_smem(P);
+    const uint32_t feat = frame_features(S, P);
+    Tuning tune = tune_in;
+    uint32_t shlevels = 0;
+    if (tune.traversal == 2u) {
+        // shared-memory stack: only for the plain instantiation and octrees of known, modest depth
+        const size_t with = ((smem + 15) & ~(size_t)15) + (size_t)S.stack_levels * 7 * 4 * kPersistentBlock;
+        if (feat == 0 && S.stack_levels >= 1 && S.stack_levels <= kShStackMax && with <= 48 * 1024) {
+            shlevels = S.stack_levels;
+            smem = with;
+        } else {
+            tune.traversal = 0;
+        }
+    }
     PersistentFn fn;
     int blocks;
     uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, false, frame_features(S, P), fn, blocks, batch);
+    cudaError_t e = persistent_grid(tune, device, smem, false, feat, fn, blocks, batch);
     if (e != cudaSuccess) return e;
+    batch |= shlevels << 24;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
     fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q, batch, BatchArgs{});
@@ -1426,9 +1462,11 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 }
 
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext, int device,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune_in, bool ext, int device,
                                 cudaStream_t st) {
     const size_t smem = mie_smem(P0);
+    Tuning tune = tune_in;
+    if (tune.traversal == 2u) tune.traversal = 0;  // batches keep the local-memory stack
     PersistentFn fn;
     int blocks;
     uint32_t batch;
