@@ -8,6 +8,7 @@
 //   memset(outputs) -> persistent kernel over all views -> step counter += 1
 // as a graph.  Launch k of a batch renders samples [k spp, (k+1) spp) of every
 // view, the same streams dr_render_tile draws with sample_base = k spp.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -37,6 +38,7 @@ struct dr_batch {
     Tuning tuning{0u, 128u, 0u, 8u, 0u, 0u, 0u, 0u};
     uint64_t n_paths = 0, launches = 0;
     bool any_sdf = false;  // a scene with surface (SDF) leaves
+    uint32_t stack_levels = 0;  // deepest traversal stack of the scenes (0: some scene's depth is unknown)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -84,7 +86,7 @@ int build_graph(dr_batch *b) {
     for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
     if (e == cudaSuccess)
         e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
-                                b->ctx->device, b->stream);
+                                b->stack_levels, b->ctx->device, b->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) {
@@ -159,12 +161,16 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
         return code;
     };
     std::vector<DevScene> ds(n_scenes);
+    bool depth_known = true;
     for (uint32_t i = 0; i < n_scenes; ++i) {
         b->scene_bufs.emplace_back(new SceneBufs());
         rc = upload_scene(hs[i], *b->scene_bufs.back(), c->use_grid, b->stream, ds[i]);
         b->any_sdf = b->any_sdf || ds[i].sdf_bricks != nullptr;
         if (rc != DR_OK) return fail(rc);
+        depth_known = depth_known && ds[i].stack_levels > 0;
+        b->stack_levels = std::max(b->stack_levels, ds[i].stack_levels);
     }
+    if (!depth_known) b->stack_levels = 0;
     size_t total = 0;
     b->out_off.resize(n_views);
     for (uint32_t v = 0; v < n_views; ++v) {

@@ -1370,11 +1370,11 @@ static PersistentFn persistent_variant_of(uint32_t minb, uint32_t traversal) {
                                               : render_persistent_kernel<5, true, BATCH, FEAT>;
         return minb >= 7 ? render_persistent_kernel<8, false, BATCH, FEAT> : render_persistent_kernel<5, false, BATCH, FEAT>;
     } else {
-        if (traversal == 2u && !BATCH) {
-            if (minb >= 8) return render_persistent_kernel<8, false, false, 0, true>;
-            if (minb >= 6) return render_persistent_kernel<6, false, false, 0, true>;
-            if (minb >= 5) return render_persistent_kernel<5, false, false, 0, true>;
-            return render_persistent_kernel<4, false, false, 0, true>;
+        if (traversal == 2u) {
+            if (minb >= 8) return render_persistent_kernel<8, false, BATCH, 0, true>;
+            if (minb >= 6) return render_persistent_kernel<6, false, BATCH, 0, true>;
+            if (minb >= 5) return render_persistent_kernel<5, false, BATCH, 0, true>;
+            return render_persistent_kernel<4, false, BATCH, 0, true>;
         }
         if (traversal == 1u) {
             if (minb >= 8) return render_persistent_kernel<8, true, BATCH, 0>;
@@ -1431,6 +1431,20 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
 // x 28 B x 128 lanes = 25 KB per block besides the phase tables.
 constexpr uint32_t kShStackMax = 7;
 
+// DR_TRAVERSAL_STACK_SHARED: only for the plain instantiation and octrees of
+// known, modest depth (and within the default 48 KB of dynamic shared memory);
+// otherwise the local-memory stack.  Returns the stack entries (0: local).
+static uint32_t shared_stack_plan(Tuning &tune, uint32_t feat, uint32_t stack_levels, size_t &smem) {
+    if (tune.traversal != 2u) return 0;
+    const size_t with = ((smem + 15) & ~(size_t)15) + (size_t)stack_levels * 7 * 4 * kPersistentBlock;
+    if (feat == 0 && stack_levels >= 1 && stack_levels <= kShStackMax && with <= 48 * 1024) {
+        smem = with;
+        return stack_levels;
+    }
+    tune.traversal = 0;
+    return 0;
+}
+
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
                                      const Tuning &tune_in, int device, cudaStream_t st) {
@@ -1438,17 +1452,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     size_t smem = mie_smem(P);
     const uint32_t feat = frame_features(S, P);
     Tuning tune = tune_in;
-    uint32_t shlevels = 0;
-    if (tune.traversal == 2u) {
-        // shared-memory stack: only for the plain instantiation and octrees of known, modest depth
-        const size_t with = ((smem + 15) & ~(size_t)15) + (size_t)S.stack_levels * 7 * 4 * kPersistentBlock;
-        if (feat == 0 && S.stack_levels >= 1 && S.stack_levels <= kShStackMax && with <= 48 * 1024) {
-            shlevels = S.stack_levels;
-            smem = with;
-        } else {
-            tune.traversal = 0;
-        }
-    }
+    const uint32_t shlevels = shared_stack_plan(tune, feat, S.stack_levels, smem);
     PersistentFn fn;
     int blocks;
     uint32_t batch;
@@ -1462,16 +1466,17 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 }
 
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune_in, bool ext, int device,
-                                cudaStream_t st) {
-    const size_t smem = mie_smem(P0);
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune_in, bool ext,
+                                uint32_t stack_levels, int device, cudaStream_t st) {
+    size_t smem = mie_smem(P0);
     Tuning tune = tune_in;
-    if (tune.traversal == 2u) tune.traversal = 0;  // batches keep the local-memory stack
+    const uint32_t shlevels = shared_stack_plan(tune, ext ? kFeatAll : 0u, stack_levels, smem);
     PersistentFn fn;
     int blocks;
     uint32_t batch;
     cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatAll : 0u, fn, blocks, batch);
     if (e != cudaSuccess) return e;
+    batch |= shlevels << 24;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
     if (B.n_paths) {

@@ -19,9 +19,10 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 // Batched persistent launch over all views of B (P0: the first view's parameters,
 // which fix the shared phase tables), then one increment of *step; Q->next is
 // cleared on st first.  The three launches are what a batch's graph captures.
+// stack_levels: the deepest traversal stack any of the batch's scenes needs (0: unknown)
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext, int device,
-                                cudaStream_t st);
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext,
+                                uint32_t stack_levels, int device, cudaStream_t st);
 // Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,

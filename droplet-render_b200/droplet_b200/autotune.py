@@ -5,8 +5,10 @@ The persistent kernel has seven knobs (`dr_tuning`):
   occupancy; the smaller register budgets spill a little to L1-resident local memory.
 * the event batch: how many lanes of a warp must be waiting on a segment end before
   the warp shades them.
-* the traversal: octree descent with a node stack, or the cell walk over the leaf
-  grid (faster where leaves are dense along rays, slower through wide empty regions).
+* the traversal: octree descent with a node stack in local memory or in shared
+  memory (octrees that keep their leaves at one depth; otherwise the library uses
+  the local stack), or the cell walk over the leaf grid (faster where
+  leaves are dense along rays, slower through wide empty regions).
 * the tile: pixels handed out row-major or square by square (ray coherence).
 * the work per loop iteration: how many octree nodes the stack traversal examines
   (0: up to the next leaf) and how many free-flight steps a lane takes before the
@@ -34,9 +36,9 @@ def stage2(best):
     """Around the best occupancy and event batch: traversal x tile, neighbouring
     event batches, and the work per loop iteration (visits x steps)."""
     k, bps, batch = best[:3]
-    out = [(k, bps, batch, trav, tile, 0, 0) for trav in (0, 1) for tile in (0, 8, 16)]
+    out = [(k, bps, batch, trav, tile, 0, 0) for trav in (0, 1, 2) for tile in (0, 8, 16)]
     out += [(k, bps, b2, 0, 0, 0, 0) for b2 in (12, 20, 28, 32) if b2 != batch]
-    out += [(k, bps, batch, 0, 0, v, st) for v in (2, 3, 4, 8) for st in (1, 2, 4)]
+    out += [(k, bps, batch, trav, 0, v, st) for trav in (0, 2) for v in (2, 3, 4, 8) for st in (1, 2, 4)]
     return out
 
 

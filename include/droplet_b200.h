@@ -232,8 +232,9 @@ typedef struct {
 } dr_tuning;
 #define DR_TRAVERSAL_STACK 0u  /* octree descent with a node stack (the reference's order) */
 #define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */
-#define DR_TRAVERSAL_STACK_SHARED 2u  /* the octree descent with its stack in shared memory (single frames whose
-                                         octree keeps every leaf at one depth <= 8; otherwise DR_TRAVERSAL_STACK) */
+#define DR_TRAVERSAL_STACK_SHARED 2u  /* the octree descent with its stack in shared memory (frames and batches
+                                         without optional features whose octrees keep every leaf at one depth
+                                         <= 8; otherwise DR_TRAVERSAL_STACK) */
 int dr_set_tuning(dr_ctx *ctx, const dr_tuning *tuning);
 int dr_get_tuning(dr_ctx *ctx, dr_tuning *tuning);
 

@@ -65,7 +65,8 @@ def batch_setup():
     r.close()
 
 
-@pytest.mark.parametrize("tuning", [(0, 5, 24, 0, 0), (0, 8, 16, 1, 8), (0, 4, 8, 0, 16)])
+@pytest.mark.parametrize("tuning", [(0, 5, 24, 0, 0), (0, 8, 16, 1, 8), (0, 4, 8, 0, 16), (0, 8, 24, 2, 0),
+                                    (0, 6, 16, 2, 8)])
 def test_batch_views_equal_restatement(batch_setup, port, tuning):
     r, b, specs, scenes = batch_setup
     b.set_tuning(*tuning)
