@@ -177,9 +177,10 @@ struct Count {
 // ---- octree traversal ----------------------------------------------------
 // The reference's step traverser (src/KernelOctree.cpp:230-349) keeps t0, t1,
 // tm for all 16 levels.  Here only the current internal node's (t0, t1) stay
-// in registers; ancestor node ids live in a 16-entry per-thread array and the
-// ancestors' (t0, t1) in a 16 x 6 float array (local memory), written on each
-// descent and read back on a pop.  Without that array (the probes) a pop
+// in registers; ancestor node ids and the ancestors' (t0, t1) live in a stack
+// (per-thread arrays in local memory, or a per-lane column of shared memory),
+// written on each descent and read back on a pop.  Without the intervals (the
+// probes) a pop
 // rebuilds the interval from the root by replaying the child slots (3 bits per
 // level), which repeats the reference's tm = 0.5f*(t0+t1) selections: the same
 // floats either way.
