@@ -275,18 +275,26 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
 enum : uint32_t { kTravMore = 0, kTravLeaf = 1, kTravDone = 2 };
 
 // Where the traversal keeps its ancestors.  LocalStack: node ids and intervals
-// in the lane's own arrays (local memory); without `iv` a pop replays the
-// interval from the root.  SharedStack: level l of this lane at col[(7l + k) *
-// STRIDE] (k = 0..5 the interval t0.xyz, t1.xyz, k = 6 the node id), one
-// column per lane of the block, so the lanes of a warp touch 32 consecutive
-// words whatever their levels (no bank conflicts); `levels` entries fit, and a
-// descent that would need more gives up like the reference's depth limit (the
-// host sizes the stack from the octree's depth, so that never happens).
+// in the lane's own arrays (local memory), the next child to examine at each
+// level in 4-bit fields of T.tns; without `iv` a pop replays the interval from
+// the root.  SharedStack: level l of this lane at col[(7l + k) * STRIDE] (k =
+// 0..5 the interval t0.xyz, t1.xyz, k = 6 the node id with the next child in
+// bits 28-31, so node ids must stay below 2^28), one column per lane of the
+// block, so the lanes of a warp touch 32 consecutive words whatever their
+// levels (no bank conflicts); `levels` entries fit, and a descent that would
+// need more gives up like the reference's depth limit (the host sizes the
+// stack from the octree's depth, so that never happens).
 struct LocalStack {
     uint32_t *nodes;
     float (*iv)[6];
-    __device__ __forceinline__ uint32_t node(int l) const { return nodes[l]; }
-    __device__ __forceinline__ void set_node(int l, uint32_t v) const { nodes[l] = v; }
+    __device__ __forceinline__ void push_entry(Trav &T, int l) const {
+        nodes[l] = T.node;
+        T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
+    }
+    __device__ __forceinline__ void pop_entry(Trav &T, int l) const {
+        T.node = nodes[l];
+        T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
+    }
     __device__ __forceinline__ bool has_iv() const { return iv != nullptr; }
     __device__ __forceinline__ float get(int l, int k) const { return iv[l][k]; }
     __device__ __forceinline__ void put(int l, int k, float v) const { iv[l][k] = v; }
@@ -297,8 +305,14 @@ template <int STRIDE>
 struct SharedStack {
     float *col;
     int levels;
-    __device__ __forceinline__ uint32_t node(int l) const { return __float_as_uint(col[(7 * l + 6) * STRIDE]); }
-    __device__ __forceinline__ void set_node(int l, uint32_t v) const { col[(7 * l + 6) * STRIDE] = __uint_as_float(v); }
+    __device__ __forceinline__ void push_entry(Trav &T, int l) const {
+        col[(7 * l + 6) * STRIDE] = __uint_as_float(T.node | (T.tn << 28));
+    }
+    __device__ __forceinline__ void pop_entry(Trav &T, int l) const {
+        const uint32_t w = __float_as_uint(col[(7 * l + 6) * STRIDE]);
+        T.node = w & 0x0fffffffu;
+        T.tn = w >> 28;
+    }
     __device__ __forceinline__ bool has_iv() const { return true; }
     __device__ __forceinline__ float get(int l, int k) const { return col[(7 * l + k) * STRIDE]; }
     __device__ __forceinline__ void put(int l, int k, float v) const { col[(7 * l + k) * STRIDE] = v; }
@@ -318,8 +332,7 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             }
             const int l = T.l - 1;
             T.l = l;
-            T.node = stk.node(l);
-            T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
+            stk.pop_entry(T, l);
             if (stk.has_iv()) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -368,7 +381,7 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             ++cnt.gave_up;
             return kTravDone;
         }
-        stk.set_node(l, T.node);
+        stk.push_entry(T, l);
         if (stk.has_iv()) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -376,7 +389,6 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
                 stk.put(l, 3 + k, T.t1[k]);
             }
         }
-        T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
         if (!stk.has_iv()) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));  // replay path only
         T.l = l + 1;
         T.node = child;

@@ -162,8 +162,9 @@ int prepare_scene(const dr_scene_desc *s, HostScene &out) {
         if (cells.empty()) cells.assign(512, kNone);
     }
     out.levels = levels;
-    // a tree with every leaf at depth d pushes at most d - 1 ancestors
-    out.stack_levels = levels >= 2 ? levels - 1 : 0u;
+    // a tree with every leaf at depth d pushes at most d - 1 ancestors; the
+    // shared-memory stack packs node ids into 28 bits
+    out.stack_levels = (levels >= 2 && s->n_nodes < (1u << 28)) ? levels - 1 : 0u;
     out.n = n;
     out.mdim = mdim;
     out.n_nodes = s->n_nodes;
