@@ -184,22 +184,27 @@ struct Count {
 // rebuilds the interval from the root by replaying the child slots (3 bits per
 // level), which repeats the reference's tm = 0.5f*(t0+t1) selections: the same
 // floats either way.
+// Child numbers here are in the node record's slot order (x bit 0, y bit 1, z
+// bit 2, src/scene.cpp:285); Revelles' paper and src/KernelOctree.cpp number
+// them with x in bit 2 and z in bit 0 and remap through nla = {0,4,2,6,1,5,3,7}.
+// The decisions are the same; in slot order the remap is one XOR with the
+// mirror mask.
 __device__ __forceinline__ uint32_t first_node(const float t0[3], const float tm[3]) {
     uint32_t a = 0;
     if (t0[0] > t0[1]) {
         if (t0[0] > t0[2]) {
             if (tm[1] < t0[0]) a |= 2;
-            if (tm[2] < t0[0]) a |= 1;
+            if (tm[2] < t0[0]) a |= 4;
             return a;
         }
     } else {
         if (t0[1] > t0[2]) {
-            if (tm[0] < t0[1]) a |= 4;
-            if (tm[2] < t0[1]) a |= 1;
+            if (tm[0] < t0[1]) a |= 1;
+            if (tm[2] < t0[1]) a |= 4;
             return a;
         }
     }
-    if (tm[0] < t0[2]) a |= 4;
+    if (tm[0] < t0[2]) a |= 1;
     if (tm[1] < t0[2]) a |= 2;
     return a;
 }
@@ -235,9 +240,10 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
         rds[k] = rd[k];
     }
     uint32_t a = 0;
-    if (rds[0] < 0.0f) { ros[0] = 2.0f * S.root_ce[3] - ros[0]; rds[0] = -rds[0]; a |= 4; }
+    // mirror mask in slot order (x bit 0, z bit 2), see first_node
+    if (rds[0] < 0.0f) { ros[0] = 2.0f * S.root_ce[3] - ros[0]; rds[0] = -rds[0]; a |= 1; }
     if (rds[1] < 0.0f) { ros[1] = 2.0f * S.root_ce[3] - ros[1]; rds[1] = -rds[1]; a |= 2; }
-    if (rds[2] < 0.0f) { ros[2] = 2.0f * S.root_ce[3] - ros[2]; rds[2] = -rds[2]; a |= 1; }
+    if (rds[2] < 0.0f) { ros[2] = 2.0f * S.root_ce[3] - ros[2]; rds[2] = -rds[2]; a |= 4; }
     const float mx = 2.0f * S.root_ce[3];
     for (int k = 0; k < 3; ++k) {
         T.t0r[k] = (0.0f - ros[k]) / rds[k];
@@ -345,9 +351,9 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             for (int k = 0; k < l; ++k) {
                 const uint32_t s = (uint32_t)(T.slots >> (3 * k)) & 7u;
                 const float mx = 0.5f * (t0[0] + t1[0]), my = 0.5f * (t0[1] + t1[1]), mz = 0.5f * (t0[2] + t1[2]);
-                if (s & 4) t0[0] = mx; else t1[0] = mx;
+                if (s & 1) t0[0] = mx; else t1[0] = mx;
                 if (s & 2) t0[1] = my; else t1[1] = my;
-                if (s & 1) t0[2] = mz; else t1[2] = mz;
+                if (s & 4) t0[2] = mz; else t1[2] = mz;
             }
             for (int k = 0; k < 3; ++k) {
                 T.t0[k] = t0[k];
@@ -358,14 +364,12 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
         const uint32_t tn = T.tn;
         float tm[3], c0[3], c1[3];
         for (int k = 0; k < 3; ++k) tm[k] = 0.5f * (T.t0[k] + T.t1[k]);
-        const bool bx = tn & 4, by = tn & 2, bz = tn & 1;
+        const bool bx = tn & 1, by = tn & 2, bz = tn & 4;
         c0[0] = bx ? tm[0] : T.t0[0]; c1[0] = bx ? T.t1[0] : tm[0];
         c0[1] = by ? tm[1] : T.t0[1]; c1[1] = by ? T.t1[1] : tm[1];
         c0[2] = bz ? tm[2] : T.t0[2]; c1[2] = bz ? T.t1[2] : tm[2];
-        T.tn = (tn == 7) ? 8u : next_node(c1, bx ? 8u : (tn | 4u), by ? 8u : (tn | 2u), bz ? 8u : (tn | 1u));
-        // nla = {0,4,2,6,1,5,3,7}: reverse the three child bits
-        const uint32_t m = tn ^ T.a;
-        const uint32_t slot = ((m & 1u) << 2) | (m & 2u) | ((m >> 2) & 1u);
+        T.tn = (tn == 7) ? 8u : next_node(c1, bx ? 8u : (tn | 1u), by ? 8u : (tn | 2u), bz ? 8u : (tn | 4u));
+        const uint32_t slot = tn ^ T.a;  // slot order throughout: no bit reversal (see first_node)
         const uint32_t child = child_entry(S, T.node, slot);
         if (c1[0] < 0.0f || c1[1] < 0.0f || c1[2] < 0.0f || child == 0u) continue;
         ++cnt.node_visits;
