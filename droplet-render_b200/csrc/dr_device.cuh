@@ -209,15 +209,6 @@ __device__ __forceinline__ uint32_t first_node(const float t0[3], const float tm
     return a;
 }
 
-__device__ __forceinline__ uint32_t next_node(const float t[3], uint32_t x, uint32_t y, uint32_t z) {
-    if (t[0] < t[1]) {
-        if (t[0] < t[2]) return x;
-    } else {
-        if (t[1] < t[2]) return y;
-    }
-    return z;
-}
-
 __device__ __forceinline__ uint32_t child_entry(const DevScene &S, uint32_t node, uint32_t slot) {
     const uint32_t *c = reinterpret_cast<const uint32_t *>(S.child) + 8u * node + slot;
     return __ldg(c);
@@ -322,7 +313,8 @@ struct SharedStack {
     __device__ __forceinline__ bool has_iv() const { return true; }
     __device__ __forceinline__ float get(int l, int k) const { return col[(7 * l + k) * STRIDE]; }
     __device__ __forceinline__ void put(int l, int k, float v) const { col[(7 * l + k) * STRIDE] = v; }
-    __device__ __forceinline__ bool full(int l) const { return l + 1 >= kMaxDepth - 1 || l >= levels; }
+    // levels <= 13 (the host allows at most 7), so the reference's depth limit is implied
+    __device__ __forceinline__ bool full(int l) const { return l >= levels; }
 };
 
 template <class ST>
@@ -368,7 +360,11 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
         c0[0] = bx ? tm[0] : T.t0[0]; c1[0] = bx ? T.t1[0] : tm[0];
         c0[1] = by ? tm[1] : T.t0[1]; c1[1] = by ? T.t1[1] : tm[1];
         c0[2] = bz ? tm[2] : T.t0[2]; c1[2] = bz ? T.t1[2] : tm[2];
-        T.tn = (tn == 7) ? 8u : next_node(c1, bx ? 8u : (tn | 1u), by ? 8u : (tn | 2u), bz ? 8u : (tn | 4u));
+        // OctreeNextNode's choice (src/KernelOctree.cpp:62-71: x if t1.x is below
+        // both others, else y if t1.y < t1.z, else z) as the exit axis's bit:
+        // past the node's far side on that axis (bit set) the node is done (8)
+        const uint32_t eb = (c1[0] < c1[1]) ? ((c1[0] < c1[2]) ? 1u : 4u) : ((c1[1] < c1[2]) ? 2u : 4u);
+        T.tn = (tn & eb) ? 8u : (tn | eb);
         const uint32_t slot = tn ^ T.a;  // slot order throughout: no bit reversal (see first_node)
         const uint32_t child = child_entry(S, T.node, slot);
         if (c1[0] < 0.0f || c1[1] < 0.0f || c1[2] < 0.0f || child == 0u) continue;
@@ -424,7 +420,7 @@ __device__ __forceinline__ bool trav_next(Trav &T, const DevScene &S, uint32_t *
 // the binary subdivision (grid_plane).  In the mirrored frame:
 //  * the first leaf is the cell containing te = max(t0) (first_node picks, at
 //    every level, the upper half of axis k iff tm_k < te);
-//  * leaving a cell, next_node moves across the exit plane with the smallest t,
+//  * leaving a cell, OctreeNextNode moves across the exit plane with the smallest t,
 //    ties going to z, then y, then x; this choice is the same at every tree
 //    level, since an ancestor's exit planes are never nearer than the cell's;
 //  * entering the sibling subtree (2^t cells per axis, t = trailing zeros of the
