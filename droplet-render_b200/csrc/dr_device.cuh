@@ -17,6 +17,12 @@ __device__ __forceinline__ float sse_min(float a, float b) { return a < b ? a : 
 __device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; } // std::max
 __device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; } // std::min
 __device__ __forceinline__ float lerp_ref(float a, float b, float t) { return t * (b - a) + a; }  // t.madd(b-a, a)
+
+// n / d for the FastDiv record of d (exact for every 32-bit n, see make_fastdiv)
+__device__ __forceinline__ uint32_t fastdiv(uint32_t n, const FastDiv &f) {
+    const uint32_t t = __umulhi(n, f.m);
+    return (t + ((n - t) >> f.s1)) >> f.s2;
+}
 // sfloat1::saturate = _mm_max_ps(_mm_min_ps(x, 1), 0): NaN gives 1.  The NaN case
 // is explicit so that no rewrite into a hardware saturate (NaN -> 0) applies.
 __device__ __forceinline__ float sat_ref(float x) { return x != x ? 1.0f : sse_max(sse_min(x, 1.0f), 0.0f); }

@@ -88,6 +88,26 @@ struct DevParams {
     float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
 };
 
+// Exact unsigned 32-bit division by an invariant d >= 1 (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, fig. 4.1): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), t = mulhi(m, n), for
+// every 32-bit n.  The path kernels use it where a path index becomes a pixel.
+struct FastDiv {
+    uint32_t m, s1, s2;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    if (d == 0) d = 1;  // unused divisor (an empty extent)
+    uint32_t l = 0;
+    while (l < 32 && (1ull << l) < d) ++l;
+    FastDiv f;
+    f.m = (uint32_t)(((((1ull << l) - d) << 32) / d) + 1);
+    f.s1 = l < 1 ? l : 1u;
+    f.s2 = l > 0 ? l - 1 : 0u;
+    return f;
+}
+
 struct TileArgs {
     uint32_t x0, y0, tw, th;
     uint32_t cols, rows;      // rendered extent: even parts of tw, th
@@ -96,6 +116,7 @@ struct TileArgs {
     uint32_t tiles_x;         // squares per row when tile > 0
     uint64_t seed, sample_base;
     uint64_t n_paths;         // path indices: cols * rows * spp (row-major) or squares * tile^2 * spp
+    FastDiv spp_div, cols_div, t2_div, tx_div, tile_div;  // division by spp, cols, tile^2, tiles_x, tile
 };
 
 struct DevCounters {

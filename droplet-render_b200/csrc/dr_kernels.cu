@@ -491,18 +491,26 @@ template <bool WALK>
 __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const DevScene &S, const DevParams &P,
                                            const TileArgs &A, uint64_t shift, Count &cnt, uint32_t &paths,
                                            uint32_t &state, Trav *slow) {
-    const uint64_t pl = p / A.spp;
-    const uint32_t s = (uint32_t)(p - pl * A.spp);
-    const uint32_t pix = (uint32_t)pl;
+    uint32_t pix, s;
+    if (p <= 0xffffffffull) {  // multiply-high divisions (FastDiv) instead of 64-bit division
+        const uint32_t p32 = (uint32_t)p;
+        pix = fastdiv(p32, A.spp_div);
+        s = p32 - pix * A.spp;
+    } else {
+        const uint64_t pl = p / A.spp;
+        s = (uint32_t)(p - pl * A.spp);
+        pix = (uint32_t)pl;
+    }
     uint32_t ix, iy;
     if (A.tile) {
-        const uint32_t t2 = A.tile * A.tile, sq = pix / t2, r = pix - sq * t2;
-        ix = (sq % A.tiles_x) * A.tile + r % A.tile;
-        iy = (sq / A.tiles_x) * A.tile + r / A.tile;
+        const uint32_t sq = fastdiv(pix, A.t2_div), r = pix - sq * (A.tile * A.tile);
+        const uint32_t sy = fastdiv(sq, A.tx_div), ry = fastdiv(r, A.tile_div);
+        ix = (sq - sy * A.tiles_x) * A.tile + (r - ry * A.tile);
+        iy = sy * A.tile + ry;
         if (ix >= A.cols || iy >= A.rows) return false;
     } else {
-        ix = pix % A.cols;
-        iy = pix / A.cols;
+        iy = fastdiv(pix, A.cols_div);
+        ix = pix - iy * A.cols;
     }
     L.px = A.x0 + ix;
     L.py = A.y0 + iy;
