@@ -562,8 +562,9 @@ def build_large(pdf, cdf, cfgs, rads):
 
 def profile_large(crop: int, launches: int = 3, spp: int = 256):
     """Capture case for ncu: the config-4 scene, an crop x crop centre crop of
-    its 3840x2160 frame at 256 spp, the tuned launch shape of the full frame
-    ([0, 8, 16, 0, 0, 4, 4]), `launches` launches; prints one line of counters."""
+    its 3840x2160 frame at 256 spp, the launch shape the bench renders the full
+    frame with (the shared-memory stack traversal, [0, 8, 24, 2, 0, 3, 2]),
+    `launches` launches; prints one line of counters."""
     import torch
 
     from droplet_b200.renderer import Renderer
@@ -573,7 +574,7 @@ def profile_large(crop: int, launches: int = 3, spp: int = 256):
     r = Renderer(0)
     r.upload(oc)
     r.set_params(settings(3840, 2160))
-    r.set_tuning(0, 8, 16, 0, 0, 4, 4)
+    r.set_tuning(0, 8, 24, 2, 0, 3, 2)
     x0, y0 = (3840 - crop) // 2, (2160 - crop) // 2
     sun = torch.empty((crop, crop, 4), device="cuda")
     sky = torch.empty_like(sun)

@@ -15,8 +15,8 @@ The persistent kernel has seven knobs (`dr_tuning`):
   warp moves on; balancing them keeps traversing and tracking lanes busy alike.
 * the kernel family (persistent, or one thread per path; single frames only).
 
-`tune` searches in two stages: occupancy x event batch first, then traversal x tile
-around the best; each candidate is timed with CUDA events on a dedicated stream.
+`tune` searches in two stages: occupancy x event batch (for both octree stacks)
+first, then traversal x tile around the best; each candidate is timed with CUDA events on a dedicated stream.
 Results are cached per (GPU name, workload key) in a small JSON file, so a later run
 with the same key skips the search.
 """
@@ -28,7 +28,9 @@ import time
 
 from . import _native as N
 
-STAGE1 = [(0, bps, batch, 0, 0, 0, 0) for bps in (4, 5, 6, 8) for batch in (8, 16, 24)]
+# occupancy x event batch for both stacks: their best occupancies differ (the
+# shared-memory stack frees local memory, so more resident blocks pay)
+STAGE1 = [(0, bps, batch, trav, 0, 0, 0) for trav in (0, 2) for bps in (4, 5, 6, 8) for batch in (8, 16, 24)]
 PER_PATH = (1, 0, 0, 0, 0, 0, 0)
 
 
