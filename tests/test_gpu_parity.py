@@ -243,6 +243,23 @@ def test_every_launch_shape_renders_the_same_paths(gpu_renderer, port):
         gpu_renderer.set_tuning(*saved)
 
 
+def test_tuning_values_are_checked(gpu_renderer):
+    """dr_set_tuning takes traversal 0 (stack, local memory), 1 (cell walk) and
+    2 (stack, shared memory) and refuses anything else without changing the
+    context's launch shape."""
+    from droplet_b200._native import DrError
+
+    saved = gpu_renderer.get_tuning()
+    try:
+        gpu_renderer.set_tuning(0, 8, 24, 2, 0, 3, 2)
+        assert gpu_renderer.get_tuning() == (0, 8, 24, 2, 0, 3, 2)
+        with pytest.raises(DrError):
+            gpu_renderer.set_tuning(0, 8, 24, 3, 0, 3, 2)
+        assert gpu_renderer.get_tuning() == (0, 8, 24, 2, 0, 3, 2)
+    finally:
+        gpu_renderer.set_tuning(*saved)
+
+
 def _rel(x, y):
     return float(np.sqrt(((x - y) ** 2).sum()) / np.sqrt((y ** 2).sum()))
 

@@ -75,7 +75,10 @@ def test_path_samples_bit_exact(renderer, port, phase, env):
         assert np.array_equal(bits(b[i]), bits(pb)), (i, b[i], pb)
 
 
-@pytest.mark.parametrize("tuning", [(0, 0, 0, 0, 0, 0, 0), (1, 0, 0, 0, 0, 0, 0), (0, 8, 24, 1, 8, 4, 4)])
+# (0, 8, 24, 2, ...): the shared-memory stack is asked for, but a frame with the
+# HG phase or an environment map renders through the local-stack instantiation
+@pytest.mark.parametrize("tuning", [(0, 0, 0, 0, 0, 0, 0), (1, 0, 0, 0, 0, 0, 0), (0, 8, 24, 1, 8, 4, 4),
+                                    (0, 8, 24, 2, 0, 3, 2)])
 def test_tiles_equal_restatement(renderer, port, tuning):
     nodes, bricks, _ = golden_octree()
     cfg = _cfg("hg", "map")
