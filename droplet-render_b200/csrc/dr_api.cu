@@ -87,6 +87,7 @@ int dr_destroy(dr_ctx *c) {
         c->mie_pack.release();
         c->depth.release();
         c->counters.release();
+        c->call_counters.release();
         c->tile_sun.release();
         c->tile_sky.release();
         c->scratch.release();
@@ -207,9 +208,53 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
                 "dr_set_params: copy environment map");
         d.env_map = c->env.p;
     }
+    d.step_budget = c->step_budget;
     c->params = d;
     c->has_params = true;
     return DR_OK;
+}
+
+int dr_set_step_budget(dr_ctx *c, uint32_t steps) {
+    if (!c) return need(false, DR_ERR_INVALID, "dr_set_step_budget: null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->step_budget = steps ? steps : kStepBudget;
+    c->params.step_budget = c->step_budget;
+    return DR_OK;
+}
+
+// A blocking call's give-ups: its own counters are added to the context's, and
+// a call whose paths gave up reports DR_ERR_GAVE_UP (its outputs are written,
+// but those paths are cut short).
+static int finish_call_counters(dr_ctx *c, const char *what) {
+    DR_CUDA(launch_add_counters(c->counters.p, c->call_counters.p, c->stream), what);
+    DevCounters h{};
+    DR_CUDA(cudaMemcpyAsync(&h, c->call_counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream), what);
+    DR_CUDA(cudaStreamSynchronize(c->stream), what);
+    if (h.gave_up == 0) return DR_OK;
+    c->gave_up_reported += h.gave_up;
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "%s: %llu path segments or blocks gave up (iteration budget): the result is incomplete",
+                  what, (unsigned long long)h.gave_up);
+    set_error(DR_ERR_GAVE_UP, msg);
+    return DR_ERR_GAVE_UP;
+}
+
+int dr_check_complete(dr_ctx *c, void *stream) {
+    if (!c) return need(false, DR_ERR_INVALID, "dr_check_complete: null context");
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    DR_CUDA(cudaStreamSynchronize(stream ? (cudaStream_t)stream : c->stream), "dr_check_complete: sync");
+    DR_CUDA(cudaStreamSynchronize(c->stream), "dr_check_complete: sync");
+    DevCounters h{};
+    DR_CUDA(cudaMemcpy(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost), "dr_check_complete: copy");
+    if (h.gave_up <= c->gave_up_reported) return DR_OK;
+    const unsigned long long n = h.gave_up - c->gave_up_reported;
+    c->gave_up_reported = h.gave_up;
+    char msg[160];
+    std::snprintf(msg, sizeof(msg),
+                  "dr_check_complete: %llu path segments or blocks gave up (iteration budget) since the last check", n);
+    set_error(DR_ERR_GAVE_UP, msg);
+    return DR_ERR_GAVE_UP;
 }
 
 static int tile_args(const dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
@@ -263,12 +308,16 @@ int dr_shadow_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t n = (size_t)tw * th;
     DR_CUDA(c->tile_sun.reserve(n), "shadow: alloc tile");
-    int rc = dr_shadow_tile_async(c, x0, y0, tw, th, spp, seed, sample_base, (float *)c->tile_sun.p, nullptr);
+    DR_CUDA(c->call_counters.reserve(1), "shadow: alloc counters");
+    TileArgs A;
+    int rc = tile_args(c, x0, y0, tw, th, spp, seed, sample_base, 0u, A);
     if (rc != DR_OK) return rc;
+    DR_CUDA(cudaMemsetAsync(c->call_counters.p, 0, sizeof(DevCounters), c->stream), "shadow: clear");
+    DR_CUDA(cudaMemsetAsync(c->tile_sun.p, 0, n * sizeof(float4), c->stream), "shadow: clear");
+    DR_CUDA(launch_shadow_tile(c->scene, c->params, A, c->tile_sun.p, c->call_counters.p, c->stream), "shadow: launch");
     DR_CUDA(cudaMemcpyAsync(out, c->tile_sun.p, n * sizeof(float4), cudaMemcpyDeviceToHost, c->stream),
             "shadow: copy out");
-    DR_CUDA(cudaStreamSynchronize(c->stream), "shadow: sync");
-    return DR_OK;
+    return finish_call_counters(c, "dr_shadow_tile");
 }
 
 int dr_set_tuning(dr_ctx *c, const dr_tuning *t) {
@@ -341,6 +390,7 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
     const size_t n = (size_t)tw * th;
     DR_CUDA(c->tile_sun.reserve(n), "render: alloc tile");
     DR_CUDA(c->tile_sky.reserve(n), "render: alloc tile");
+    DR_CUDA(c->call_counters.reserve(1), "render: alloc counters");
     int rc = ensure_pipeline(c, n);
     if (rc != DR_OK) return rc;
     const uint32_t rows = 2 * (th / 2);
@@ -349,6 +399,7 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
     hb += hb & 1u;
     DR_CUDA(cudaMemsetAsync(c->tile_sun.p, 0, n * sizeof(float4), c->stream), "render: clear");
     DR_CUDA(cudaMemsetAsync(c->tile_sky.p, 0, n * sizeof(float4), c->stream), "render: clear");
+    DR_CUDA(cudaMemsetAsync(c->call_counters.p, 0, sizeof(DevCounters), c->stream), "render: clear");
     DR_CUDA(cudaEventRecord(c->ev_clear, c->stream), "render: record");
     DR_CUDA(cudaStreamWaitEvent(c->band_stream[0], c->ev_clear, 0), "render: wait");
     DR_CUDA(cudaStreamWaitEvent(c->band_stream[1], c->ev_clear, 0), "render: wait");
@@ -364,9 +415,9 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
         float4 *sd = c->tile_sun.p + off, *kd = c->tile_sky.p + off;
         cudaStream_t bs = c->band_stream[k & 1];
         if (c->tuning.kernel == DR_KERNEL_PER_PATH)
-            err = launch_render_tile(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->counters.p, bs);
+            err = launch_render_tile(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->call_counters.p, bs);
         else
-            err = launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->counters.p,
+            err = launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->call_counters.p,
                                            c->band_work.p + k, c->tuning, c->device, bs);
         if (err == cudaSuccess) err = cudaEventRecord(c->band_done[k], bs);
         if (err == cudaSuccess) err = cudaStreamWaitEvent(c->copy_stream, c->band_done[k], 0);
@@ -400,7 +451,7 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
         std::memset(sun_out + 4 * (size_t)rows * tw, 0, (size_t)tw * sizeof(float4));
         std::memset(sky_out + 4 * (size_t)rows * tw, 0, (size_t)tw * sizeof(float4));
     }
-    return DR_OK;
+    return finish_call_counters(c, "dr_render_tile");
 }
 
 int dr_synchronize(dr_ctx *c) {
@@ -430,6 +481,7 @@ int dr_reset_counters(dr_ctx *c) {
     DeviceGuard g(c->device);
     DR_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(DevCounters), c->stream), "dr_reset_counters");
     DR_CUDA(cudaStreamSynchronize(c->stream), "dr_reset_counters: sync");
+    c->gave_up_reported = 0;
     return DR_OK;
 }
 

@@ -138,6 +138,7 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
         std::vector<unsigned char> pack;
         int rc = prepare_params(bv.params, hv[v].P, pack);
         if (rc != DR_OK) return rc;
+        hv[v].P.step_budget = c->step_budget;
         if (v == 0) pack0 = pack;
         else if (pack != pack0)
             return need(false, DR_ERR_INVALID, "dr_batch_create: every view must use the same phase tables and mode");

@@ -1062,7 +1062,7 @@ struct NoVisit {
 // SDF: the scene may hold surface leaves (src/kernel.cpp:241-305); without it
 // every leaf is a fog leaf and the surface tests are not compiled in.
 template <class Visit, bool SDF = true>
-__device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
+__device__ __forceinline__ uint32_t track_v(const DevScene &S, SegMedium med, const float ro[3], const float rd[3],
                                             Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
                                             const Visit &visit);
 
@@ -1070,20 +1070,21 @@ template <bool SDF = true>
 __device__ __forceinline__ uint32_t track(const DevScene &S, const DevParams &P, const float ro[3], const float rd[3],
                                           Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt) {
     const NoVisit nv;
-    return track_v<NoVisit, SDF>(S, P.sigma_e, ro, rd, g, depth, td_out, nstack, cnt, nv);
+    return track_v<NoVisit, SDF>(S, seg_medium(P), ro, rd, g, depth, td_out, nstack, cnt, nv);
 }
 
 template <class Visit, bool SDF>
-__device__ __forceinline__ uint32_t track_v(const DevScene &S, float sigma_e, const float ro[3], const float rd[3],
+__device__ __forceinline__ uint32_t track_v(const DevScene &S, SegMedium med, const float ro[3], const float rd[3],
                                             Rng &g, float depth, float &td_out, uint32_t *nstack, Count &cnt,
                                             const Visit &visit) {
+    const float sigma_e = med.sigma_e;
     Trav T;
     trav_init(T, S, ro, rd, cnt);
     ++cnt.vertices;
     float td = 0.0f;
     uint32_t leaf;
     float tra, trb;
-    uint32_t budget = kStepBudget;
+    uint32_t budget = med.budget;
     float tstack[kMaxDepth][6];
     while (trav_next_k(T, S, nstack, leaf, tra, trb, cnt, 0xffffffffu, tstack) == kTravLeaf) {
         if (!(td < depth)) break;

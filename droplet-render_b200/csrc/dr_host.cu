@@ -294,6 +294,7 @@ int prepare_params(const dr_render_params *p, DevParams &d, std::vector<unsigned
         const float zz = p->proji[8 + 2] + p->proji[12 + 2], zw = p->proji[8 + 3] + p->proji[12 + 3];
         d.clip_end = -zz / zw;
     }
+    d.step_budget = kStepBudget;
     const size_t n_ex = p->phase_mode == DR_PHASE_MIE_EXACT ? 8 * (size_t)p->mie_n + 4 : 0;
     pack.assign((size_t)p->mie_n * 20 + 4 * n_ex, 0);
     for (uint32_t i = 0; i < p->mie_n; ++i) {

@@ -127,6 +127,9 @@ struct dr_ctx {
     dr::DevBuf<float> depth;
     dr::DevBuf<float> env;            // environment map texels (DR_ENV_MAP)
     dr::DevBuf<dr::DevCounters> counters;
+    dr::DevBuf<dr::DevCounters> call_counters;  // a blocking call's own counts (added to `counters` at its end)
+    uint32_t step_budget = dr::kStepBudget;     // dr_set_step_budget
+    unsigned long long gave_up_reported = 0;    // counters.gave_up when dr_check_complete last looked
     dr::DevBuf<float4> tile_sun, tile_sky;
     dr::DevBuf<unsigned char> scratch;
     dr::DevBuf<dr::WorkQueue> work;

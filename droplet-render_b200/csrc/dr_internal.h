@@ -86,7 +86,15 @@ struct DevParams {
     const float *env_map;     // kEnvMap: env_w * env_h RGBA texels (device)
     uint32_t env_w, env_h;
     float clip_end;           // far clip distance: -z/w of (0,0,1,1) * projInv (src/kernel.cpp:574-575)
+    uint32_t step_budget;     // tracking steps per segment before a path gives up (kStepBudget unless set)
 };
+
+// What a tracking loop needs of the parameters: the extinction and the step budget.
+struct SegMedium {
+    float sigma_e;
+    uint32_t budget;
+};
+DR_HD inline SegMedium seg_medium(const DevParams &P) { return SegMedium{P.sigma_e, P.step_budget}; }
 
 // Exact unsigned 32-bit division by an invariant d >= 1 (Granlund and
 // Montgomery, "Division by invariant integers using multiplication", PLDI

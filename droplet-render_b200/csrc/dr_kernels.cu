@@ -244,8 +244,8 @@ __device__ __noinline__ SlowLeaf slow_next(Trav *T, DevScene S, uint32_t *nstack
 }
 
 template <bool WALK>
-__device__ __forceinline__ void begin_segment(PathLane<WALK> &L, const DevScene &S, Count &cnt, uint32_t &state,
-                                              Trav *slow) {
+__device__ __forceinline__ void begin_segment(PathLane<WALK> &L, const DevScene &S, uint32_t budget, Count &cnt,
+                                              uint32_t &state, Trav *slow) {
     if constexpr (WALK) {
         L.wmode = walk_init(L.st.w, S, L.ro, L.rd, cnt);
         if (L.wmode == 2u)
@@ -256,7 +256,7 @@ __device__ __forceinline__ void begin_segment(PathLane<WALK> &L, const DevScene 
     }
     ++cnt.vertices;
     L.td = 0.0f;
-    L.budget = kStepBudget;
+    L.budget = budget;
     state = kTrav;
 }
 
@@ -480,7 +480,7 @@ __device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S,
     // one segment start for both kinds of event, so that lanes of a batch that
     // ended a shadow segment and lanes that scattered run it together
     L.depth = 3.402823466e+38f;
-    begin_segment(L, S, cnt, state, slow);
+    begin_segment(L, S, P.step_budget, cnt, state, slow);
 }
 
 // Starts path number p; returns false when p lies outside the frame (no work).
@@ -522,7 +522,7 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     L.r = 0;
     L.seg = kSegMain;
     L.depth = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
-    begin_segment(L, S, cnt, state, slow);
+    begin_segment(L, S, P.step_budget, cnt, state, slow);
     // A camera ray that misses the root box draws no random number: its
     // sample is exactly zero.  Seed the stream only for rays that enter.
     if (L.wmode != 0u) L.g = rng_seed(A.seed, (uint64_t)L.py * P.w + L.px, A.sample_base + shift + s);
@@ -658,6 +658,16 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
 
 // Advances the launch counter of a batch (the last node of its graph).
 __global__ void batch_step_kernel(unsigned long long *step) { *step += 1ull; }
+
+// Adds a blocking call's own counters into the context's.
+__global__ void add_counters_kernel(DevCounters *dst, const DevCounters *src) {
+    dst->paths += src->paths;
+    dst->vertices += src->vertices;
+    dst->node_visits += src->node_visits;
+    dst->density_lookups += src->density_lookups;
+    dst->mie_evals += src->mie_evals;
+    dst->gave_up += src->gave_up;
+}
 
 // ---- parity probes ------------------------------------------------------------
 __global__ void probe_leaf_kernel(DevScene S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
@@ -866,17 +876,17 @@ struct ScatterVisit {
 // One copy of the tracking loop per visitor for the whole adjoint (each call
 // site inlining it would multiply the code the warps fetch).
 template <bool SDF>
-__device__ __noinline__ uint32_t track_plain(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
+__device__ __noinline__ uint32_t track_plain(const DevScene S, SegMedium med, const float *ro, const float *rd, Rng &g,
                                              float depth, float &td, uint32_t *nstack, Count &cnt) {
     const NoVisit nv;
-    return track_v<NoVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, nv);
+    return track_v<NoVisit, SDF>(S, med, ro, rd, g, depth, td, nstack, cnt, nv);
 }
 
 template <bool SDF>
-__device__ __noinline__ uint32_t track_scatter(const DevScene S, float sigma_e, const float *ro, const float *rd,
+__device__ __noinline__ uint32_t track_scatter(const DevScene S, SegMedium med, const float *ro, const float *rd,
                                                Rng &g, float depth, float &td, uint32_t *nstack, Count &cnt,
                                                const ScatterVisit &sv) {
-    return track_v<ScatterVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, sv);
+    return track_v<ScatterVisit, SDF>(S, med, ro, rd, g, depth, td, nstack, cnt, sv);
 }
 
 constexpr uint32_t kEscBits = 64;  // shadow segments whose outcome pass 1 records
@@ -905,10 +915,10 @@ struct RatioVisit {
 };
 
 template <bool SDF>
-__device__ __noinline__ uint32_t track_ratio(const DevScene S, float sigma_e, const float *ro, const float *rd, Rng &g,
+__device__ __noinline__ uint32_t track_ratio(const DevScene S, SegMedium med, const float *ro, const float *rd, Rng &g,
                                              float depth, float &td, uint32_t *nstack, Count &cnt,
                                              const RatioVisit &rv) {
-    return track_v<RatioVisit, SDF>(S, sigma_e, ro, rd, g, depth, td, nstack, cnt, rv);
+    return track_v<RatioVisit, SDF>(S, med, ro, rd, g, depth, td, nstack, cnt, rv);
 }
 
 struct PathTotals {
@@ -953,17 +963,17 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
         uint32_t res;
         if constexpr (SCATTER) {
             vis.w = tot.w - (dot3f(dsun, acc_sun) + dot3f(dsky, acc_sky));
-            res = track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
+            res = track_scatter<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, vis);
         } else if constexpr (RATIO) {
             // the segment's ratios scale everything the path adds from here on
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
-            res = track_ratio<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, rv);
+            res = track_ratio<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt, rv);
             T0 = T0 * ws;
             T1 = T1 * ws;
             T2 = T2 * ws;
         } else {
-            res = track_plain<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
+            res = track_plain<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), ro, rd, g, r == 0 ? depth0 : 3.402823466e+38f, td, nstack, cnt);
         }
         if (res == kTrackCut) break;
         if (res == kTrackEscaped) {
@@ -1005,7 +1015,7 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
             const bool known = r < kEscBits;
             const Rng g0 = g;
             ScatterVisit sv{(known && ((tot.esc >> r) & 1ull)) ? dot3f(dsun, cn) : 0.0f, grad, S.bricks};
-            const uint32_t sres = track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
+            const uint32_t sres = track_scatter<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, sv);
             if (known) {
                 lit = (tot.esc >> r) & 1ull;
             } else {
@@ -1014,17 +1024,17 @@ __device__ __forceinline__ void adjoint_pass(const DevScene &S, const DevParams 
                 if (lit && sv.w != 0.0f) {
                     Rng g1 = g0;  // the same draws again: ends in the state g already holds
                     float t2;
-                    (void)track_scatter<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
+                    (void)track_scatter<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), rc, lrd, g1, 3.402823466e+38f, t2, nstack, cnt, sv);
                 }
             }
         } else if constexpr (RATIO) {
             float ws = 1.0f;
             const RatioVisit rv{&ws, pert, S.bricks};
-            const uint32_t sres = track_ratio<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
+            const uint32_t sres = track_ratio<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt, rv);
             lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             cn = f3(cn.x * ws, cn.y * ws, cn.z * ws);
         } else {
-            const uint32_t sres = track_plain<(FEAT & kFeatSdf) != 0>(S, P.sigma_e, rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
+            const uint32_t sres = track_plain<(FEAT & kFeatSdf) != 0>(S, seg_medium(P), rc, lrd, g, 3.402823466e+38f, tds, nstack, cnt);
             lit = sres == kTrackEscaped && !((FEAT & kFeatOcc) && P.embree && occluded(S, rc, lrd));
             if (lit && r < kEscBits) tot.esc |= 1ull << r;
         }
@@ -1245,10 +1255,10 @@ __global__ void adjoint_transmittance_kernel(DevScene S, DevParams P, const floa
         Rng g = rng_seed(seed, r, s);
         const Rng g0 = g;
         float td;
-        if (track_plain<true>(S, P.sigma_e, o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped) {
+        if (track_plain<true>(S, seg_medium(P), o, d, g, 3.402823466e+38f, td, nstack, cnt) == kTrackEscaped) {
             ++esc;
             Rng g1 = g0;
-            (void)track_scatter<true>(S, P.sigma_e, o, d, g1, 3.402823466e+38f, td, nstack, cnt, sv);
+            (void)track_scatter<true>(S, seg_medium(P), o, d, g1, 3.402823466e+38f, td, nstack, cnt, sv);
         }
     }
     atomicAdd(&escapes[r], (unsigned long long)esc);
@@ -1494,6 +1504,11 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
         if (e != cudaSuccess) return e;
     }
     batch_step_kernel<<<1, 1, 0, st>>>(step);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_counters(DevCounters *dst, const DevCounters *src, cudaStream_t st) {
+    add_counters_kernel<<<1, 1, 0, st>>>(dst, src);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,9 @@ cudaError_t launch_adjoint_transmittance(const DevScene &S, const DevParams &P, 
 cudaError_t launch_leaf_majorants(float4 *leaf, const uint32_t *leaf_nodes, uint32_t n_leafnodes, const float *bricks,
                                   float scale, cudaStream_t st);
 
+// dst += src, field by field (one thread; a blocking call's counters).
+cudaError_t launch_add_counters(DevCounters *dst, const DevCounters *src, cudaStream_t st);
+
 // Allocation-free transmittance: scratch in a file-scope device array.
 uint32_t noalloc_max_rays();
 cudaError_t noalloc_scratch(int device, unsigned long long **out);

@@ -53,6 +53,14 @@ class DrError(RuntimeError):
         self.code = code
 
 
+class DrGaveUp(DrError):
+    """DR_ERR_GAVE_UP: the call finished, but some paths were cut short by an
+    iteration budget, so its outputs are incomplete.  `result` holds the
+    outputs where the raising method has them (else None)."""
+
+    result = None
+
+
 class DrNode(C.Structure):
     """Octree node record, the reference's OctreeStructure (src/scene.h:21-31)."""
 
@@ -181,6 +189,8 @@ SIGNATURES = {
          C.c_void_p],
     ),
     "dr_synchronize": (C.c_int, [C.c_void_p]),
+    "dr_check_complete": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dr_set_step_budget": (C.c_int, [C.c_void_p, C.c_uint32]),
     "dr_set_bricks_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]),
     "dr_get_majorants": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dr_adjoint_tile_async": (
@@ -261,7 +271,8 @@ def lib() -> C.CDLL:
 
 def check(rc: int) -> None:
     if rc != DR_OK:
-        raise DrError(rc, lib().dr_last_error().decode(errors="replace"))
+        msg = lib().dr_last_error().decode(errors="replace")
+        raise (DrGaveUp if rc == DR_ERR_GAVE_UP else DrError)(rc, msg)
 
 
 def device_count() -> int:

@@ -202,10 +202,15 @@ class Renderer:
         else:
             sun = np.zeros((th, tw, 4), np.float32)
             sky = np.zeros((th, tw, 4), np.float32)
-        N.check(N.lib().dr_render_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, sun.ctypes.data,
-                                       sky.ctypes.data))
-        if sample_base is None:
+        rc = N.lib().dr_render_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, sun.ctypes.data,
+                                    sky.ctypes.data)
+        if sample_base is None and rc in (N.DR_OK, N.DR_ERR_GAVE_UP):
             self.sample_base += spp
+        try:
+            N.check(rc)
+        except N.DrGaveUp as e:
+            e.result = (sun, sky)  # written, but with some paths cut short
+            raise
         return sun, sky
 
     def render_shadow_tile(self, x0: int, y0: int, tw: int, th: int, spp: int, seed: int = 0,
@@ -215,9 +220,14 @@ class Renderer:
         the reference.  Returns (shadow, zeros): the reference writes phb[0] only."""
         base = self.sample_base if sample_base is None else int(sample_base)
         out = np.zeros((th, tw, 4), np.float32)
-        N.check(N.lib().dr_shadow_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, out.ctypes.data))
-        if sample_base is None:
+        rc = N.lib().dr_shadow_tile(self._ctx, x0, y0, tw, th, spp, int(seed), base, out.ctypes.data)
+        if sample_base is None and rc in (N.DR_OK, N.DR_ERR_GAVE_UP):
             self.sample_base += spp
+        try:
+            N.check(rc)
+        except N.DrGaveUp as e:
+            e.result = (out, np.zeros_like(out))
+            raise
         return out, np.zeros_like(out)
 
     def shadow_tile_async(self, x0, y0, tw, th, spp, seed, sample_base, out_dev_ptr: int, stream_ptr: int = 0):
@@ -232,6 +242,15 @@ class Renderer:
 
     def synchronize(self):
         N.check(N.lib().dr_synchronize(self._ctx))
+
+    def check_complete(self, stream_ptr: int = 0):
+        """Waits for the stream (0: the context's) and raises DrGaveUp if paths of
+        the asynchronous calls since the last check were cut short."""
+        N.check(N.lib().dr_check_complete(self._ctx, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def set_step_budget(self, steps: int = 0):
+        """Tracking steps a path segment may take before it gives up (0: 2^24)."""
+        N.check(N.lib().dr_set_step_budget(self._ctx, int(steps)))
 
     def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
                    tile: int = 0, visits: int = 0, steps: int = 0):

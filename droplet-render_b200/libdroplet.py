@@ -71,6 +71,7 @@ _scene_built = False
 _build_error = None
 _job = None               # dict describing the parsed scene
 _tile = None              # (sun, sky) arrays of the last Render/Shadow call
+_tile_error = None        # why the last Render/Shadow call produced no complete tile
 _tile_size = (0, 0)
 _phase = None
 _sky_dataset = None
@@ -304,7 +305,7 @@ def BeginRender(scene, data, tilex, tiley, w, h, smask):
 
 
 def _tile_worker(kind, x0, y0, tw, th, samples):
-    global _tile, _tile_size, _state, _build_error
+    global _tile, _tile_size, _state, _build_error, _tile_error
     try:
         if kind == "render":
             sun, sky = _renderer.render_tile(x0, y0, tw, th, samples)
@@ -313,9 +314,10 @@ def _tile_worker(kind, x0, y0, tw, th, samples):
         with _lock:
             _tile = (sun.reshape(-1, 4), sky.reshape(-1, 4))
             _tile_size = (tw, th)
-    except Exception as e:
+    except Exception as e:  # QueryResult raises it (a partial tile is not returned as if complete)
         with _lock:
             _build_error = f"{type(e).__name__}: {e}"
+            _tile_error = _build_error
             _tile = None
     finally:
         with _lock:
@@ -323,7 +325,7 @@ def _tile_worker(kind, x0, y0, tw, th, samples):
 
 
 def _start_tile(kind, x0, y0, tilew, tileh, samples):
-    global _state
+    global _state, _tile_error
     for v in (x0, y0, tilew, tileh, samples):
         if not isinstance(v, (int, np.integer)) or v < 0:
             _fail("invalid arguments")
@@ -335,6 +337,7 @@ def _start_tile(kind, x0, y0, tilew, tileh, samples):
         if _state != ENGINE_STATE_READY:
             return None
         _state = ENGINE_STATE_PROCESSING
+        _tile_error = None
     threading.Thread(target=_tile_worker, args=(kind, x0, y0, tilew, tileh, samples), daemon=True).start()
     return None
 
@@ -359,13 +362,15 @@ def QueryResult(bindex):
             return None
         if not isinstance(bindex, (int, np.integer)) or bindex not in (0, 1):
             _fail("invalid arguments")
+        if _tile_error is not None:
+            _fail(f"the last Render/Shadow call failed: {_tile_error}")
         if _tile is None:
             return []
         return _tile[bindex].tolist()
 
 
 def EndRender():
-    global _renderer, _job, _tile, _scene_built, _state, _build_error
+    global _renderer, _job, _tile, _scene_built, _state, _build_error, _tile_error
     with _lock:
         if _renderer is not None:
             _renderer.close()
@@ -374,5 +379,6 @@ def EndRender():
         _tile = None
         _scene_built = False
         _build_error = None
+        _tile_error = None
         _state = ENGINE_STATE_READY
     return None

@@ -28,7 +28,9 @@ extern "C" {
 #define DR_ERR_CUDA (-2)      /* CUDA runtime failure (message has the CUDA error) */
 #define DR_ERR_STATE (-3)     /* call out of order (no scene, no parameters, busy) */
 #define DR_ERR_NOMEM (-4)     /* host or device allocation failed */
-#define DR_ERR_GAVE_UP (-5)   /* a kernel hit its iteration budget and stopped */
+#define DR_ERR_GAVE_UP (-5)   /* some paths hit an iteration budget and were cut short: the outputs
+                                  are written but incomplete (dr_render_tile, dr_shadow_tile,
+                                  dr_check_complete) */
 #define DR_ERR_NODEVICE (-6)  /* no CUDA device */
 
 #define DR_NONE 0xffffffffu
@@ -115,7 +117,8 @@ typedef struct {
     uint64_t node_visits;      /* octree node records examined */
     uint64_t density_lookups;  /* trilinear brick lookups */
     uint64_t mie_evals;        /* phase table evaluations and samples */
-    uint64_t gave_up;          /* paths stopped by the iteration budget */
+    uint64_t gave_up;          /* path segments cut by the step budget, plus blocks whose table
+                                  staging timed out (and so rendered nothing) */
 } dr_counters;
 
 typedef struct dr_ctx dr_ctx;
@@ -193,7 +196,9 @@ int dr_sky_cook(const double *const dataset_rgb[3], const double *const dataset_
  * each.  As in the reference only the even part of an odd tile is rendered
  * (2x2 pixel blocks); pixels outside the image or not rendered are 0.
  * Path (pixel p = py*w + px, sample s) draws from stream (seed, p, sample_base + s).
- * Blocking; host buffers. */
+ * Blocking; host buffers.  Returns DR_ERR_GAVE_UP, with the tiles written,
+ * when some of the call's paths were cut short by an iteration budget (the
+ * reference has no budget: it renders every path to its end). */
 int dr_render_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                    uint64_t sample_base, float *sun_out, float *sky_out);
 /* Same on device buffers, enqueued on stream (NULL = context stream); returns
@@ -207,7 +212,8 @@ int dr_render_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uin
  * sun(lrd)/colour for segments that escape (pixels without such geometry count
  * every sample as lit).  Alpha is +inf, as in the reference (its division by
  * float4::load(&colour) has w = 0).  Sample s of pixel p draws from stream
- * (seed, p, sample_base + s).  Blocking; host buffer. */
+ * (seed, p, sample_base + s).  Blocking; host buffer; DR_ERR_GAVE_UP as for
+ * dr_render_tile. */
 int dr_shadow_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                    uint64_t sample_base, float *out);
 int dr_shadow_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp,
@@ -215,6 +221,23 @@ int dr_shadow_tile_async(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uin
 
 /* Waits for all work on the context stream. */
 int dr_synchronize(dr_ctx *ctx);
+
+/* Give-up report for the calls that return before their work ends
+ * (dr_render_tile_async, dr_shadow_tile_async, dr_batch_launch,
+ * dr_adjoint_tile_async, ...).  Waits for `stream` (NULL = the context stream)
+ * and the context stream, then returns DR_ERR_GAVE_UP if the context's
+ * gave_up counter rose since the previous check (or dr_reset_counters), i.e.
+ * some path segment hit the tracking-step budget or some block timed out
+ * staging its tables; the outputs are then incomplete.  Give-ups that a
+ * blocking call already reported are not reported again.  No reference
+ * counterpart: the reference has no budgets. */
+int dr_check_complete(dr_ctx *ctx, void *stream);
+
+/* Tracking steps (null collisions) a path segment may take before it gives up
+ * (0 = the default, 2^24).  Applies to the context's parameters and to batches
+ * created afterwards.  No reference counterpart (the reference loops until
+ * the segment ends); a small budget makes give-ups reproducible in tests. */
+int dr_set_step_budget(dr_ctx *ctx, uint32_t steps);
 
 /* ---- launch shape (no reference counterpart: the reference schedules 2x2
  * pixel blocks with TBB, src/kernel.cpp:453) ------------------------------- */
@@ -362,8 +385,10 @@ int dr_probe_transmittance(dr_ctx *ctx, const float *ro, const float *rd, uint32
  * process exits.  Larger batches are rejected with DR_ERR_INVALID.
  *
  * The first call on a device looks up the array's address and caches it, so
- * make that first call before any stream capture.  All calls share the array,
- * so calls that overlap on the GPU race.
+ * make that first call before any stream capture.  The cached address belongs
+ * to the device's primary context: do not reset the device (cudaDeviceReset,
+ * or a primary-context reset by the application) while the library is loaded.
+ * All calls share the array, so calls that overlap on the GPU race.
  *
  * The work is enqueued on `stream` (NULL = the context stream) and the call
  * returns without waiting. */
