@@ -12,4 +12,4 @@ Two checkers live here:
     (oracle/port/*.c), which also holds the OpenVDB-free scene build and the
     FP64 quadrature references.
 """
-from .oracle import Port, Reference, ref_available, port_available  # noqa: F401
+from .oracle import Port, Reference, ref_available, port_available, reference_src  # noqa: F401

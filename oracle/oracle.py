@@ -14,6 +14,19 @@ NODE_DTYPE = np.dtype([("ce", "<f4", 4), ("chn", "<u4", 8), ("volx", "<u4", 2), 
 assert NODE_DTYPE.itemsize == 64
 
 
+def reference_src() -> str:
+    """Directory of the reference's sources: $DROPLET_REFERENCE_SRC, else the
+    `REF ?=` default of oracle/Makefile (the recipe that compiles them)."""
+    env = os.environ.get("DROPLET_REFERENCE_SRC")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    raise RuntimeError("oracle/Makefile has no REF default")
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 

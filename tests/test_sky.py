@@ -7,7 +7,9 @@ import pytest
 from conftest import golden
 from droplet_b200 import sky
 
-DATASET = "/root/reference/src/ArHosekSkyModelData_RGB.h"
+from oracle import reference_src
+
+DATASET = os.path.join(reference_src(), "ArHosekSkyModelData_RGB.h")
 
 
 @pytest.fixture(scope="module")

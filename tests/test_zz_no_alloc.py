@@ -6,8 +6,9 @@ cannot absorb the synchronisation cudaMalloc/cudaFree can cause.  The caller
 supplies device buffers for the rays and the result; the library's per-ray
 counters live in a fixed device array.
 
-The test calls it through the C ABI twice in a row and checks each result
-against the existing entry point (dr_probe_transmittance) on the same rays and
+The test calls it through the C ABI twice in a row on the caller's torch
+stream, then once on the context's own stream, and checks each result against
+the existing entry point (dr_probe_transmittance) on the same rays and random
 streams.  Both count the same delta-tracked samples, so the tolerance is the
 transmittance test's 1e-4 relative (they agree exactly in practice).  The
 second call also shows that a call clears the counters the previous one left.
@@ -27,7 +28,7 @@ def test_noalloc_transmittance_matches_existing_entry_point():
     import torch
 
     from droplet_b200 import _native as N
-    from droplet_b200.renderer import Renderer
+    from droplet_b200.renderer import Renderer, stream_handle
     from droplet_b200.scene import Octree
 
     nodes, bricks, mlevel = golden_octree()
@@ -48,14 +49,30 @@ def test_noalloc_transmittance_matches_existing_entry_point():
 
         ro_d = torch.as_tensor(ro, device="cuda").contiguous()
         rd_d = torch.as_tensor(rd, device="cuda").contiguous()
+        # Two calls in a row on the caller's own stream (the entry point's main
+        # use): the fills below are queued on that stream too, so they come
+        # before the clear / track / finish kernels of the call.
+        ts = torch.cuda.current_stream()
         for _ in range(2):
             out_d = torch.full((n,), -1.0, dtype=torch.float64, device="cuda")
             rc = N.lib().dr_transmittance_noalloc(r.handle, C.c_void_p(ro_d.data_ptr()), C.c_void_p(rd_d.data_ptr()),
-                                                  n, nsamp, seed, C.c_void_p(out_d.data_ptr()), None)
+                                                  n, nsamp, seed, C.c_void_p(out_d.data_ptr()),
+                                                  C.c_void_p(stream_handle(ts)))
             N.check(rc)
-            r.synchronize()
+            ts.synchronize()
             got = out_d.cpu().numpy()
             assert np.allclose(got, expected, rtol=1e-4, atol=0.0), np.abs(got - expected).max()
+
+        # One call on the context's own stream (NULL): torch's fill must have
+        # finished before it starts, so synchronise the device first.
+        out_d = torch.full((n,), -1.0, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        rc = N.lib().dr_transmittance_noalloc(r.handle, C.c_void_p(ro_d.data_ptr()), C.c_void_p(rd_d.data_ptr()),
+                                              n, nsamp, seed, C.c_void_p(out_d.data_ptr()), None)
+        N.check(rc)
+        r.synchronize()
+        got = out_d.cpu().numpy()
+        assert np.allclose(got, expected, rtol=1e-4, atol=0.0), np.abs(got - expected).max()
 
         too_many = N.DR_NOALLOC_MAX_RAYS + 1
         rc = N.lib().dr_transmittance_noalloc(r.handle, C.c_void_p(ro_d.data_ptr()), C.c_void_p(rd_d.data_ptr()),
