@@ -41,6 +41,11 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 W_IMG, H_IMG, SPP = 1920, 1080, 64
 METRIC = "path-vertices/s (plain renderer, single large cumulus 512^3, 1920x1080, 64 spp)"
 CPU_CROP = 384  # reference / cpu_baseline sample: centre crop at full spp (about 10 s of 16 cores)
+TRAVERSALS = {0: "octree stack traversal (local memory)", 1: "leaf-grid cell walk",
+              2: "octree stack traversal (shared memory)"}
+PHASE_SAMPLER = ("the reference's Mie sampler (src/KernelSampler.cpp:258-273: interpolated scan of the red CDF), "
+                 "reproduced for image parity; it fails a chi-square test against its own table (the last two "
+                 "theta bins are never drawn); DR_PHASE_MIE_EXACT is the sampler that passes")
 
 
 def log(*a):
@@ -357,6 +362,148 @@ def port_vertices(nodes, bricks, cfg, threads: int) -> int:
     return cnt["vertices"]
 
 
+def c0_settings(pdf, cdf, cfgs, rads, w: int = 256, h: int = 256):
+    """Config 0: the 64^3 puff (sigma_t 20, albedo 0.99, 8 events) seen by the
+    standard camera at w x h; returns (render configuration dict, settings)."""
+    from droplet_b200.renderer import PhaseTable, RenderSettings
+    from droplet_b200.sky import SkyState
+
+    sd = cam.sun_direction(W.SUN["elevation"], W.SUN["azimuth"])
+    eye = cam.orbit_eye(W.CENTER, W.CAMERA["distance"], W.CAMERA["azimuth"], W.CAMERA["elevation"])
+    viewi, proji = cam.camera_matrices(eye, W.CENTER, W.CAMERA["fov"], w, h)
+    ss, sa, ev = W.medium("c0")
+    cfg = dict(sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=sd, sun_color=np.asarray(W.SUN["color"], np.float32),
+               sun_angle=W.SUN["angle"], turbidity=W.SKY["turbidity"], ground_albedo=W.SKY["albedo"],
+               sky_configs=cfgs, sky_radiances=rads, mie_pdf=pdf, mie_cdf=cdf, viewi=viewi, proji=proji, w=w, h=h)
+    st = RenderSettings(sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=sd, sun_color=cfg["sun_color"],
+                        sun_angle=W.SUN["angle"], sky=SkyState(cfgs, rads), phase=PhaseTable(pdf, cdf), viewi=viewi,
+                        proji=proji, w=w, h=h)
+    return cfg, st
+
+
+def measure_c0(r, pdf, cdf, cfgs, rads, steps: int, warmup: int, cpu: bool, cpu_runs: int = 3):
+    """Config 0 timed in full on both sides (the reference's CPU-runnable case):
+    the 256x256 frame at 16 spp, 8 events.
+      * GPU kernel: CUDA events around each frame on the renderer's stream
+        (device buffers; the 256 MB L2 flush before each frame);
+      * GPU end to end: dr_render_tile with host buffers (parameters uploaded,
+        render, both tiles copied back), host clock;
+      * reference CPU: RenderKernel::Render over the whole frame (oracle/_ref,
+        all host threads), host clock; its vertex count is the GPU's count on
+        the same frame (the same estimator; the reference is not instrumented);
+      * seconds to 1% relative RMSE against the reference's converged frame
+        (tests/golden/ref_c0_converged_256.npz: two 32768-spp reference
+        renders, their noise removed): error e16 of a 16-spp frame, spp
+        needed n* = 16 (e16 / 0.01)^2 (MSE falls as 1/spp), checked by a GPU
+        render at n* spp; the CPU's n* comes from its own timed frames."""
+    import torch
+
+    from droplet_b200 import autotune
+    from droplet_b200.scene import build_octree
+
+    z = np.load(os.path.join(GOLDEN, "c0_octree.npz"))
+    oc = build_octree(z["block_origin"], z["block_values"], 1.0 / 64, 12)
+    cfg, st = c0_settings(pdf, cdf, cfgs, rads)
+    spp, w, h = 16, 256, 256
+    saved = r.get_tuning()
+    r.upload(oc)
+    r.set_params(st)
+    best, _ = autotune.tune(r, (0, 0, w, h), spp, key="c0", use_cache=False)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sun = torch.empty((h, w, 4), device="cuda")
+    sky = torch.empty_like(sun)
+    with torch.cuda.stream(stream):
+        for k in range(warmup):
+            r.render_tile_async(0, 0, w, h, spp, 3, k * spp, sun.data_ptr(), sky.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    r.reset_counters()
+    ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r.render_tile_async(0, 0, w, h, spp, 3, (warmup + k) * spp, sun.data_ptr(), sky.data_ptr(),
+                                stream.cuda_stream)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+    cnt = r.counters()
+    verts = cnt["vertices"] / steps
+    kernel = verts / (np.mean(ms) / 1e3)
+    frame = (np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.float32))
+    r.render_tile(0, 0, w, h, 1, seed=3, sample_base=0, out=frame)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        r.set_params(st)
+        r.render_tile(0, 0, w, h, spp, seed=3, sample_base=(warmup + k) * spp, out=frame)
+    e2e_s = (time.perf_counter() - t0) / steps
+
+    g = np.load(os.path.join(GOLDEN, "ref_c0_converged_256.npz"))
+    R = g["mean"].astype(np.float64)
+    ok = g["finite"]
+    noise = float(np.asarray(g["noise_mse"]).reshape(-1)[0])
+    scale = float((R[ok] ** 2).mean())
+
+    def rel(X):
+        m = ok & np.isfinite(X)
+        return float(np.sqrt(max(float(((X - R)[m] ** 2).mean()) - noise, 0.0) / scale))
+
+    def gpu_image(n, seed):
+        acc = np.zeros((h, w, 3))
+        done = 0
+        while done < n:
+            k = min(4096, n - done)
+            a, b = r.render_tile(0, 0, w, h, k, seed=seed, sample_base=done)
+            acc += (a + b)[..., :3]
+            done += k
+        return acc / n
+
+    e16 = float(np.mean([rel(gpu_image(spp, 9100 + i)) for i in range(4)]))
+    n_star = int(np.ceil(spp * (e16 / 0.01) ** 2))
+    check = rel(gpu_image(n_star, 9200)) if n_star <= 1 << 20 else None
+    out = {
+        "workload": "c0: 64^3 puff (seed 1), sigma_t 20, albedo 0.99, 8 events, 256x256 at 16 spp, whole frame",
+        "same_config": True, "tuning": list(best),
+        "gpu": {"value": kernel, "unit": "vertices/s", "ms_per_frame": float(np.mean(ms)), "launch_ms": ms,
+                "vertices_per_frame": verts, "paths_per_frame": cnt["paths"] / steps},
+        "gpu_e2e": {"value": verts / e2e_s, "unit": "vertices/s", "ms_per_frame": e2e_s * 1e3,
+                    "h2d_bytes_per_step": int(pdf.nbytes / 3 * 4 + cdf.nbytes / 3 + 16 * 4 * 2 + 64),
+                    "d2h_bytes_per_step": 2 * w * h * 16},
+        "seconds_to_1pct_rmse": {
+            "reference_image": "mean of 2 x 32768-spp reference (oracle/_ref) renders, noise removed "
+                               "(tests/golden/ref_c0_converged_256.npz)",
+            "reference_noise_rel": float(np.sqrt(noise / scale)), "rmse_at_16spp_gpu": e16, "spp_needed": n_star,
+            "check_rmse_at_spp_needed": check, "gpu_seconds": n_star / spp * float(np.mean(ms)) / 1e3,
+            "gpu_e2e_seconds": n_star / spp * e2e_s},
+    }
+    if cpu:
+        from oracle import Reference
+
+        threads = os.cpu_count() or 1
+        ref = Reference()
+        ref.set_threads(threads)
+        rs = ref.scene(oc.nodes, oc.bricks)
+        rs.render(cfg, 96, 96, 16, 16, spp)  # warm-up
+        times, errs = [], []
+        for _ in range(cpu_runs):
+            t = time.perf_counter()
+            a, b = rs.render(cfg, 0, 0, w, h, spp)
+            times.append(time.perf_counter() - t)
+            errs.append(rel((a + b)[..., :3].astype(np.float64) / spp))
+        cpu_s = float(np.mean(times))
+        cpu_n = int(np.ceil(spp * (float(np.mean(errs)) / 0.01) ** 2))
+        out["reference_cpu"] = {"value": verts / cpu_s, "unit": "vertices/s", "cores": threads, "kind": "reference",
+                                "s_per_frame": cpu_s, "frame_s": times,
+                                "sample": "the whole 256x256 frame at 16 spp per run (RenderKernel::Render)"}
+        out["seconds_to_1pct_rmse"].update({"rmse_at_16spp_cpu": float(np.mean(errs)), "spp_needed_cpu": cpu_n,
+                                            "cpu_seconds": cpu_n / spp * cpu_s})
+        out["gpu_over_reference"] = {"kernel": kernel / (verts / cpu_s), "e2e": (verts / e2e_s) / (verts / cpu_s)}
+    r.set_tuning(*saved)
+    return out
+
+
 def c3_views(pdf, cdf, cfgs, rads, n_views: int = 16, side: int = 256):
     """The inverse-rendering workload's views: the config-0 camera and sun at
     n_views evenly spaced azimuths."""
@@ -640,7 +787,8 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
     achieved = b_v * plain / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "algorithmic_bytes_per_vertex": b_v,
-                "calibration": "counters of the timed frames" + ("" if best[3] == 0 else " (cell walk: grid cells)")}
+                "calibration": "counters of the timed frames, " + TRAVERSALS.get(best[3], f"traversal {best[3]}")
+                               + (" (node visits are grid cells)" if best[3] == 1 else "")}
     bt = Batch(r, [oc], [BatchView(0, big, spp, 11, (x0, y0, 1920, 1080)) for (x0, y0) in tiles])
     bt.set_tuning(*best)
     for _ in range(warmup):
@@ -930,6 +1078,18 @@ def run_b200(args):
         except Exception as e:  # the reference oracle needs oracle/_ref
             cpu = {"value": None, "unit": "vertices/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    c0 = None
+    if rank == 0 and world == 1 and not args.no_c0:
+        c0 = measure_c0(r, pdf, cdf, cfgs, rads, steps=max(3, args.steps), warmup=max(3, args.warmup),
+                        cpu=not args.no_cpu)
+        r.upload(Octree(nodes, bricks, mlevel))
+        r.set_params(settings)
+        log(f"c0: gpu {c0['gpu']['value'] / 1e9:.3f} G/s ({c0['gpu']['ms_per_frame']:.3f} ms/frame), "
+            f"e2e {c0['gpu_e2e']['value'] / 1e9:.3f} G/s, cpu "
+            f"{(c0.get('reference_cpu') or {}).get('value', float('nan')) / 1e6:.2f} M/s; s to 1%: gpu "
+            f"{c0['seconds_to_1pct_rmse']['gpu_seconds']:.3f}, cpu "
+            f"{c0['seconds_to_1pct_rmse'].get('cpu_seconds', float('nan')):.1f}")
+
     rmse = None
     if rank == 0 and world == 1 and not args.no_rmse:
         rmse = seconds_to_rmse(r, stream, (X0, Y0, TW, TH), t_local / args.steps * 1e3)
@@ -968,7 +1128,7 @@ def run_b200(args):
                        "spp": SPP, "scattevs": 64, "sigma_t": 60.0, "albedo": 0.999, "leaves": int(len(bricks)),
                        "nodes": int(len(nodes)), "octree_depth": int(mlevel), "occupancy": occ,
                        "l2": "flushed between steps (256 MB write)", "region": [X0, Y0, TW, TH],
-                       "tuning": tuning},
+                       "tuning": tuning, "phase_sampler": PHASE_SAMPLER},
             "e2e": {"value": e2e_value, "unit": "vertices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "gpu_launches": args.steps,
@@ -976,6 +1136,7 @@ def run_b200(args):
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "seconds_to_1pct_rmse": rmse,
+            "c0": c0,
             "batched": batched,
             "adjoint": adjoint,
             "large_sparse": large,
@@ -1002,6 +1163,7 @@ def main():
     ap.add_argument("--no-rmse", action="store_true", help="skip the seconds-to-1%%-RMSE measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the inverse-rendering (adjoint) measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the large sparse scene (config 4)")
+    ap.add_argument("--no-c0", action="store_true", help="skip the config-0 whole-frame section")
     ap.add_argument("--profile-large", type=int, default=0,
                     help="profiling case only: an NxN centre crop of the config-4 frame, 3 launches")
     ap.add_argument("--fd-groups", type=int, default=8, help="seed groups of the finite-difference check")

@@ -22,6 +22,12 @@ Fixtures (all produced by the reference, none hand-written):
                            lookups (SampleVoxelSpace) on fixed inputs
   ref_c0_images.npz        two independent reference renders of config 0 at
                            128x128, 65536 spp (sums), for the image parity gate
+  ref_c0_converged_256.npz the converged config-0 frame (256x256) for the
+                           seconds-to-1%-RMSE measurement: the mean R of two
+                           independent 32768-spp reference renders A and B,
+                           as (sun + sky) rgb per sample, and their noise
+                           MSE(A, B) / 4 (`python tests/golden/make_golden.py
+                           c0conv` writes this file alone)
 """
 from __future__ import annotations
 
@@ -66,10 +72,36 @@ def sky_by_degree(ref: Reference):
         json.dump(states, f)
 
 
+def c0_converged(ref: Reference, spp: int = 32768):
+    pdf, cdf = ref.mie_tables()
+    w = h = 256
+    cfg = c0_config(ref, w, h, pdf, cdf)
+    z = np.load(os.path.join(HERE, "c0_octree.npz"))
+    rs = ref.scene(z["nodes"].view(np.dtype([("ce", "<f4", 4), ("chn", "<u4", 8), ("volx", "<u4", 2),
+                                             ("qval", "<f4", 2)])).reshape(-1), z["bricks"])
+    ref.set_threads(0)
+    t = time.time()
+    imgs = []
+    for _ in range(2):
+        sun, sky = rs.render(cfg, 0, 0, w, h, spp)
+        imgs.append(((sun + sky)[..., :3].astype(np.float64) / spp))
+    A, B = imgs
+    ok = np.isfinite(A) & np.isfinite(B)
+    R = 0.5 * (A + B)
+    noise = float(((A - B)[ok] ** 2).mean()) / 4.0
+    print(f"c0 converged: 2 x {w}x{h}x{spp} reference renders in {time.time() - t:.1f}s, "
+          f"noise rel {np.sqrt(noise / float((R[ok] ** 2).mean())):.2e}")
+    np.savez_compressed(os.path.join(HERE, "ref_c0_converged_256.npz"), mean=R.astype(np.float32), finite=ok,
+                        noise_mse=noise, spp=spp, w=w, h=h)
+
+
 def main():
     ref, port = Reference(), Port()
     if sys.argv[1:] == ["sky"]:
         sky_by_degree(ref)
+        return
+    if sys.argv[1:] == ["c0conv"]:
+        c0_converged(ref)
         return
     sky_by_degree(ref)
     pdf, cdf = ref.mie_tables()
