@@ -96,6 +96,10 @@ class Port:
         L.orc_optical_depth.argtypes = [C.POINTER(OrcScene), vp, vp, C.c_double]
         L.orc_optical_depth.restype = C.c_double
         L.orc_optical_depth_grad.argtypes = [C.POINTER(OrcScene), vp, vp, C.c_double, vp]
+        L.orc_single_scatter_sun.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), vp, vp, C.c_uint32, C.c_double,
+                                             C.c_uint32, C.c_uint32, vp, vp, vp]
+        L.orc_sun_hit_fraction.argtypes = [C.POINTER(OrcParams), C.c_uint32, C.c_uint32]
+        L.orc_sun_hit_fraction.restype = C.c_double
         L.orc_render_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                          C.c_uint64, C.c_uint64, vp, vp, C.POINTER(OrcCounters), C.c_int]
         L.orc_render_tile_mt.restype = C.c_int
@@ -376,6 +380,24 @@ class Port:
         grad = np.zeros(S.n_leaves * 512, np.float64)
         self.L.orc_optical_depth_grad(C.byref(S), _p(ro), _p(rd), tmax, _p(grad))
         return grad.reshape(-1, 512)
+
+    def single_scatter_sun(self, S, P, ro, rd, wc=(1.0, 1.0, 1.0), grad=True, nu=4, nphi=8, p_hit=None):
+        """FP64 quadrature of the expected sun sum of one path sample per camera
+        ray with scattevs = 1 (out (n, 3)), and d(sum_r sum_c wc_c out[r, c])/d
+        brick sample (n_leaves, lvoxc^3) when grad (port/fp64.c)."""
+        ro = np.ascontiguousarray(ro, np.float32).reshape(-1, 3)
+        rd = np.ascontiguousarray(rd, np.float32).reshape(-1, 3)
+        if p_hit is None:
+            p_hit = self.sun_hit_fraction(P)
+        out = np.zeros((len(ro), 3), np.float64)
+        w = np.ascontiguousarray(wc, np.float64)
+        g = np.zeros((S.n_leaves, S.lvoxc ** 3), np.float64) if grad else None
+        self.L.orc_single_scatter_sun(C.byref(S), C.byref(P), _p(ro), _p(rd), len(ro), float(p_hit), nu, nphi, _p(w),
+                                      _p(out), None if g is None else _p(g))
+        return out, g
+
+    def sun_hit_fraction(self, P, n1=2048, n2=512):
+        return float(self.L.orc_sun_hit_fraction(C.byref(P), n1, n2))
 
     def optical_depth(self, S, ro, rd, tmax=1e30):
         ro = np.ascontiguousarray(ro, np.float64)

@@ -133,6 +133,11 @@ void orc_camera_ray(const orc_params *P, uint32_t px, uint32_t py, float ro[3], 
 /* Optical depth integral of the brick density along ro + t rd, t in [0, tmax],
  * leaf by leaf, exact Gauss-Legendre on every brick-cell segment. */
 double orc_optical_depth(const orc_scene *S, const double ro[3], const double rd[3], double tmax);
+/* FP64 quadrature of the single-scatter (scattevs = 1) sun image and its
+ * brick gradient: the adjoint's independent check (fp64.c). */
+void orc_single_scatter_sun(const orc_scene *S, const orc_params *P, const float *ro, const float *rd, uint32_t n_rays,
+                            double p_hit, uint32_t nu, uint32_t nphi, const double wc[3], double *out, double *grad);
+double orc_sun_hit_fraction(const orc_params *P, uint32_t n1, uint32_t n2);
 
 /* ---- estimator ----------------------------------------------------------- */
 /* Free-flight tracking of one segment (src/kernel.cpp:197-317, fog leaves).
