@@ -210,6 +210,7 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
         tiles_v += r.counters()["vertices"]
     tiles = tiles_v / t_tiles
     b.close()
+    small = measure_small_views(r, scenes, settings, views, best, stream, flush, steps, warmup)
     r.set_tuning(*saved)
     return {
         "workload": "8 fields (config-0 puffs, seeds 10-17, {64..512}^3, sigma_t U[10,80]) x 8 views "
@@ -219,11 +220,76 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
         "plain_per_view": {"value": plain, "ms": plain_ms, "launches": len(views)},
         "plain_addon_tiles_64": {"value": tiles, "seconds": t_tiles, "calls": n_tiles},
         "speedup_vs_plain_per_view": batched / plain, "speedup_vs_addon_tiles": batched / tiles,
+        "small_views": small,
         "tuning": {"choice": list(best), "seconds": round(t_tune, 2), "probe": "centre <=128^2 crops, 4 spp",
                    "top": [[c, round(m, 3)] for c, m in table[:6]]},
         "graph": "memset outputs -> persistent kernel over all views -> step counter", "build_s": round(t_build, 1),
         "l2": "flushed before each timed launch (256 MB write)",
     }
+
+
+def measure_small_views(r, scenes, settings, views, tuning, stream, flush, steps: int, warmup: int,
+                        max_paths: int = 1 << 21):
+    """The batch's small views (at most max_paths paths, side^2 x spp: a few
+    per lane of the persistent grid, 148 SMs x 8 blocks x 128 lanes; when fewer
+    than 4 are that small, the 8 views with the fewest paths): one batched
+    launch of just those views against one plain launch per view, both
+    device-timed.  A view that small leaves most lanes idle in the tail of a
+    launch of its own."""
+    import torch
+
+    from droplet_b200.renderer import Batch, BatchView
+
+    pick = [i for i, v in enumerate(views) if v["side"] ** 2 * v["spp"] <= max_paths]
+    rule = f"views of at most {max_paths} paths"
+    if len(pick) < 4:
+        pick = sorted(range(len(views)), key=lambda i: views[i]["side"] ** 2 * views[i]["spp"])[:8]
+        rule = "the 8 views with the fewest paths"
+    b = Batch(r, scenes, [BatchView(views[i]["field"], settings[i], views[i]["spp"], 100 + i) for i in pick])
+    b.set_tuning(*tuning)
+    for _ in range(max(1, warmup)):
+        b.launch(stream.cuda_stream)
+    stream.synchronize()
+    r.reset_counters()
+    ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b.launch(stream.cuda_stream)
+            e.record(stream)
+            e.synchronize()
+            ms.append(a.elapsed_time(e))
+    verts = r.counters()["vertices"] / steps
+    b.close()
+    batched = verts / (np.mean(ms) / 1e3)
+    r.set_tuning(*tuning)
+    side_max = max(views[i]["side"] for i in pick)
+    sun = torch.empty((side_max, side_max, 4), device="cuda")
+    sky = torch.empty_like(sun)
+    cur, plain_ms, plain_v = -1, 0.0, 0
+    for i in pick:
+        v = views[i]
+        if v["field"] != cur:
+            r.upload(scenes[v["field"]])
+            cur = v["field"]
+        r.set_params(settings[i])
+        r.reset_counters()
+        flush.fill_(1.0)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r.render_tile_async(0, 0, v["side"], v["side"], v["spp"], 100 + i, 0, sun.data_ptr(), sky.data_ptr(),
+                            stream.cuda_stream)
+        e.record(stream)
+        e.synchronize()
+        plain_ms += a.elapsed_time(e)
+        plain_v += r.counters()["vertices"]
+    plain = plain_v / (plain_ms / 1e3)
+    return {"rule": rule, "views": len(pick), "paths": int(sum(views[i]["side"] ** 2 * views[i]["spp"] for i in pick)),
+            "batched": {"value": batched, "unit": "vertices/s", "ms": float(np.mean(ms))},
+            "plain_per_view": {"value": plain, "unit": "vertices/s", "ms": plain_ms},
+            "speedup_vs_plain_per_view": batched / plain}
 
 
 class ClockSampler:
@@ -295,6 +361,34 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def kernel_source_sha16() -> str:
+    """Digest of the CUDA sources (droplet-render_b200/csrc): a profile summary
+    records the digest of the build it measured, so a stale one is detected."""
+    import hashlib
+
+    d = os.path.join(ROOT, "droplet-render_b200", "csrc")
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(d)):
+        if name.endswith((".cu", ".cuh", ".h", ".cpp")):
+            with open(os.path.join(d, name), "rb") as f:
+                h.update(name.encode() + b"\0" + f.read())
+    return h.hexdigest()[:16]
+
+
+def profile_lines(name: str) -> dict:
+    """`key: value` lines of a committed profile summary (profiles/<name>)."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if ":" in line and not line.startswith(("|", "#", " ", "*")):
+                    k, v = line.split(":", 1)
+                    out[k.strip()] = v.strip()
+    except OSError:
+        pass
+    return out
+
+
 def profiled_l2():
     """L2 figures of the render kernel from the committed ncu summary
     (profiles/render_persistent_kernel_c1.md, lines "l2_throughput_pct: X" and
@@ -313,17 +407,16 @@ def profiled_l2():
 
 
 def profiled_traffic():
-    """DRAM bytes per vertex of the render kernel from the committed ncu summary
-    (profiles/render_persistent_kernel_c1.md, line "dram_bytes_per_vertex: X")."""
-    p = os.path.join(ROOT, "profiles", "render_persistent_kernel_c1.md")
-    try:
-        with open(p) as f:
-            for line in f:
-                if line.startswith("dram_bytes_per_vertex:"):
-                    return {"dram_bytes_per_vertex": float(line.split(":")[1])}
-    except Exception:
-        pass
-    return None
+    """DRAM bytes of one full-frame render launch (dram__bytes_read.sum +
+    dram__bytes_write.sum) from the committed ncu summary
+    (profiles/render_persistent_kernel_c1.md, lines "dram_bytes_per_frame: X",
+    "frame_tuning: ..." and "source_sha16: ..."), used only when it measured
+    this build's sources."""
+    kv = profile_lines("render_persistent_kernel_c1.md")
+    if "dram_bytes_per_frame" not in kv:
+        return None
+    return {"bytes": float(kv["dram_bytes_per_frame"]), "source_sha16": kv.get("source_sha16"),
+            "tuning": kv.get("frame_tuning"), "current": kv.get("source_sha16") == kernel_source_sha16()}
 
 
 def cpu_reference_times(nodes, bricks, cfg, threads: int, steps: int = 1, warmup: int = 0):
@@ -1057,11 +1150,15 @@ def run_b200(args):
     avg_s = t_local / args.steps
     achieved = bytes_per_step / avg_s / 1e9
     traffic = profiled_traffic()
+    tuned = ",".join(str(v) for v in r.get_tuning())
+    usable = bool(traffic and traffic["current"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
-                "traffic": (traffic["dram_bytes_per_vertex"] * cnt["vertices"] / args.steps) if traffic else None,
-                "traffic_source": "ncu dram__bytes_read.sum + write.sum on a 512^2 crop launch, per vertex, scaled "
-                                  "by this frame's vertices (profiles/render_persistent_kernel_c1.md)",
+                "traffic": traffic["bytes"] if usable else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-frame launch "
+                                  "(profiles/render_persistent_kernel_c1.md)"
+                                  + (f"; captured at tuning {traffic['tuning']}, this run {tuned}" if usable else
+                                     "; not used: " + ("no capture" if not traffic else "captured on other sources")),
                 "algorithmic_bytes_per_vertex": b_v,
                 "calibration": "B_v from a 16-spp frame (seed 4242) with the octree stack traversal"}
     # the scene (23 MB of bricks) is L2-resident: the L2's own throughput as a
