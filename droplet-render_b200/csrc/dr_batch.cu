@@ -78,7 +78,6 @@ int build_graph(dr_batch *b) {
     B.scenes = b->scenes.p;
     B.begins = b->begins.p;
     B.n_views = (uint32_t)b->host_views.size();
-    B.n_scenes = (uint32_t)b->scenes.n;
     B.n_paths = b->n_paths;
     B.step = b->step.p;
     DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");

@@ -161,7 +161,6 @@ struct BatchArgs {
     const DevScene *scenes;
     const uint64_t *begins;
     uint32_t n_views;
-    uint32_t n_scenes;
     uint64_t n_paths;
     const unsigned long long *step;  // launches so far: view samples start at sample_base + step * spp
 };

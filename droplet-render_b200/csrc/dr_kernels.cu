@@ -597,27 +597,14 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     float ts[kMaxDepth][6];  // ancestors' intervals of the stack traversal (local memory)
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t mbar;
-    // BATCH: the scene records in shared memory (up to kSceneCache of them),
-    // so that a lane's traversal reads its scene's fields without a dependent
-    // global load through its view record
-    __shared__ __align__(16) DevScene sh_scenes[BATCH ? kSceneCache : 1];
     uint32_t mb;
     MieSmem M;
     uint64_t n_total, shift = 0;
-    const DevScene *scene_base = nullptr;
     if constexpr (BATCH) {
         mb = mie_bytes(B.views[0].P);
         M = mie_view(B.views[0].P, smem);
         n_total = B.n_paths;
         shift = *B.step;
-        scene_base = B.scenes;
-        if (B.n_scenes <= kSceneCache) {
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(B.scenes);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(sh_scenes);
-            const uint32_t words = B.n_scenes * (uint32_t)(sizeof(DevScene) / 4);
-            for (uint32_t i = threadIdx.x; i < words; i += kPersistentBlock) dst[i] = __ldg(src + i);
-            scene_base = sh_scenes;  // filled before stage_mie's barrier
-        }
     } else {
         mb = mie_bytes(P);
         M = mie_view(P, smem);
@@ -631,7 +618,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     uint32_t nstack[kMaxDepth];
     Trav slow[1];
     PathLane<WALK> L;
-    uint32_t view = 0, sidx = 0;
+    uint32_t view = 0;
     uint32_t state = staged ? kFetch : kDone;
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
     const uint32_t lane = threadIdx.x & 31u;
@@ -653,8 +640,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
                     if constexpr (BATCH) {
                         view = find_view(B, p);
                         const BatchView &V = B.views[view];
-                        sidx = V.scene;
-                        ok = start_path(L, p - V.begin, scene_base[sidx], V.P, V.A, shift * V.A.spp, cnt, paths,
+                        ok = start_path(L, p - V.begin, B.scenes[V.scene], V.P, V.A, shift * V.A.spp, cnt, paths,
                                         state, slow);
                     } else {
                         ok = start_path(L, p, S, P, A, 0ull, cnt, paths, state, slow);
@@ -669,7 +655,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         const bool events = ev && ((uint32_t)__popc(ev) >= event_batch || busy == 0);
         if constexpr (BATCH) {
             const BatchView &V = B.views[view];
-            lane_work<WALK, FEAT, SHS>(L, events, scene_base[sidx], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack,
+            lane_work<WALK, FEAT, SHS>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack,
                                       slow, visits, steps, ts, shcol, shlevels);
         } else {
             lane_work<WALK, FEAT, SHS>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits,

@@ -7,7 +7,6 @@ namespace dr {
 
 constexpr int kRenderBlock = 128;
 constexpr int kPersistentBlock = 128;
-constexpr uint32_t kSceneCache = 16;  // batch scene records a persistent block keeps in shared memory
 
 cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
