@@ -348,7 +348,7 @@ int make_tile_args(uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t 
 }
 
 bool valid_tuning(const dr_tuning *t) {
-    return t && t->kernel <= DR_KERNEL_POOLED && t->event_batch <= 32 && t->blocks_per_sm <= 64 &&
+    return t && t->kernel <= DR_KERNEL_PER_PATH && t->event_batch <= 32 && t->blocks_per_sm <= 64 &&
            t->traversal <= 2 && t->tile <= 64 && t->visits <= 255 && t->steps <= 255;
 }
 

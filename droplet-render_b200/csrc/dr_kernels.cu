@@ -453,12 +453,11 @@ __device__ __forceinline__ void scatter_event(PathLane<WALK> &L, const DevScene 
     L.seg = kSegShadow;
 }
 
-// Segment end without the next segment's start: light gathered, the path
-// finished (state becomes kFetch) or set up for its next segment.
+// Segment end: the body of path_sample() between two track() calls.
 template <bool WALK, uint32_t FEAT>
-__device__ __forceinline__ void path_event_core(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
-                                                const MieSmem &M, const TileArgs &A, float4 *sun_out,
-                                                float4 *sky_out, Count &cnt, uint32_t &state) {
+__device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
+                                        const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
+                                        uint32_t &state, Trav *slow) {
     if (L.seg == kSegShadow) {
         if (L.esc == kTrackEscaped && !((FEAT & kFeatOcc) && occluded(S, L.ro, L.rd))) {
             const bool hit = sun_hit(P, L.rd);
@@ -476,16 +475,8 @@ __device__ __forceinline__ void path_event_core(PathLane<WALK> &L, const DevScen
         L.seg = kSegMain;
     } else {
         scatter_event<WALK, FEAT>(L, S, P, M, A, sun_out, sky_out, cnt, state);
+        if (state == kFetch) return;
     }
-}
-
-// Segment end: the body of path_sample() between two track() calls.
-template <bool WALK, uint32_t FEAT>
-__device__ __forceinline__ void path_event(PathLane<WALK> &L, const DevScene &S, const DevParams &P, const MieSmem &M,
-                                        const TileArgs &A, float4 *sun_out, float4 *sky_out, Count &cnt,
-                                        uint32_t &state, Trav *slow) {
-    path_event_core<WALK, FEAT>(L, S, P, M, A, sun_out, sky_out, cnt, state);
-    if (state == kFetch) return;
     // one segment start for both kinds of event, so that lanes of a batch that
     // ended a shadow segment and lanes that scattered run it together
     L.depth = 3.402823466e+38f;
@@ -661,174 +652,6 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
             lane_work<WALK, FEAT, SHS>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits,
                                       steps, ts, shcol, shlevels);
         }
-    }
-    warp_sum_counts(cnt, C, paths);
-}
-
-// ---- persistent kernel with block-pooled events ---------------------------------
-// The warp-gated events above leave lanes idle while a warp waits for enough of
-// its lanes to need shading.  Here the four warps of a block run K iterations
-// of segment work (fetch, traversal, free-flight steps; no events), then meet
-// at a barrier: every lane whose segment ended copies its path record into a
-// block-wide pool in shared memory, the block's first threads shade one record
-// each (so the events of all four warps fill as few warps as possible), and
-// the owners read the results back and start their next segments.  The owner
-// keeps its lane throughout; only the event inputs and outputs travel.  Every
-// thread runs the same phases, so the barriers need no waits of their own.
-// Path results are those of the per-path estimator (the same draws in the
-// same order), as for the kernel above.
-constexpr uint32_t kRecWords = 33;   // words of a pooled path record
-constexpr uint32_t kPoolCap = 64;    // records per block and phase
-
-// Record layout (word w of record i at pool[w * kPoolCap + i]): 0 px | py << 16,
-// 1-4 the random stream, 5-7 ro, 8-10 rd, 11 td, 12-14 T, 15-18 sun, 19-22
-// sky, 23 r | seg << 16 | esc << 24 | finished << 31, 24-26 srd, 27-29 tn,
-// 30-32 sw.
-template <bool WALK>
-__device__ __forceinline__ void rec_store(const PathLane<WALK> &L, float *pool, uint32_t i, bool finished) {
-    uint32_t *u = reinterpret_cast<uint32_t *>(pool);
-    u[0 * kPoolCap + i] = L.px | (L.py << 16);
-    u[1 * kPoolCap + i] = (uint32_t)L.g.state;
-    u[2 * kPoolCap + i] = (uint32_t)(L.g.state >> 32);
-    u[3 * kPoolCap + i] = (uint32_t)L.g.inc;
-    u[4 * kPoolCap + i] = (uint32_t)(L.g.inc >> 32);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        pool[(5 + k) * kPoolCap + i] = L.ro[k];
-        pool[(8 + k) * kPoolCap + i] = L.rd[k];
-        pool[(12 + k) * kPoolCap + i] = L.T[k];
-        pool[(24 + k) * kPoolCap + i] = L.srd[k];
-        pool[(27 + k) * kPoolCap + i] = L.tn[k];
-        pool[(30 + k) * kPoolCap + i] = L.sw[k];
-    }
-    pool[11 * kPoolCap + i] = L.td;
-    pool[15 * kPoolCap + i] = L.sun.x;
-    pool[16 * kPoolCap + i] = L.sun.y;
-    pool[17 * kPoolCap + i] = L.sun.z;
-    pool[18 * kPoolCap + i] = L.sun.w;
-    pool[19 * kPoolCap + i] = L.sky.x;
-    pool[20 * kPoolCap + i] = L.sky.y;
-    pool[21 * kPoolCap + i] = L.sky.z;
-    pool[22 * kPoolCap + i] = L.sky.w;
-    u[23 * kPoolCap + i] = L.r | (L.seg << 16) | (L.esc << 24) | (finished ? 0x80000000u : 0u);
-}
-
-template <bool WALK>
-__device__ __forceinline__ bool rec_load(PathLane<WALK> &L, const float *pool, uint32_t i) {
-    const uint32_t *u = reinterpret_cast<const uint32_t *>(pool);
-    const uint32_t pp = u[0 * kPoolCap + i];
-    L.px = pp & 0xffffu;
-    L.py = pp >> 16;
-    L.g.state = (uint64_t)u[1 * kPoolCap + i] | ((uint64_t)u[2 * kPoolCap + i] << 32);
-    L.g.inc = (uint64_t)u[3 * kPoolCap + i] | ((uint64_t)u[4 * kPoolCap + i] << 32);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        L.ro[k] = pool[(5 + k) * kPoolCap + i];
-        L.rd[k] = pool[(8 + k) * kPoolCap + i];
-        L.T[k] = pool[(12 + k) * kPoolCap + i];
-        L.srd[k] = pool[(24 + k) * kPoolCap + i];
-        L.tn[k] = pool[(27 + k) * kPoolCap + i];
-        L.sw[k] = pool[(30 + k) * kPoolCap + i];
-    }
-    L.td = pool[11 * kPoolCap + i];
-    L.sun = make_float4(pool[15 * kPoolCap + i], pool[16 * kPoolCap + i], pool[17 * kPoolCap + i],
-                        pool[18 * kPoolCap + i]);
-    L.sky = make_float4(pool[19 * kPoolCap + i], pool[20 * kPoolCap + i], pool[21 * kPoolCap + i],
-                        pool[22 * kPoolCap + i]);
-    const uint32_t w = u[23 * kPoolCap + i];
-    L.r = w & 0xffffu;
-    L.seg = (w >> 16) & 0xffu;
-    L.esc = (w >> 24) & 0x7fu;
-    return (w >> 31) != 0u;
-}
-
-// knobs: bits 0-7 segment iterations per phase, 8-15 node visits per
-// traversal unit (0: to the next leaf), 16-23 free-flight steps per
-// iteration, 24-31 shared-memory stack entries.  The stack traversal with its
-// stack in shared memory; plain features only (no occluders, Hosek sky, Mie
-// phase, fog leaves); image sides and event limits below 65536.
-template <int MINB>
-__global__ void __launch_bounds__(kPersistentBlock, MINB) render_pooled_kernel(DevScene S, DevParams P, TileArgs A,
-                                                                         const void *mie_pack, float4 *sun_out,
-                                                                         float4 *sky_out, DevCounters *C,
-                                                                         WorkQueue *Q, uint32_t knobs) {
-    constexpr int kWarps = kPersistentBlock / 32;
-    const uint32_t K = (knobs & 0xffu) ? (knobs & 0xffu) : 4u, visits = (knobs >> 8) & 0xffu;
-    const uint32_t steps = ((knobs >> 16) & 0xffu) ? ((knobs >> 16) & 0xffu) : 1u;
-    const int shlevels = (int)(knobs >> 24);
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint64_t mbar;
-    __shared__ uint32_t warp_ev[kWarps];
-    const uint32_t mb = mie_bytes(P);
-    const MieSmem M = mie_view(P, smem);
-    const bool staged = stage_mie(mie_pack, mb, smem, &mbar);
-    float *const cols = reinterpret_cast<float *>(smem + ((mb + 15u) & ~15u));
-    float *const shcol = cols + threadIdx.x;
-    float *const pool = cols + (size_t)shlevels * 7 * kPersistentBlock;
-    Count cnt;
-    cnt.zero();
-    uint32_t paths = 0;
-    uint32_t nstack[kMaxDepth];
-    Trav slow[1];
-    float ts[1][6];
-    PathLane<false> L;
-    uint32_t state = staged ? kFetch : kDone;
-    if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    const unsigned FULL = 0xffffffffu;
-    for (;;) {
-        // segment work: fetch, traversal and free-flight steps
-        for (uint32_t k = 0; k < K; ++k) {
-            const uint32_t want = __ballot_sync(FULL, state == kFetch);
-            if (want) {
-                const uint32_t leader = __ffs(want) - 1;
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(&Q->next, (unsigned long long)__popc(want));
-                base = __shfl_sync(FULL, base, leader);
-                if (state == kFetch) {
-                    const uint64_t p = base + __popc(want & lt_mask);
-                    if (p >= A.n_paths) state = kDone;
-                    else if (!start_path(L, p, S, P, A, 0ull, cnt, paths, state, slow)) state = kFetch;
-                }
-            }
-            if (!__any_sync(FULL, state == kTrav || state == kStep || state == kFetch)) break;
-            lane_work<false, 0, true>(L, false, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits,
-                                      steps, ts, shcol, shlevels);
-        }
-        // events of the whole block, packed into the first threads
-        const uint32_t wv = __ballot_sync(FULL, state == kEvent);
-        if (lane == 0) warp_ev[warp] = __popc(wv);
-        __syncthreads();
-        uint32_t base = 0, total = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t c = warp_ev[w];
-            base += (uint32_t)w < warp ? c : 0u;
-            total += c;
-        }
-        const uint32_t rank = base + __popc(wv & lt_mask);
-        const bool exported = state == kEvent && rank < kPoolCap;
-        if (exported) rec_store(L, pool, rank, false);
-        const uint32_t n_ev = total < kPoolCap ? total : kPoolCap;
-        __syncthreads();
-        if (threadIdx.x < n_ev) {
-            PathLane<false> E;
-            rec_load(E, pool, threadIdx.x);
-            uint32_t st = kEvent;
-            path_event_core<false, 0>(E, S, P, M, A, sun_out, sky_out, cnt, st);
-            rec_store(E, pool, threadIdx.x, st == kFetch);
-        }
-        __syncthreads();
-        if (exported) {
-            if (rec_load(L, pool, rank)) {
-                state = kFetch;
-            } else {
-                L.depth = 3.402823466e+38f;
-                begin_segment(L, S, P.step_budget, cnt, state, slow);
-            }
-        }
-        if (__syncthreads_and(state == kDone)) break;
     }
     warp_sum_counts(cnt, C, paths);
 }
@@ -1640,55 +1463,13 @@ static uint32_t shared_stack_plan(Tuning &tune, uint32_t feat, uint32_t stack_le
     return 0;
 }
 
-using PooledFn = void (*)(DevScene, DevParams, TileArgs, const void *, float4 *, float4 *, DevCounters *, WorkQueue *,
-                         uint32_t);
-
-static PooledFn pooled_variant(uint32_t minb) {
-    if (minb >= 8) return render_pooled_kernel<8>;
-    if (minb >= 6) return render_pooled_kernel<6>;
-    return render_pooled_kernel<5>;
-}
-
-// The pooled-event kernel (kernel 2): frames with plain features, the stack in
-// shared memory, and records that fit their 16-bit fields; other frames take
-// the warp-gated kernel.
-static bool pooled_applies(const DevScene &S, const DevParams &P, uint32_t feat) {
-    return feat == 0 && S.stack_levels >= 1 && S.stack_levels <= kShStackMax && P.w < 65536u && P.h < 65536u &&
-           P.scattevs < 65536u;
-}
-
-static cudaError_t launch_pooled(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
-                                 float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q, const Tuning &tune,
-                                 int device, cudaStream_t st) {
-    const size_t smem = ((mie_smem(P) + 15) & ~(size_t)15) + (size_t)S.stack_levels * 7 * 4 * kPersistentBlock +
-                        (size_t)kRecWords * kPoolCap * 4;
-    int sms = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    const PooledFn fn = pooled_variant(tune.blocks_per_sm ? tune.blocks_per_sm : 6u);
-    int maxb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, kPersistentBlock, smem) != cudaSuccess || maxb < 1)
-        maxb = 1;
-    const int bps = tune.blocks_per_sm && (int)tune.blocks_per_sm < maxb ? (int)tune.blocks_per_sm : maxb;
-    const uint32_t knobs = (tune.event_batch ? (tune.event_batch > 255 ? 255u : tune.event_batch) : 4u) |
-                           ((tune.visits > 255 ? 255u : tune.visits) << 8) |
-                           ((tune.steps > 255 ? 255u : tune.steps) << 16) | (S.stack_levels << 24);
-    e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
-    if (e != cudaSuccess) return e;
-    fn<<<sms * bps, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q, knobs);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
                                      const Tuning &tune_in, int device, cudaStream_t st) {
     if (A.n_paths == 0) return cudaSuccess;
     size_t smem = mie_smem(P);
     const uint32_t feat = frame_features(S, P);
-    if (tune_in.kernel == 2u && pooled_applies(S, P, feat))
-        return launch_pooled(S, P, A, mie_pack, sun_out, sky_out, C, Q, tune_in, device, st);
     Tuning tune = tune_in;
-    if (tune.kernel == 2u) tune.traversal = 2u;  // the warp-gated kernel with the same stack
     const uint32_t shlevels = shared_stack_plan(tune, feat, S.stack_levels, smem);
     PersistentFn fn;
     int blocks;

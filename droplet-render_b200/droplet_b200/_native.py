@@ -30,9 +30,6 @@ DR_ENV_NONE = 1
 DR_ENV_MAP = 2
 DR_VERSION = 200  # include/droplet_b200.h: the struct layouts below
 DR_KERNEL_DEPTHCOMP = 0x1
-DR_KERNEL_PERSISTENT = 0
-DR_KERNEL_PER_PATH = 1
-DR_KERNEL_POOLED = 2
 DR_KERNEL_FINITE_PATHS = 0x2
 DR_KERNEL_EMBREE = 0x4
 

@@ -243,11 +243,6 @@ int dr_set_step_budget(dr_ctx *ctx, uint32_t steps);
  * pixel blocks with TBB, src/kernel.cpp:453) ------------------------------- */
 #define DR_KERNEL_PERSISTENT 0u  /* resident warps take paths from a queue (default) */
 #define DR_KERNEL_PER_PATH 1u    /* one thread per path sample */
-#define DR_KERNEL_POOLED 2u      /* persistent, with the events of a block's warps shaded together: every
-                                    event_batch iterations (0 = 4) the block pools its ended segments in
-                                    shared memory and shades them packed into its first warps (frames
-                                    without occluders, HG, environment maps or surface leaves; the stack
-                                    traversal in shared memory; others fall back to DR_KERNEL_PERSISTENT) */
 typedef struct {
     uint32_t kernel;         /* DR_KERNEL_* */
     uint32_t blocks_per_sm;  /* persistent kernel: resident blocks per SM, 0 = as many as fit */

@@ -11,8 +11,8 @@ tests/deep_configs.py; the fixtures come from the compiled reference
     reference traversers' bit for bit (any NaN matches any NaN);
   * GPU path samples of a 16x16 crop equal the CPU restatement's bit for bit
     with every traversal (octree stack in local or shared memory, cell walk,
-    one thread per path) and with the block-pooled events, the restatement
-    being pinned to the reference at these depths by tests/test_oracle_deep.py;
+    one thread per path), the restatement being pinned to the reference at
+    these depths by tests/test_oracle_deep.py;
   * 32x32 crops at 256 spp, 16 runs, per traversal: per-run sums over the crop
     and its 4x4 blocks of 8x8 pixels agree with the reference's 16 runs within
     Welch z 4.5 (crop) and 5 (blocks).
@@ -30,8 +30,7 @@ pytestmark = pytest.mark.gpu
 
 NAMES = ["c1", "c4"]
 # (kernel, blocks/SM, event batch, traversal, tile, visits, steps)
-TUNINGS = [(0, 8, 24, 2, 0, 3, 4), (0, 6, 24, 0, 0, 3, 2), (0, 5, 24, 1, 0, 0, 1), (1, 0, 0, 0, 0, 0, 0),
-           (2, 6, 4, 2, 0, 3, 4)]
+TUNINGS = [(0, 8, 24, 2, 0, 3, 4), (0, 6, 24, 0, 0, 3, 2), (0, 5, 24, 1, 0, 0, 1), (1, 0, 0, 0, 0, 0, 0)]
 
 
 def _i(a) -> int:

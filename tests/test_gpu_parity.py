@@ -351,7 +351,7 @@ def test_banded_host_render_equals_restatement(port):
     with Renderer(0) as r:
         r.upload(Octree(nodes, bricks, mlevel))
         r.set_params(settings_from_cfg(cfg))
-        for tuning in ((0, 5, 24, 0, 8), (0, 8, 24, 2, 0), (1, 0, 0, 0, 0), (2, 8, 4, 2, 0, 3, 4), (2, 5, 1, 2, 0, 0, 1)):
+        for tuning in ((0, 5, 24, 0, 8), (0, 8, 24, 2, 0), (1, 0, 0, 0, 0)):
             r.set_tuning(*tuning)
             r.reset_counters()
             sun, sky = r.render_tile(0, 0, 40, 601, 8, seed=77, sample_base=16)
@@ -387,7 +387,7 @@ def test_large_sparse_scene_recipe_paths_equal_restatement(port):
     with Renderer(0) as r:
         r.upload(oc)
         r.set_params(settings_from_cfg(cfg))
-        for tuning in ((0, 6, 20, 0, 0), (0, 8, 24, 2, 0, 3, 2), (1, 0, 0, 0, 0), (2, 6, 8, 2, 0, 3, 2)):
+        for tuning in ((0, 6, 20, 0, 0), (0, 8, 24, 2, 0, 3, 2), (1, 0, 0, 0, 0)):
             r.set_tuning(*tuning)
             r.reset_counters()
             sun, sky = r.render_tile(40, 20, 80, 50, 16, seed=4, sample_base=0)
