@@ -5,15 +5,17 @@ no likelihood-ratio algebra with the adjoint.
 
 Config 0 with one scattering event, a 16x16 crop of the 64x64 frame, loss
 L = sum over pixels and rgb of the sun sums per sample (dsun = 1/spp, dsky = 0).
-The adjoint runs 16 independent seed groups of 2048 spp (8.4 M paths); on the
-256 voxels of largest FP64 gradient each voxel's mean agrees within 2% plus 4
-standard errors, and the projection of the adjoint on the FP64 gradient is
-within 1% of it."""
+The adjoint runs 16 independent seed groups of 16384 spp (67 M paths).  The
+criteria are those of tests/test_single_scatter_fp64.py (where the reason for
+the density threshold is given): the projection of the mean adjoint on the FP64
+gradient's 256 largest entries within 2%; among voxels holding at least 1% of
+their leaf majorant, the 256 of largest gradient each within 2% plus 4 standard
+errors and their projection within 1%."""
 import numpy as np
 import pytest
 
 from conftest import settings_from_cfg
-from test_single_scatter_fp64 import crop_setup
+from test_single_scatter_fp64 import adjoint_vs_quadrature, crop_setup
 
 pytestmark = pytest.mark.gpu
 
@@ -28,7 +30,7 @@ def test_adjoint_matches_fp64_single_scatter_gradient(port):
     nodes, bricks, cfg, P, keep, ro, rd = crop_setup(port)
     S = port.scene(nodes, bricks)
     out, g64 = port.single_scatter_sun(S, P, ro, rd)
-    spp, groups = 2048, 16
+    spp, groups = 16384, 16
     n = 16
     with Renderer(0) as r:
         _, _, mlevel = golden_octree()
@@ -56,12 +58,7 @@ def test_adjoint_matches_fp64_single_scatter_gradient(port):
     # the forward image agrees with the quadrature (the model the gradient differentiates)
     fw = np.asarray(fw)
     assert abs(fw.mean() - out.sum()) < 4 * fw.std(ddof=1) / np.sqrt(groups) + 2e-3 * out.sum()
-    top = np.argsort(-np.abs(g64).ravel())[:256]
-    want = g64.ravel()[top]
-    got = G.reshape(groups, -1)[:, top]
-    m, se = got.mean(0), got.std(0, ddof=1) / np.sqrt(groups)
-    bad = np.abs(m - want) > 0.02 * np.abs(want) + 4 * se
-    assert bad.sum() == 0, (np.flatnonzero(bad)[:8], m[bad][:8], want[bad][:8], se[bad][:8])
-    proj = float(m @ want / (want @ want))
-    assert abs(proj - 1.0) < 0.01, proj
-    assert float(np.median(se / np.abs(want))) < 0.02  # the check resolves 2%
+    proj_all, bad, proj, rel_se = adjoint_vs_quadrature(g64, G.reshape(groups, -1), bricks, nodes)
+    assert abs(proj_all - 1.0) < 0.02, proj_all
+    assert bad == 0 and abs(proj - 1.0) < 0.01, (bad, proj)
+    assert rel_se < 0.02, rel_se  # the check resolves 2% per voxel

@@ -12,7 +12,19 @@ tests/test_gpu_adjoint_fp64.py):
   * the quadrature equals the estimator (the restatement's Monte Carlo render
     of the same crop, 8 independent runs) within 4 standard errors and 0.2%;
   * its gradient equals central differences of the quadrature itself on the
-    voxels of largest gradient (relative 1e-4)."""
+    voxels of largest gradient (relative 1e-4);
+  * the restatement's path-replay adjoint (the GPU adjoint's arithmetic, path
+    for path) against it: see adjoint_vs_quadrature.
+
+How the comparison reads.  The adjoint differentiates the probability of each
+delta-tracking decision: w/rho for a real collision, -w/(rho_max - rho) for a
+null one (w the voxel's trilinear weight).  Where the density is near zero a
+real collision is rare and its weight 1/rho is huge, so the estimate is
+unbiased but heavy-tailed: a finite sample misses the rare large terms.  So
+the per-voxel check (2% plus 4 standard errors) takes the voxels of largest
+gradient among those holding at least 1% of their leaf's majorant, and the
+projection onto the FP64 gradient (which averages the tails) is checked on the
+largest-gradient voxels of all."""
 import numpy as np
 import pytest
 
@@ -66,3 +78,40 @@ def test_quadrature_gradient_equals_its_central_differences(port):
         b[li, vi] = v0
         fd = (vals[0] - vals[1]) / (steps[0] - steps[1])
         assert abs(fd - g[li, vi]) <= 1e-4 * abs(g[li, vi]) + 1e-12, (idx, fd, g[li, vi])
+
+
+def adjoint_vs_quadrature(g64, G, bricks, nodes):
+    """(projection of the mean adjoint on the FP64 gradient over its 256
+    largest entries, per-voxel failures among the 256 largest entries of voxels
+    holding >= 1% of their leaf majorant, projection on those, median relative
+    standard error there).  G: (groups, n_leaves * 512) independent estimates."""
+    groups = G.shape[0]
+    maj = np.zeros(len(bricks))
+    fog = nodes["volx"][:, 1] != 0xFFFFFFFF
+    maj[nodes["volx"][fog, 1]] = nodes["qval"][fog, 1]
+    val = np.asarray(bricks, np.float64).ravel()
+    gflat = g64.ravel()
+    top = np.argsort(-np.abs(gflat))[:256]
+    m_all = G[:, top].mean(0)
+    proj_all = float(m_all @ gflat[top] / (gflat[top] @ gflat[top]))
+    cand = np.flatnonzero(val >= 0.01 * np.repeat(maj, 512))
+    sel = cand[np.argsort(-np.abs(gflat[cand]))[:256]]
+    want = gflat[sel]
+    m, se = G[:, sel].mean(0), G[:, sel].std(0, ddof=1) / np.sqrt(groups)
+    bad = int((np.abs(m - want) > 0.02 * np.abs(want) + 4 * se).sum())
+    return proj_all, bad, float(m @ want / (want @ want)), float(np.median(se / np.abs(want)))
+
+
+def test_restated_adjoint_matches_quadrature_gradient(port):
+    nodes, bricks, cfg, P, keep, ro, rd = crop_setup(port)
+    S = port.scene(nodes, bricks)
+    _, g64 = port.single_scatter_sun(S, P, ro, rd)
+    spp, groups = 4096, 16
+    dsun = np.zeros((16, 16, 4), np.float32)
+    dsun[..., :3] = 1.0 / spp
+    G = np.stack([np.asarray(port.adjoint_tile(S, P, 24, 24, 16, 16, spp, 700 + k, 0, dsun, np.zeros_like(dsun))[0],
+                             np.float64).ravel() for k in range(groups)])
+    proj_all, bad, proj, rel_se = adjoint_vs_quadrature(g64, G, bricks, nodes)
+    assert abs(proj_all - 1.0) < 0.02, proj_all
+    assert bad == 0 and abs(proj - 1.0) < 0.01, (bad, proj)
+    assert rel_se < 0.04  # the check resolves a few per cent per voxel
