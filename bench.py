@@ -758,10 +758,11 @@ def measure_adjoint(r, pdf, cdf, cfgs, rads, steps: int = 3, warmup: int = 3, fd
                                        "quotient counts flipped real/null decisions, each an O(1) jump, so its "
                                        "standard error exceeds the signal (se_of_diff below)",
                      "independent_checks": [
-                         "FP64 single-scatter sun image by quadrature, its exact gradient against the GPU adjoint "
-                         "on the 256 voxels of largest gradient, 2% per voxel + 4 SE and 1% in projection "
-                         "(tests/test_gpu_adjoint_fp64.py; the quadrature against the estimator and its own central "
-                         "differences in tests/test_single_scatter_fp64.py)",
+                         "FP64 single-scatter sun image by quadrature, its exact gradient against the GPU adjoint: "
+                         "2% per voxel + 4 SE and 1% in projection on the 256 largest-gradient voxels holding >= 1% "
+                         "of their leaf majorant, 5% in projection on the 256 largest of all (near-empty voxels give "
+                         "heavy-tailed estimates) (tests/test_gpu_adjoint_fp64.py; the quadrature against the "
+                         "estimator and its own central differences in tests/test_single_scatter_fp64.py)",
                          "FP64 transmittance gradient (quadrature) against the GPU transmittance adjoint "
                          "(tests/test_gpu_adjoint.py::test_transmittance_adjoint_equals_restatement_and_fp64)"],
                      "reweighted_note": "the reweighted replay shares the adjoint's likelihood-ratio weights: it "
