@@ -525,6 +525,8 @@ def measure_c0(r, pdf, cdf, cfgs, rads, steps: int, warmup: int, cpu: bool, cpu_
     cnt = r.counters()
     verts = cnt["vertices"] / steps
     kernel = verts / (np.mean(ms) / 1e3)
+    b_v = (64.0 * cnt["node_visits"] + 32.0 * cnt["density_lookups"] + 24.0 * cnt["mie_evals"]) / cnt["vertices"]
+    peak, peak_kind = measured_peak()
     frame = (np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.float32))
     r.render_tile(0, 0, w, h, 1, seed=3, sample_base=0, out=frame)
     t0 = time.perf_counter()
@@ -560,7 +562,10 @@ def measure_c0(r, pdf, cdf, cfgs, rads, steps: int, warmup: int, cpu: bool, cpu_
         "workload": "c0: 64^3 puff (seed 1), sigma_t 20, albedo 0.99, 8 events, 256x256 at 16 spp, whole frame",
         "same_config": True, "tuning": list(best),
         "gpu": {"value": kernel, "unit": "vertices/s", "ms_per_frame": float(np.mean(ms)), "launch_ms": ms,
-                "vertices_per_frame": verts, "paths_per_frame": cnt["paths"] / steps},
+                "vertices_per_frame": verts, "paths_per_frame": cnt["paths"] / steps,
+                "roofline": {"algorithmic_bytes_per_vertex": b_v, "achieved": b_v * kernel / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": b_v * kernel / 1e9 / peak, "peak_kind": peak_kind,
+                             "calibration": "counters of the timed frames"}},
         "gpu_e2e": {"value": verts / e2e_s, "unit": "vertices/s", "ms_per_frame": e2e_s * 1e3,
                     "h2d_bytes_per_step": int(pdf.nbytes / 3 * 4 + cdf.nbytes / 3 + 16 * 4 * 2 + 64),
                     "d2h_bytes_per_step": 2 * w * h * 16},
@@ -841,7 +846,41 @@ def profile_large(crop: int, launches: int = 3, spp: int = 256):
     r.close()
 
 
-def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp: int = 256):
+def large_cpu_reference(r, oc, settings_big, crop: int = 64, spp: int = 256):
+    """The reference renderer (oracle/_ref, all host threads) on a crop x crop
+    block of the large scene's 3840x2160 frame at full spp, centred on puff 15
+    (the medium, not the empty sky); its vertex count is the GPU renderer's on
+    the same block (the same estimator: the reference is not instrumented)."""
+    from oracle import Reference
+
+    threads = os.cpu_count() or 1
+    p = np.asarray(W.slab_recipe(2048).puffs[15].center, np.float64)
+    vi, pj = settings_big.viewi, settings_big.proji
+    ys, xs = np.mgrid[0:2160:8, 0:3840:8]
+    ro, rd, _ = cam.camera_rays(vi, pj, 3840, 2160, xs.ravel(), ys.ravel())
+    v = p - ro.astype(np.float64)
+    d = rd.astype(np.float64)
+    k = int(np.argmin(np.linalg.norm(v - (v * d).sum(1, keepdims=True) * d, axis=1)))
+    x0, y0 = (int(xs.ravel()[k]) - crop // 2) & ~1, (int(ys.ravel()[k]) - crop // 2) & ~1
+    ss, sa, ev = W.medium("c4")
+    cfg = dict(sigma_s=ss, sigma_a=sa, scattevs=ev, sun_dir=settings_big.sun_dir, sun_color=settings_big.sun_color,
+               sun_angle=settings_big.sun_angle, turbidity=W.SKY["turbidity"], ground_albedo=W.SKY["albedo"],
+               viewi=vi, proji=pj, w=3840, h=2160)
+    ref = Reference()
+    ref.set_threads(threads)
+    rs = ref.scene(oc.nodes, oc.bricks)
+    t = time.perf_counter()
+    rs.render(cfg, x0, y0, crop, crop, spp)
+    dt = time.perf_counter() - t
+    r.reset_counters()
+    r.render_tile(x0, y0, crop, crop, spp, seed=11, sample_base=0)
+    verts = r.counters()["vertices"]
+    return {"value": verts / dt, "unit": "vertices/s", "cores": threads, "kind": "reference", "seconds": dt,
+            "sample": f"{crop}x{crop} block at ({x0},{y0}) of the 3840x2160 frame (on puff 15) at {spp} spp; vertex "
+                      "count measured by the GPU renderer on the same block"}
+
+
+def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp: int = 256, cpu: bool = False):
     """The large sparse scene (config 4): 24 puffs (workloads.slab_recipe) on a
     2048^3 grid, sigma_t = 100, albedo 0.99, 128 scattering events, 3840x2160 at
     256 spp rendered as 4 camera tiles of 1920x1080: plain (one launch per tile)
@@ -935,8 +974,15 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
         e2.record(cs)
         e2.synchronize()
         times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+    cpu_ref = None
+    if cpu:
+        try:
+            cpu_ref = large_cpu_reference(r, oc, big)
+        except Exception as e:  # the reference oracle needs oracle/_ref
+            cpu_ref = {"value": None, "sample": f"unavailable: {e}"}
     r.set_tuning(*saved)
     return {
+        "reference_cpu": cpu_ref,
         "workload": "24 puffs (seeds 20-43, radii U[0.02,0.12], default_rng(2044)) in a 1x1x0.3 slab on a 2048^3 grid, "
                     "sigma_t 100, albedo 0.99, 128 events, 3840x2160 at 256 spp as 4 tiles of 1920x1080",
         "nonzero_voxels": nonzero, "occupancy": nonzero / 2048 ** 3, "blocks": n_blocks,
@@ -1219,7 +1265,7 @@ def run_b200(args):
 
     large = None
     if rank == 0 and world == 1 and not args.no_large:
-        large = measure_large(r, pdf, cdf, cfgs, rads)
+        large = measure_large(r, pdf, cdf, cfgs, rads, cpu=not args.no_cpu)
         log(f"large: plain {large['plain']['value'] / 1e9:.3f} G/s ({large['plain']['ms_per_frame']:.0f} ms/frame), "
             f"batched {large['batched']['value'] / 1e9:.3f} G/s, adjoint step {large['adjoint_512']['ratio']:.2f}x")
 
