@@ -30,9 +30,13 @@ __device__ __forceinline__ float sat_ref(float x) { return x != x ? 1.0f : sse_m
 // ---- bit-reproducible transcendentals --------------------------------------
 // Same operation sequences as the CPU restatement, built from IEEE binary32
 // operations and explicit fused multiply-adds:
-//   log : e ln2 + 2 atanh(s), s = (m-1)/(m+1), atanh by Maclaurin series to s^11
-//   exp : Cody-Waite reduction by ln2, Taylor series to r^11
-//   sincos: Cody-Waite reduction by pi/2 (three parts), Taylor series on |r| <= pi/4
+//   log : e ln2 + 2 atanh(s), s = (m-1)/(m+1), atanh by Maclaurin series to s^9
+//         (|s| <= 0.1716: the next term is below 2e-9 relative)
+//   exp : Cody-Waite reduction by ln2, Taylor series to r^7 (|r| <= ln2/2: the
+//         next term is below 8e-9 relative)
+//   sincos: Cody-Waite reduction by pi/2 (three parts), Taylor series of sin to
+//         r^9 and cos to r^10 on |r| <= pi/4 (next terms below 3e-9)
+//   x^1.5 : x sqrt(x)
 constexpr float kLn2Hi = 0.693115234375f;
 constexpr float kLn2Lo = 3.19461833e-05f;
 constexpr float kPio2_1 = 1.5703125f;
@@ -51,8 +55,7 @@ __device__ __forceinline__ float dlog(float x) {
     if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
     float s = (m - 1.0f) / (m + 1.0f);
     float s2 = s * s;
-    float p = 0.0909090909f;
-    p = fmaf(p, s2, 0.111111111f);
+    float p = 0.111111111f;
     p = fmaf(p, s2, 0.142857143f);
     p = fmaf(p, s2, 0.2f);
     p = fmaf(p, s2, 0.333333333f);
@@ -69,11 +72,7 @@ __device__ __forceinline__ float dexp(float x) {
     float k = floorf(fmaf(x, 1.44269504f, 0.5f));
     float r = fmaf(-k, kLn2Hi, x);
     r = fmaf(-k, kLn2Lo, r);
-    float p = 2.50521084e-08f;
-    p = fmaf(p, r, 2.75573192e-07f);
-    p = fmaf(p, r, 2.75573192e-06f);
-    p = fmaf(p, r, 2.48015873e-05f);
-    p = fmaf(p, r, 1.98412698e-04f);
+    float p = 1.98412698e-04f;
     p = fmaf(p, r, 1.38888889e-03f);
     p = fmaf(p, r, 8.33333333e-03f);
     p = fmaf(p, r, 4.16666667e-02f);
@@ -94,24 +93,24 @@ __device__ __forceinline__ float dpow(float x, float y) {
     return dexp(y * dlog(x));
 }
 
+// x^1.5 for x >= 0 (the sky's and HG's exponent); negative x or NaN gives NaN.
+__device__ __forceinline__ float dpow15(float x) {
+    if (x < 0.0f || x != x) return __int_as_float(0x7fc00000);
+    return x * sqrtf(x);
+}
+
 __device__ __forceinline__ void dsincos(float x, float *ps, float *pc) {
     float k = rintf(x * 0.636619772f);
     float r = fmaf(-k, kPio2_1, x);
     r = fmaf(-k, kPio2_2, r);
     r = fmaf(-k, kPio2_3, r);
     float r2 = r * r;
-    float sp = -7.64716373e-13f;
-    sp = fmaf(sp, r2, 1.60590438e-10f);
-    sp = fmaf(sp, r2, -2.50521084e-08f);
-    sp = fmaf(sp, r2, 2.75573192e-06f);
+    float sp = 2.75573192e-06f;
     sp = fmaf(sp, r2, -1.98412698e-04f);
     sp = fmaf(sp, r2, 8.33333333e-03f);
     sp = fmaf(sp, r2, -1.66666667e-01f);
     float sn = fmaf(sp * r2, r, r);
-    float cp = 4.77947733e-14f;
-    cp = fmaf(cp, r2, -1.14707456e-11f);
-    cp = fmaf(cp, r2, 2.08767570e-09f);
-    cp = fmaf(cp, r2, -2.75573192e-07f);
+    float cp = -2.75573192e-07f;
     cp = fmaf(cp, r2, 2.48015873e-05f);
     cp = fmaf(cp, r2, -1.38888889e-03f);
     cp = fmaf(cp, r2, 4.16666667e-02f);
@@ -775,7 +774,7 @@ __device__ __forceinline__ void mie_sample(const MieSmem &M, const float iv[3], 
 // ---- phase function: HGPhase, src/KernelSampler.cpp:164-204 (DR_PHASE_HG) ----
 // g = HGPhase::g1 (blcloudsampling.phasea); the same value for r, g and b.
 __device__ __forceinline__ float hg_eval(float g, float ct) {
-    const float den = 12.566371f * dpow((1.0f + g * g) - (2.0f * g) * ct, 1.5f);  // float(4 SM_PI) * pow(., 1.5)
+    const float den = 12.566371f * dpow15((1.0f + g * g) - (2.0f * g) * ct);  // float(4 SM_PI) * pow(., 1.5)
     return (1.0f - g * g) / den;
 }
 
@@ -835,14 +834,15 @@ __device__ __forceinline__ float3 sky_eval(const DevParams &P, const float rd[3]
     const float gacs = sat_ref(cph);
     const float thcs = sse_max(rdz, 0.0f);
     const float raym = gacs * gacs;
+    const float zenh = sqrtf(thcs);
+    const float izen = 1.0f / (thcs + 0.01f);  // c1 / (thcs + 0.01) as c1 * izen: one division for three channels
     float out[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const float *c = P.sky_cfg[i];
         const float expm = dexp(c[4] * gmma);
-        const float miem = (1.0f + raym) / dpow((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs, 1.5f);
-        const float zenh = sqrtf(thcs);
-        float ca = (1.0f + c[0] * dexp(c[1] / (thcs + 0.01f))) *
+        const float miem = (1.0f + raym) / dpow15((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs);
+        float ca = (1.0f + c[0] * dexp(c[1] * izen)) *
                    ((((c[2] + c[3] * expm) + c[5] * raym) + c[6] * miem) + c[7] * zenh);
         ca = ca * P.sky_rad[i];
         out[i] = 1e-3f * dpow(ca, 2.2f);

@@ -100,6 +100,7 @@ class Port:
                                              C.c_uint32, C.c_uint32, vp, vp, vp]
         L.orc_sun_hit_fraction.argtypes = [C.POINTER(OrcParams), C.c_uint32, C.c_uint32]
         L.orc_sun_hit_fraction.restype = C.c_double
+        L.orc_math_eval.argtypes = [C.c_int, vp, C.c_uint32, vp]
         L.orc_render_tile_mt.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcParams), u32, u32, u32, u32, u32,
                                          C.c_uint64, C.c_uint64, vp, vp, C.POINTER(OrcCounters), C.c_int]
         L.orc_render_tile_mt.restype = C.c_int
@@ -395,6 +396,13 @@ class Port:
         self.L.orc_single_scatter_sun(C.byref(S), C.byref(P), _p(ro), _p(rd), len(ro), float(p_hit), nu, nphi, _p(w),
                                       _p(out), None if g is None else _p(g))
         return out, g
+
+    def math_eval(self, kind: int, x):
+        """orc_math.h's function `kind` (0 log, 1 exp, 2 sin, 3 cos, 4 x^1.5, 5 x^2.2) on float32 x."""
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros_like(x)
+        self.L.orc_math_eval(int(kind), _p(x), len(x), _p(out))
+        return out
 
     def sun_hit_fraction(self, P, n1=2048, n2=512):
         return float(self.L.orc_sun_hit_fraction(C.byref(P), n1, n2))

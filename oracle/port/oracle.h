@@ -138,6 +138,7 @@ double orc_optical_depth(const orc_scene *S, const double ro[3], const double rd
 void orc_single_scatter_sun(const orc_scene *S, const orc_params *P, const float *ro, const float *rd, uint32_t n_rays,
                             double p_hit, uint32_t nu, uint32_t nphi, const double wc[3], double *out, double *grad);
 double orc_sun_hit_fraction(const orc_params *P, uint32_t n1, uint32_t n2);
+void orc_math_eval(int kind, const float *x, uint32_t n, float *out);
 
 /* ---- estimator ----------------------------------------------------------- */
 /* Free-flight tracking of one segment (src/kernel.cpp:197-317, fog leaves).

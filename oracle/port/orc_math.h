@@ -6,10 +6,14 @@
  * operations gives the same bits on the host and on the device.
  *
  *   orc_log   : ln(m 2^e) = e ln2 + 2 atanh(s), s = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2));
- *               atanh by its Maclaurin series to s^11 (|s| <= 0.1716).
- *   orc_exp   : Cody-Waite reduction x = k ln2 + r, |r| <= ln2/2, Taylor to r^11.
+ *               atanh by its Maclaurin series to s^9 (|s| <= 0.1716; the next
+ *               term is below 2e-9 relative).
+ *   orc_exp   : Cody-Waite reduction x = k ln2 + r, |r| <= ln2/2, Taylor to r^7
+ *               (the next term is below 8e-9 relative).
+ *   orc_pow15 : x^1.5 = x sqrt(x).
  *   orc_sincos: reduction by multiples of pi/2 (three-part Cody-Waite split),
- *               Taylor series of sin to r^15 and cos to r^16 on |r| <= pi/4.
+ *               Taylor series of sin to r^9 and cos to r^10 on |r| <= pi/4
+ *               (next terms below 3e-9).
  *   orc_acos_ref: the reference's polynomial arccos (src/smmath.inl:414-420),
  *               reproduced because the reference's Mie lookup and sky use it.
  *   PCG32     : O'Neill's permuted congruential generator (XSH-RR output).
@@ -39,8 +43,7 @@ static inline float orc_log(float x) {
     if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
     float s = (m - 1.0f) / (m + 1.0f);
     float s2 = s * s;
-    float p = 0.0909090909f;                  /* 1/11 */
-    p = fmaf(p, s2, 0.111111111f);            /* 1/9  */
+    float p = 0.111111111f;                   /* 1/9  */
     p = fmaf(p, s2, 0.142857143f);            /* 1/7  */
     p = fmaf(p, s2, 0.2f);                    /* 1/5  */
     p = fmaf(p, s2, 0.333333333f);            /* 1/3  */
@@ -57,11 +60,7 @@ static inline float orc_exp(float x) {
     float k = floorf(fmaf(x, 1.44269504f, 0.5f));
     float r = fmaf(-k, ORC_LN2_HI, x);
     r = fmaf(-k, ORC_LN2_LO, r);
-    float p = 2.50521084e-08f;                /* 1/11! */
-    p = fmaf(p, r, 2.75573192e-07f);          /* 1/10! */
-    p = fmaf(p, r, 2.75573192e-06f);          /* 1/9!  */
-    p = fmaf(p, r, 2.48015873e-05f);          /* 1/8!  */
-    p = fmaf(p, r, 1.98412698e-04f);          /* 1/7!  */
+    float p = 1.98412698e-04f;                /* 1/7!  */
     p = fmaf(p, r, 1.38888889e-03f);          /* 1/6!  */
     p = fmaf(p, r, 8.33333333e-03f);          /* 1/5!  */
     p = fmaf(p, r, 4.16666667e-02f);          /* 1/4!  */
@@ -84,6 +83,12 @@ static inline float orc_pow(float x, float y) {
     return orc_exp(y * orc_log(x));
 }
 
+/* x^1.5 for x >= 0 (the sky's and HG's exponent); negative x or NaN gives NaN. */
+static inline float orc_pow15(float x) {
+    if (x < 0.0f || x != x) return NAN;
+    return x * sqrtf(x);
+}
+
 #define ORC_PIO2_1 1.5703125f                 /* pi/2 rounded to 12 bits (exact) */
 #define ORC_PIO2_2 4.83751297e-04f            /* pi/2 - PIO2_1 rounded to 12 bits */
 #define ORC_PIO2_3 7.54979013e-08f            /* pi/2 - PIO2_1 - PIO2_2, binary32 */
@@ -94,18 +99,12 @@ static inline void orc_sincos(float x, float *ps, float *pc) {
     r = fmaf(-k, ORC_PIO2_2, r);
     r = fmaf(-k, ORC_PIO2_3, r);
     float r2 = r * r;
-    float sp = -7.64716373e-13f;              /* -1/15! */
-    sp = fmaf(sp, r2, 1.60590438e-10f);       /*  1/13! */
-    sp = fmaf(sp, r2, -2.50521084e-08f);      /* -1/11! */
-    sp = fmaf(sp, r2, 2.75573192e-06f);       /*  1/9!  */
+    float sp = 2.75573192e-06f;               /*  1/9!  */
     sp = fmaf(sp, r2, -1.98412698e-04f);      /* -1/7!  */
     sp = fmaf(sp, r2, 8.33333333e-03f);       /*  1/5!  */
     sp = fmaf(sp, r2, -1.66666667e-01f);      /* -1/3!  */
     float sn = fmaf(sp * r2, r, r);
-    float cp = 4.77947733e-14f;               /*  1/16! */
-    cp = fmaf(cp, r2, -1.14707456e-11f);      /* -1/14! */
-    cp = fmaf(cp, r2, 2.08767570e-09f);       /*  1/12! */
-    cp = fmaf(cp, r2, -2.75573192e-07f);      /* -1/10! */
+    float cp = -2.75573192e-07f;              /* -1/10! */
     cp = fmaf(cp, r2, 2.48015873e-05f);       /*  1/8!  */
     cp = fmaf(cp, r2, -1.38888889e-03f);      /* -1/6!  */
     cp = fmaf(cp, r2, 4.16666667e-02f);       /*  1/4!  */

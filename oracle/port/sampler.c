@@ -297,12 +297,13 @@ void orc_sky_eval(const orc_params *P, const float rd[3], float out[3]) {
     float gacs = sse_max(sse_min(cph, 1.0f), 0.0f);
     float thcs = sse_max(rdz, 0.0f);
     float raym = gacs * gacs;
+    float zenh = sqrtf(thcs);
+    float izen = 1.0f / (thcs + 0.01f); /* c1 / (thcs + 0.01) taken as c1 * izen (within an ulp) */
     for (int i = 0; i < 3; ++i) {
         const float *c = P->sky_cfg[i];
         float expm = orc_exp(c[4] * gmma);
-        float miem = (1.0f + raym) / orc_pow((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs, 1.5f);
-        float zenh = sqrtf(thcs);
-        float ca = (1.0f + c[0] * orc_exp(c[1] / (thcs + 0.01f))) *
+        float miem = (1.0f + raym) / orc_pow15((1.0f + c[8] * c[8]) - (2.0f * c[8]) * gacs);
+        float ca = (1.0f + c[0] * orc_exp(c[1] * izen)) *
                    ((((c[2] + c[3] * expm) + c[5] * raym) + c[6] * miem) + c[7] * zenh);
         ca = ca * P->sky_rad[i];
         out[i] = 1e-3f * orc_pow(ca, 2.2f);
@@ -314,7 +315,7 @@ void orc_sky_eval(const orc_params *P, const float rd[3], float out[3]) {
  * binary32; Sample: sq = (1 - g g) / (1 - g + 2 g u1), ct = (1 + g g - sq sq) /
  * (2 g), composed with SamplingBasis like the Mie sampler. */
 float orc_hg_eval(float g, float ct) {
-    float den = 12.566371f * orc_pow((1.0f + g * g) - (2.0f * g) * ct, 1.5f);
+    float den = 12.566371f * orc_pow15((1.0f + g * g) - (2.0f * g) * ct);
     return (1.0f - g * g) / den;
 }
 
@@ -407,4 +408,20 @@ void orc_camera_ray(const orc_params *P, uint32_t px, uint32_t py, float ro[3], 
         ro[k] = V[12 + k];
     }
     *in_frame = (hx > -1.0f && hx < 1.0f) && (hy > -1.0f && hy < 1.0f);
+}
+
+/* The scalar math of orc_math.h over an array (accuracy tests): kind 0 log,
+ * 1 exp, 2 sin, 3 cos, 4 x^1.5, 5 x^2.2. */
+void orc_math_eval(int kind, const float *x, uint32_t n, float *out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        float s, c;
+        switch (kind) {
+        case 0: out[i] = orc_log(x[i]); break;
+        case 1: out[i] = orc_exp(x[i]); break;
+        case 2: orc_sincos(x[i], &s, &c); out[i] = s; break;
+        case 3: orc_sincos(x[i], &s, &c); out[i] = c; break;
+        case 4: out[i] = orc_pow15(x[i]); break;
+        default: out[i] = orc_pow(x[i], 2.2f); break;
+        }
+    }
 }
