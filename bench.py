@@ -872,9 +872,14 @@ def large_cpu_reference(r, oc, settings_big, crop: int = 64, spp: int = 256):
     t = time.perf_counter()
     rs.render(cfg, x0, y0, crop, crop, spp)
     dt = time.perf_counter() - t
+    saved = r.get_tuning()
+    r.upload(oc)  # the scene and frame may have changed since (the adjoint step sets its own)
+    r.set_params(settings_big)
+    r.set_tuning()
     r.reset_counters()
     r.render_tile(x0, y0, crop, crop, spp, seed=11, sample_base=0)
     verts = r.counters()["vertices"]
+    r.set_tuning(*saved)
     return {"value": verts / dt, "unit": "vertices/s", "cores": threads, "kind": "reference", "seconds": dt,
             "sample": f"{crop}x{crop} block at ({x0},{y0}) of the 3840x2160 frame (on puff 15) at {spp} spp; vertex "
                       "count measured by the GPU renderer on the same block"}

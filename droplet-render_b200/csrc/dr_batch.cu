@@ -55,6 +55,8 @@ void drop_graph(dr_batch *b) {
 // Lays the view's paths out for the current tile order and (re)captures the graph.
 int build_graph(dr_batch *b) {
     drop_graph(b);
+    bool ext = b->any_sdf;  // surface leaves, or a view with the HG phase or a non-Hosek environment
+    for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
     uint64_t begin = 0;
     std::vector<uint64_t> begins(b->host_views.size());
     for (size_t v = 0; v < b->host_views.size(); ++v) {
@@ -62,6 +64,8 @@ int build_graph(dr_batch *b) {
         TileArgs A;
         int rc = make_tile_args(V.A.x0, V.A.y0, V.A.tw, V.A.th, V.A.spp, V.A.seed, 0, b->tuning.tile, A);
         if (rc != DR_OK) return rc;
+        // sky terms through the warps' queues (not with a whole-path finiteness check)
+        A.defer_sky = (!ext && !V.P.finite_paths) ? 1u : 0u;
         V.A = A;
         V.begin = begin;
         begins[v] = begin;
@@ -82,8 +86,6 @@ int build_graph(dr_batch *b) {
     B.step = b->step.p;
     DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");
     cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
-    bool ext = b->any_sdf;  // surface leaves, or a view with the HG phase or a non-Hosek environment
-    for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
     if (e == cudaSuccess)
         e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
                                 b->stack_levels, b->ctx->device, b->stream);

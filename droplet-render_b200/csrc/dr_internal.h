@@ -125,6 +125,10 @@ struct TileArgs {
     uint64_t seed, sample_base;
     uint64_t n_paths;         // path indices: cols * rows * spp (row-major) or squares * tile^2 * spp
     FastDiv spp_div, cols_div, t2_div, tx_div, tile_div;  // division by spp, cols, tile^2, tiles_x, tile
+    // Persistent kernel only (its launcher sets it): the sky term of a path
+    // that escapes after scattering goes to the warp's queue of sky terms and is
+    // evaluated 32 at a time (Hosek sky, no whole-path finiteness check).
+    uint32_t defer_sky;
 };
 
 struct DevCounters {

@@ -186,6 +186,13 @@ __global__ void __launch_bounds__(kRenderBlock) shadow_tile_kernel(DevScene S, D
 // Per path, the operations and random draws are those of path_sample()/track():
 // a path's result is bit-identical to the one-thread-per-path kernel.
 enum : uint32_t { kFetch = 0, kTrav = 1, kStep = 2, kEvent = 3, kDone = 4 };
+// Segment result of a path that escaped after scattering and left its sky term
+// to the warp's sky queue (the loop enqueues it after the event pass).
+constexpr uint32_t kTrackDeferSky = 3;
+// Per warp in dynamic shared memory: 32 sky terms, 7 words each (rd.xyz,
+// T.xyz, output offset; the batch adds the view), stored word-major so a
+// lane's slot is one column.
+template <bool BATCH> __host__ __device__ constexpr uint32_t sky_queue_words() { return (BATCH ? 8u : 7u) * 32u; }
 enum : uint32_t { kSegMain = 0, kSegShadow = 1 };
 
 template <bool WALK> struct SegTrav;
@@ -417,14 +424,20 @@ __device__ __forceinline__ void scatter_event(PathLane<WALK> &L, const DevScene 
                 L.sun.y = L.sun.y + L.T[1] * 0.0f;
                 L.sun.z = L.sun.z + L.T[2] * 0.0f;
             }
-            const float3 sky = escape_sky<FEAT>(P, L.rd);
-            L.sky.x = L.sky.x + L.T[0] * sky.x;
-            L.sky.y = L.sky.y + L.T[1] * sky.y;
-            L.sky.z = L.sky.z + L.T[2] * sky.z;
+            if (FEAT == 0 && A.defer_sky) {
+                // the sky term, T * sky(rd) (the path's sky sum is 0 until this
+                // escape), goes to the warp's sky queue after the event pass
+                L.esc = kTrackDeferSky;
+            } else {
+                const float3 sky = escape_sky<FEAT>(P, L.rd);
+                L.sky.x = L.sky.x + L.T[0] * sky.x;
+                L.sky.y = L.sky.y + L.T[1] * sky.y;
+                L.sky.z = L.sky.z + L.T[2] * sky.z;
+            }
         }
     }
     // one store for escaped, cut and last-event paths alike
-    if (L.esc == kTrackEscaped || L.esc == kTrackCut || L.r >= P.scattevs) {
+    if (L.esc == kTrackEscaped || L.esc == kTrackDeferSky || L.esc == kTrackCut || L.r >= P.scattevs) {
         finish_path(L, P, A, sun_out, sky_out);
         state = kFetch;
         return;
@@ -556,6 +569,77 @@ __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const 
     }
 }
 
+// The sky terms of a persistent launch are evaluated by full warps: after an
+// event pass, the lanes whose path escaped with its sky term deferred append
+// (rd, T, pixel[, view]) to the warp's queue (q: sky_queue_words floats, nq
+// entries, warp-uniform); whenever it holds 32, every lane evaluates one,
+// T * sky(rd), and adds it to the pixel.  That is the value the path would
+// have added in place (its sky sum is 0 before the escape); the pixel's total
+// differs only in the order of the float additions, as between any two runs.
+template <bool BATCH>
+__device__ __forceinline__ void sky_queue_eval(const DevParams &P, float4 *sky_out, const BatchArgs &B, const float *q,
+                                               uint32_t lane) {
+    const float rd[3] = {q[lane], q[32 + lane], q[64 + lane]};
+    const uint32_t off = __float_as_uint(q[192 + lane]);
+    float3 sky;
+    float4 *out;
+    if constexpr (BATCH) {
+        const BatchView &V = B.views[__float_as_uint(q[224 + lane])];
+        sky = escape_sky<0>(V.P, rd);
+        out = V.sky;
+    } else {
+        sky = escape_sky<0>(P, rd);
+        out = sky_out;
+    }
+    atomicAdd(&out[off], make_float4(q[96 + lane] * sky.x, q[128 + lane] * sky.y, q[160 + lane] * sky.z, 0.0f));
+}
+
+template <bool BATCH, bool WALK>
+__device__ __forceinline__ void sky_queue_put(float *q, uint32_t slot, const PathLane<WALK> &L, const TileArgs &A,
+                                              uint32_t view) {
+    q[slot] = L.rd[0];
+    q[32 + slot] = L.rd[1];
+    q[64 + slot] = L.rd[2];
+    q[96 + slot] = L.T[0];
+    q[128 + slot] = L.T[1];
+    q[160 + slot] = L.T[2];
+    q[192 + slot] = __uint_as_float((L.py - A.y0) * A.tw + (L.px - A.x0));
+    if constexpr (BATCH) q[224 + slot] = __uint_as_float(view);
+}
+
+// Called by the whole warp after an event pass; A and view are the lane's.
+template <bool BATCH, bool WALK>
+__device__ __forceinline__ void sky_queue_push(PathLane<WALK> &L, const TileArgs &A, uint32_t view,
+                                               const DevParams &P, float4 *sky_out, const BatchArgs &B, float *q,
+                                               uint32_t &nq, uint32_t lane, uint32_t lt_mask) {
+    const bool mine = L.esc == kTrackDeferSky;
+    const uint32_t dm = __ballot_sync(0xffffffffu, mine);
+    if (!dm) return;
+    const uint32_t pos = nq + __popc(dm & lt_mask);
+    const uint32_t total = nq + __popc(dm);
+    if (mine) {
+        L.esc = kTrackEscaped;
+        if (pos < 32u) sky_queue_put<BATCH>(q, pos, L, A, view);
+    }
+    if (total < 32u) {
+        nq = total;
+        return;
+    }
+    __syncwarp();
+    sky_queue_eval<BATCH>(P, sky_out, B, q, lane);
+    __syncwarp();
+    if (mine && pos >= 32u) sky_queue_put<BATCH>(q, pos - 32u, L, A, view);
+    nq = total - 32u;
+}
+
+// The rest of the queue (whole warp, after its last path).
+template <bool BATCH>
+__device__ __forceinline__ void sky_queue_flush(const DevParams &P, float4 *sky_out, const BatchArgs &B,
+                                                const float *q, uint32_t nq, uint32_t lane) {
+    __syncwarp();
+    if (lane < nq) sky_queue_eval<BATCH>(P, sky_out, B, q, lane);
+}
+
 // View owning global path index p: the last v with begins[v] <= p.
 __device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
     uint32_t lo = 0, hi = B.n_views - 1;
@@ -609,12 +693,18 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     uint32_t nstack[kMaxDepth];
     Trav slow[1];
     PathLane<WALK> L;
+    L.esc = kTrackEscaped;  // read by every lane after an event pass (sky queue), before its first segment ends
     uint32_t view = 0;
     uint32_t state = staged ? kFetch : kDone;
     if (!staged && threadIdx.x == 0) atomicAdd(&C->gave_up, 1ull);
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const unsigned FULL = 0xffffffffu;
+    // this warp's sky queue, after the phase tables and the shared traversal stack
+    float *const skyq = reinterpret_cast<float *>(smem + ((mb + 15u) & ~15u) +
+                                                  (size_t)shlevels * 7u * 4u * kPersistentBlock) +
+                        (threadIdx.x >> 5) * sky_queue_words<BATCH>();
+    uint32_t nsky = 0;
     for (;;) {
         const uint32_t want = __ballot_sync(FULL, state == kFetch);
         if (want) {
@@ -648,10 +738,21 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
             const BatchView &V = B.views[view];
             lane_work<WALK, FEAT, SHS>(L, events, B.scenes[V.scene], V.P, M, V.A, V.sun, V.sky, cnt, state, nstack,
                                       slow, visits, steps, ts, shcol, shlevels);
+            // FEAT == 0: the launcher reserved the queue (views that defer set V.A.defer_sky)
+            if constexpr (FEAT == 0) {
+                if (events) sky_queue_push<true>(L, V.A, view, P, sky_out, B, skyq, nsky, lane, lt_mask);
+            }
         } else {
             lane_work<WALK, FEAT, SHS>(L, events, S, P, M, A, sun_out, sky_out, cnt, state, nstack, slow, visits,
                                       steps, ts, shcol, shlevels);
+            if constexpr (FEAT == 0) {
+                if (events && A.defer_sky)
+                    sky_queue_push<false>(L, A, 0u, P, sky_out, B, skyq, nsky, lane, lt_mask);
+            }
         }
+    }
+    if constexpr (FEAT == 0) {
+        if (BATCH || A.defer_sky) sky_queue_flush<BATCH>(P, sky_out, B, skyq, nsky, lane);
     }
     warp_sum_counts(cnt, C, paths);
 }
@@ -1345,6 +1446,14 @@ static size_t mie_smem(const DevParams &P) {
     return (size_t)P.mie_n * 20u + (P.phase_mode == 1u ? (2u * (size_t)P.mie_n + 1u) * 16u : 0u);
 }
 
+// Dynamic shared memory above the default 48 KB (phase tables of more than
+// about 2,400 entries) needs the kernel's opt-in, up to the 227 KB a block can have.
+template <class F> static cudaError_t allow_smem(F fn, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+}
+
 // Feature bits a frame needs.
 static uint32_t frame_features(const DevScene &S, const DevParams &P) {
     return ((S.occ_nodes && P.embree) ? kFeatOcc : 0u) |
@@ -1356,12 +1465,10 @@ cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const Tile
     if (A.n_paths == 0) return cudaSuccess;
     const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
-    if (frame_features(S, P))
-        render_tile_kernel<kFeatAll><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out,
-                                                                                       sky_out, C);
-    else
-        render_tile_kernel<0><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out,
-                                                                                C);
+    const auto fn = frame_features(S, P) ? render_tile_kernel<kFeatAll> : render_tile_kernel<0>;
+    const cudaError_t e = allow_smem(fn, mie_smem(P));
+    if (e != cudaSuccess) return e;
+    fn<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, sun_out, sky_out, C);
     return cudaGetLastError();
 }
 
@@ -1419,8 +1526,9 @@ static PersistentFn persistent_variant(uint32_t minb, uint32_t traversal, bool b
 
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persistent_variant(variant, traversal, false),
-                                                      kPersistentBlock, smem_bytes) != cudaSuccess)
+    const PersistentFn fn = persistent_variant(variant, traversal, false);
+    if (allow_smem(fn, smem_bytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kPersistentBlock, smem_bytes) != cudaSuccess)
         return 1;
     return nb > 0 ? nb : 1;
 }
@@ -1434,6 +1542,8 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
     if (e != cudaSuccess) return e;
     const uint32_t variant = tune.blocks_per_sm ? tune.blocks_per_sm : 4u;
     fn = persistent_variant(variant, tune.traversal, batch, feat);
+    e = allow_smem(fn, smem);
+    if (e != cudaSuccess) return e;
     int maxb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, kPersistentBlock, smem) != cudaSuccess || maxb < 1)
         maxb = 1;
@@ -1471,6 +1581,11 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     const uint32_t feat = frame_features(S, P);
     Tuning tune = tune_in;
     const uint32_t shlevels = shared_stack_plan(tune, feat, S.stack_levels, smem);
+    // sky terms evaluated by full warps (Hosek sky only; a whole-path
+    // finiteness check needs the path's sky sum in place)
+    TileArgs Ad = A;
+    Ad.defer_sky = (feat == 0 && !P.finite_paths) ? 1u : 0u;
+    if (Ad.defer_sky) smem = ((smem + 15) & ~(size_t)15) + (size_t)sky_queue_words<false>() * 4u * (kPersistentBlock / 32);
     PersistentFn fn;
     int blocks;
     uint32_t batch;
@@ -1479,7 +1594,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     batch |= shlevels << 24;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
-    fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, A, mie_pack, sun_out, sky_out, C, Q, batch, BatchArgs{});
+    fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, Ad, mie_pack, sun_out, sky_out, C, Q, batch, BatchArgs{});
     return cudaGetLastError();
 }
 
@@ -1489,6 +1604,7 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
     size_t smem = mie_smem(P0);
     Tuning tune = tune_in;
     const uint32_t shlevels = shared_stack_plan(tune, ext ? kFeatAll : 0u, stack_levels, smem);
+    if (!ext) smem = ((smem + 15) & ~(size_t)15) + (size_t)sky_queue_words<true>() * 4u * (kPersistentBlock / 32);
     PersistentFn fn;
     int blocks;
     uint32_t batch;
@@ -1533,6 +1649,8 @@ cudaError_t launch_probe_density(const DevScene &S, const uint32_t *nodes, const
 cudaError_t launch_probe_paths(const DevScene &S, const DevParams &P, const void *mie_pack, const uint32_t *px,
                                const uint32_t *py, const uint64_t *sample, uint32_t n, uint64_t seed,
                                float4 *out_sun, float4 *out_sky, DevCounters *C, cudaStream_t st) {
+    const cudaError_t e = allow_smem(probe_paths_kernel, mie_smem(P));
+    if (e != cudaSuccess) return e;
     probe_paths_kernel<<<(n + 127) / 128, 128, mie_smem(P), st>>>(S, P, mie_pack, px, py, sample, n, seed, out_sun,
                                                                   out_sky, C);
     return cudaGetLastError();
@@ -1540,6 +1658,8 @@ cudaError_t launch_probe_paths(const DevScene &S, const DevParams &P, const void
 
 cudaError_t launch_probe_sampler(const DevParams &P, const void *mie_pack, uint32_t what, const float *in, uint32_t n,
                                  float *out, cudaStream_t st) {
+    const cudaError_t e = allow_smem(probe_sampler_kernel, mie_smem(P));
+    if (e != cudaSuccess) return e;
     probe_sampler_kernel<<<(n + 127) / 128, 128, mie_smem(P), st>>>(P, mie_pack, what, in, n, out);
     return cudaGetLastError();
 }
@@ -1573,6 +1693,10 @@ cudaError_t launch_adjoint_tile(const DevScene &S, const DevParams &P, const Til
     }
     const size_t smem = mie_smem(P);
     const uint32_t feat = frame_features(S, P);
+    e = allow_smem(feat ? adjoint_totals_kernel<kFeatAll> : adjoint_totals_kernel<0>, smem);
+    if (e != cudaSuccess) return e;
+    e = allow_smem(feat ? adjoint_scatter_kernel<kFeatAll> : adjoint_scatter_kernel<0>, smem);
+    if (e != cudaSuccess) return e;
     PathRecord *rec = (PathRecord *)records;
     for (uint64_t p0 = 0; p0 < A.n_paths; p0 += chunk) {
         const uint64_t n = A.n_paths - p0 < chunk ? A.n_paths - p0 : chunk;
@@ -1609,13 +1733,11 @@ cudaError_t launch_reweighted_loss(const DevScene &S, const DevParams &P, const 
     if (A.n_paths > 0) {
         const uint64_t blocks = (A.n_paths + kRenderBlock - 1) / kRenderBlock;
         if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
-        if (frame_features(S, P))
-            reweighted_loss_kernel<kFeatAll><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(
-                S, P, A, mie_pack, dsun, dsky, pert, slots, C);
-        else
-            reweighted_loss_kernel<0><<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, dsun,
-                                                                                        dsky, pert, slots, C);
-        const cudaError_t e = cudaGetLastError();
+        const auto fn = frame_features(S, P) ? reweighted_loss_kernel<kFeatAll> : reweighted_loss_kernel<0>;
+        cudaError_t e = allow_smem(fn, mie_smem(P));
+        if (e != cudaSuccess) return e;
+        fn<<<(unsigned)blocks, kRenderBlock, mie_smem(P), st>>>(S, P, A, mie_pack, dsun, dsky, pert, slots, C);
+        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     sum_slots_kernel<<<1, 256, 0, st>>>(loss, slots);

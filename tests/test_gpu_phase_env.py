@@ -122,3 +122,50 @@ def test_adjoint_equals_restatement(renderer, port):
     assert scale > 0
     assert np.allclose(g_gpu, g_cpu, rtol=1e-3, atol=1e-4 * scale)
     assert abs(float(ga.item()) - a_cpu) <= 1e-4 * abs(a_cpu) + 1e-6
+
+
+def _large_tables(n):
+    """The config-0 phase tables resampled to n entries (linear in the index)."""
+    from conftest import mie_table
+
+    pdf, cdf = mie_table()
+    x = np.linspace(0.0, len(pdf) - 1.0, n)
+    i = np.arange(len(pdf), dtype=np.float64)
+
+    def big(t):
+        return np.stack([np.interp(x, i, t[:, c]) for c in range(3)], 1).astype(np.float32)
+
+    return big(pdf), big(cdf)
+
+
+# 4096 entries: 80 KB of phase tables in shared memory, above the 48 KB a
+# kernel gets without opting in; every kernel that stages them must still run
+@pytest.mark.parametrize("tuning", [(0, 0, 0, 0, 0, 0, 0), (1, 0, 0, 0, 0, 0, 0), (0, 8, 24, 2, 0, 3, 4)])
+def test_largest_phase_tables(renderer, port, tuning):
+    nodes, bricks, _ = golden_octree()
+    cfg = c0_cfg(64, 64)
+    cfg["mie_pdf"], cfg["mie_cdf"] = _large_tables(4096)
+    renderer.set_params(settings_from_cfg(cfg))
+    keep = []
+    P = port.params(cfg, keep)
+    S = port.scene(nodes, bricks)
+    saved = renderer.get_tuning()
+    try:
+        renderer.set_tuning(*tuning)
+        sun, sky = renderer.render_tile(8, 10, 48, 44, 16, seed=6, sample_base=0)
+    finally:
+        renderer.set_tuning(*saved)
+    psun, psky, pcnt = port.render_tile(S, P, 8, 10, 48, 44, 16, seed=6, sample_base=0)
+    assert pcnt["mie_evals"] > 1000
+    for g, p in ((sun, psun), (sky, psky)):
+        assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), tuning
+    assert sky[..., :3].sum() > 0
+    rng = np.random.default_rng(3)
+    n = 500
+    px = rng.integers(16, 48, n).astype(np.uint32)
+    py = rng.integers(20, 44, n).astype(np.uint32)
+    sm = rng.integers(0, 1 << 40, n).astype(np.uint64)
+    a, b = renderer.probe_paths(px, py, sm, seed=80)
+    for i in range(0, n, 5):
+        pa, pb, _ = port.render_path(S, P, int(px[i]), int(py[i]), 80, int(sm[i]))
+        assert np.array_equal(bits(a[i]), bits(pa)) and np.array_equal(bits(b[i]), bits(pb)), i
