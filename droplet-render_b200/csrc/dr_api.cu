@@ -100,6 +100,11 @@ int dr_destroy(dr_ctx *c) {
         c->env.release();
         c->occ_tris.release();
         c->band_work.release();
+        c->cam_head.release();
+        c->cam_pool.release();
+        c->band_cam_head.release();
+        c->band_cam_pool.release();
+        c->cam_used.release();
         for (int k = 0; k < 2; ++k)
             if (c->band_stream[k]) cudaStreamSynchronize(c->band_stream[k]), cudaStreamDestroy(c->band_stream[k]);
         if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
@@ -264,6 +269,27 @@ static int tile_args(const dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uin
     return make_tile_args(x0, y0, tw, th, spp, seed, base, tile, A);
 }
 
+// Camera leaf list storage of a persistent launch: slot 0 for the asynchronous
+// render, 1 + (band & 1) for the blocking render's band streams (head_off: the
+// band's first pixel among the tile's headers).  A failed allocation leaves
+// the launch without lists (its camera segments traverse).
+static CamLists cam_lists(dr_ctx *c, uint32_t slot, size_t head_pixels, size_t head_off) {
+    CamLists L;
+    DevBuf<uint4> &head = slot ? c->band_cam_head : c->cam_head;
+    DevBuf<uint4> &pool = slot ? c->band_cam_pool : c->cam_pool;
+    const size_t pool_n = (slot ? 2u : 1u) * (size_t)dr_ctx::kCamPool;
+    if (c->cam_used.reserve(3) != cudaSuccess || head.reserve(head_pixels) != cudaSuccess ||
+        pool.reserve(pool_n) != cudaSuccess) {
+        cudaGetLastError();  // not an error of the render
+        return L;
+    }
+    L.head = head.p + head_off;
+    L.pool = pool.p + (slot == 2 ? (size_t)dr_ctx::kCamPool : 0u);
+    L.cap = dr_ctx::kCamPool;
+    L.used = c->cam_used.p + slot;
+    return L;
+}
+
 int dr_render_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                          uint64_t sample_base, float *sun_dev, float *sky_dev, void *stream) {
     if (!c || !sun_dev || !sky_dev) return need(false, DR_ERR_INVALID, "dr_render_tile_async: null argument");
@@ -281,8 +307,9 @@ int dr_render_tile_async(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint3
                                    c->counters.p, st),
                 "render: launch");
     } else {
+        const CamLists lists = cam_lists(c, 0, (size_t)A.cols * A.rows, 0);
         DR_CUDA(launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, (float4 *)sun_dev, (float4 *)sky_dev,
-                                         c->counters.p, c->work.p, c->tuning, c->device, st),
+                                         c->counters.p, c->work.p, c->tuning, c->device, st, lists),
                 "render: launch");
     }
     return DR_OK;
@@ -418,7 +445,8 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
             err = launch_render_tile(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->call_counters.p, bs);
         else
             err = launch_render_persistent(c->scene, c->params, A, c->mie_pack.p, sd, kd, c->call_counters.p,
-                                           c->band_work.p + k, c->tuning, c->device, bs);
+                                           c->band_work.p + k, c->tuning, c->device, bs,
+                                           cam_lists(c, 1u + (k & 1u), (size_t)rows * A.cols, (size_t)r0 * A.cols));
         if (err == cudaSuccess) err = cudaEventRecord(c->band_done[k], bs);
         if (err == cudaSuccess) err = cudaStreamWaitEvent(c->copy_stream, c->band_done[k], 0);
         if (err == cudaSuccess)

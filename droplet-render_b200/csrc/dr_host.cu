@@ -334,6 +334,8 @@ int make_tile_args(uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t 
     A.seed = seed;
     A.sample_base = base;
     A.defer_sky = 0;
+    A.cam_head = nullptr;
+    A.cam_pool = nullptr;
     A.spp_div = make_fastdiv(spp);
     A.cols_div = make_fastdiv(A.cols);
     A.t2_div = make_fastdiv(tile * tile);

@@ -152,6 +152,13 @@ struct dr_ctx {
     cudaEvent_t band_done[kBands] = {};
     cudaEvent_t copy_done[kBands] = {};
     dr::DevBuf<dr::WorkQueue> band_work;
+    // camera leaf lists of the persistent kernel (TileArgs::cam_head): headers
+    // per pixel of a launch and a pool of kCamPool entries with a fill counter,
+    // for the asynchronous render (slot 0) and each band stream of the blocking
+    // render (slots 1, 2); allocated on first use
+    static constexpr uint32_t kCamPool = 1u << 23;
+    dr::DevBuf<uint4> cam_head, cam_pool, band_cam_head, band_cam_pool;
+    dr::DevBuf<unsigned int> cam_used;
     float *pinned = nullptr;  // 2 * pinned_n float4: sun then sky
     size_t pinned_n = 0;
 };

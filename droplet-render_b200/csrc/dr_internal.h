@@ -129,6 +129,15 @@ struct TileArgs {
     // that escapes after scattering goes to the warp's queue of sky terms and is
     // evaluated 32 at a time (Hosek sky, no whole-path finiteness check).
     uint32_t defer_sky;
+    // Persistent kernel, stack traversals: the camera rays' leaf sequences,
+    // built once per launch by camera_list_kernel (every sample of a pixel
+    // shares its camera ray).  cam_head[iy * cols + ix] = (first entry in
+    // cam_pool, leaves, node visits of the root test, node visits after the
+    // last leaf), or x = ~0 when the pixel's list did not fit (its samples
+    // traverse); cam_pool entries = (leaf, tra bits, trb bits, node visits
+    // since the previous leaf).  Null: every segment traverses.
+    const uint4 *cam_head;
+    const uint4 *cam_pool;
 };
 
 struct DevCounters {

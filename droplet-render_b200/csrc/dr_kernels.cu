@@ -199,6 +199,9 @@ template <bool WALK> struct SegTrav;
 template <> struct SegTrav<true> { Walk w; };
 template <> struct SegTrav<false> { Trav t; };
 
+// PathLane::wmode of a camera segment that reads its pixel's leaf list
+constexpr uint32_t kWalkListed = 4;
+
 template <bool WALK>
 struct PathLane {
     // path
@@ -211,7 +214,8 @@ struct PathLane {
     float srd[3], tn[3], sw[3];  // pending continuation while the shadow segment runs
     // segment
     SegTrav<WALK> st;
-    uint32_t wmode;  // 0 no leaf on the ray, 1 cell walk, 2 stack traversal in local memory, 3 stack traversal
+    uint32_t wmode;  // 0 no leaf on the ray, 1 cell walk, 2 stack traversal in local memory, 3 stack traversal,
+                     // 4 (kWalkListed) the pixel's camera leaf list
     float td, depth;
     uint32_t budget;
     uint32_t esc;  // segment result: kTrackCollided, kTrackEscaped or kTrackCut
@@ -287,15 +291,32 @@ __device__ __forceinline__ void finish_path(PathLane<WALK> &L, const DevParams &
 // entries) instead of the lane's local arrays nstack / tstack.
 template <bool WALK, uint32_t FEAT, bool SHS>
 __device__ __forceinline__ uint32_t trav_step(PathLane<WALK> &L, const DevScene &S, const DevParams &P,
-                                              uint32_t *nstack, Trav *slow, Count &cnt, uint32_t visits,
-                                              float (*tstack)[6], float *shcol, int shlevels) {
+                                              const uint4 *cam_pool, uint32_t *nstack, Trav *slow, Count &cnt,
+                                              uint32_t visits, float (*tstack)[6], float *shcol, int shlevels) {
     uint32_t leaf = 0;
     float tra = 0.0f, trb = 0.0f;
     uint32_t r;
     if constexpr (!WALK) {
         // at most `visits` examinations per loop iteration (0: up to the next leaf)
         const uint32_t budget = visits ? visits : 0xffffffffu;
-        if constexpr (SHS)
+        if (L.wmode == kWalkListed) {
+            // camera segment: the next leaf of the pixel's list (node = next
+            // entry, l = entries left, tn = node visits after the last leaf)
+            if (L.st.t.l > 0) {
+                const uint4 e = __ldg(&cam_pool[L.st.t.node]);
+                ++L.st.t.node;
+                --L.st.t.l;
+                leaf = e.x;
+                tra = __uint_as_float(e.y);
+                trb = __uint_as_float(e.z);
+                cnt.node_visits += e.w;
+                r = kTravLeaf;
+            } else {
+                cnt.node_visits += L.st.t.tn;
+                L.st.t.tn = 0;
+                r = kTravDone;
+            }
+        } else if constexpr (SHS)
             r = L.wmode == 3u ? trav_next_s(L.st.t, S, SharedStack<kPersistentBlock>{shcol, shlevels}, leaf, tra,
                                             trb, cnt, budget)
                               : kTravDone;
@@ -535,7 +556,25 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     L.r = 0;
     L.seg = kSegMain;
     L.depth = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
-    begin_segment(L, S, P.step_budget, cnt, state, slow);
+    bool listed = false;
+    if constexpr (!WALK) {
+        const uint4 h = A.cam_head ? __ldg(&A.cam_head[(size_t)iy * A.cols + ix]) : make_uint4(kNone, 0u, 0u, 0u);
+        if (h.x != kNone) {
+            // the pixel's camera leaf list: what trav_init and the traversal
+            // would find, node visits included (h.z = 1: the root test passed)
+            ++cnt.vertices;
+            cnt.node_visits += h.z;
+            L.wmode = h.z ? kWalkListed : 0u;
+            L.st.t.node = h.x;
+            L.st.t.l = (int)h.y;
+            L.st.t.tn = h.w;
+            L.td = 0.0f;
+            L.budget = P.step_budget;
+            state = kTrav;
+            listed = true;
+        }
+    }
+    if (!listed) begin_segment(L, S, P.step_budget, cnt, state, slow);
     // A camera ray that misses the root box draws no random number: its
     // sample is exactly zero.  Seed the stream only for rays that enter.
     if (L.wmode != 0u) L.g = rng_seed(A.seed, (uint64_t)L.py * P.w + L.px, A.sample_base + shift + s);
@@ -553,7 +592,8 @@ __device__ __forceinline__ void lane_work(PathLane<WALK> &L, bool events, const 
         return;
     }
     if (state == kTrav) {
-        const uint32_t r = trav_step<WALK, FEAT, SHS>(L, S, P, nstack, slow, cnt, visits, tstack, shcol, shlevels);
+        const uint32_t r =
+            trav_step<WALK, FEAT, SHS>(L, S, P, A.cam_pool, nstack, slow, cnt, visits, tstack, shcol, shlevels);
         if (r == 1u) {
             state = kStep;
         } else if (r == 2u) {
@@ -768,6 +808,51 @@ __global__ void add_counters_kernel(DevCounters *dst, const DevCounters *src) {
     dst->density_lookups += src->density_lookups;
     dst->mie_evals += src->mie_evals;
     dst->gave_up += src->gave_up;
+}
+
+// Leaf lists of the launch's camera rays (one thread per pixel of the tile):
+// the stack traversal of the pixel's camera ray run to its end, as every
+// sample of the pixel would run it, recorded for the persistent kernel
+// (TileArgs::cam_head / cam_pool).  The leaves are counted first, then a
+// contiguous range of the pool is taken and filled by a second traversal; a
+// pixel whose range does not fit gets x = ~0 and its samples traverse.
+__global__ void __launch_bounds__(128) camera_list_kernel(DevScene S, DevParams P, TileArgs A, uint4 *head,
+                                                          uint4 *pool, uint32_t cap, unsigned int *used) {
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= A.cols * A.rows) return;
+    const uint32_t iy = pix / A.cols, ix = pix - iy * A.cols;
+    float ro[3], rd[3];
+    uint4 h = make_uint4(0u, 0u, 0u, 0u);
+    if (camera_ray(P, A.x0 + ix, A.y0 + iy, ro, rd)) {
+        uint32_t nstack[kMaxDepth];
+        float tstack[kMaxDepth][6];
+        Trav T;
+        Count c;
+        c.zero();
+        trav_init(T, S, ro, rd, c);
+        h.z = c.node_visits;
+        uint32_t leaf, n = 0;
+        float tra, trb;
+        while (trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack) == kTravLeaf) ++n;
+        const unsigned int off = n ? atomicAdd(used, n) : 0u;
+        if (n && (off > cap || n > cap - off)) {
+            h.x = kNone;
+        } else {
+            h.x = off;
+            h.y = n;
+            c.zero();
+            trav_init(T, S, ro, rd, c);
+            c.zero();
+            for (uint32_t k = 0; k < n; ++k) {
+                trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);
+                pool[off + k] = make_uint4(leaf, __float_as_uint(tra), __float_as_uint(trb), (uint32_t)c.node_visits);
+                c.zero();
+            }
+            trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);  // kTravDone
+            h.w = c.node_visits;
+        }
+    }
+    head[pix] = h;
 }
 
 // ---- parity probes ------------------------------------------------------------
@@ -1575,7 +1660,7 @@ static uint32_t shared_stack_plan(Tuning &tune, uint32_t feat, uint32_t stack_le
 
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
-                                     const Tuning &tune_in, int device, cudaStream_t st) {
+                                     const Tuning &tune_in, int device, cudaStream_t st, const CamLists &lists) {
     if (A.n_paths == 0) return cudaSuccess;
     size_t smem = mie_smem(P);
     const uint32_t feat = frame_features(S, P);
@@ -1594,6 +1679,17 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     batch |= shlevels << 24;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
+    if (lists.head && tune.traversal != 1u) {  // the cell walk counts grid cells: it keeps its own traversal
+        e = cudaMemsetAsync(lists.used, 0, sizeof(unsigned int), st);
+        if (e != cudaSuccess) return e;
+        const uint32_t npix = A.cols * A.rows;
+        camera_list_kernel<<<(npix + 127) / 128, 128, 0, st>>>(S, P, A, lists.head, lists.pool, lists.cap,
+                                                               lists.used);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        Ad.cam_head = lists.head;
+        Ad.cam_pool = lists.pool;
+    }
     fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, Ad, mie_pack, sun_out, sky_out, C, Q, batch, BatchArgs{});
     return cudaGetLastError();
 }

@@ -12,10 +12,20 @@ cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const Tile
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
 cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const TileArgs &A, float4 *out, DevCounters *C,
                                cudaStream_t st);
+// Camera leaf list storage for one persistent launch: head[cols * rows],
+// pool[cap] and its fill counter (head null: no lists).
+struct CamLists {
+    uint4 *head = nullptr;
+    uint4 *pool = nullptr;
+    uint32_t cap = 0;
+    unsigned int *used = nullptr;
+};
 // Persistent path kernel; Q->next must be 0 (the launcher clears it on st).
+// With a stack traversal and lists given, the camera rays' leaf lists are built
+// on st first (camera_list_kernel).
 cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
                                      float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
-                                     const Tuning &tune, int device, cudaStream_t st);
+                                     const Tuning &tune, int device, cudaStream_t st, const CamLists &lists = {});
 // Batched persistent launch over all views of B (P0: the first view's parameters,
 // which fix the shared phase tables), then one increment of *step; Q->next is
 // cleared on st first.  The three launches are what a batch's graph captures.
