@@ -216,6 +216,16 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     d.step_budget = c->step_budget;
     c->params = d;
     c->has_params = true;
+    // camera leaf list storage for tiles up to the whole frame, so that renders
+    // allocate nothing (without it their camera segments traverse)
+    const size_t frame = (size_t)p->w * p->h;
+    if (c->cam_used.reserve(3) != cudaSuccess || c->cam_head.reserve(frame) != cudaSuccess ||
+        c->band_cam_head.reserve(frame) != cudaSuccess || c->cam_pool.reserve(dr_ctx::kCamPool) != cudaSuccess ||
+        c->band_cam_pool.reserve(2 * (size_t)dr_ctx::kCamPool) != cudaSuccess) {
+        c->cam_head.release();
+        c->band_cam_head.release();
+        cudaGetLastError();  // not an error of the parameters
+    }
     return DR_OK;
 }
 

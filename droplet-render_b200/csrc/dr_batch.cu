@@ -31,6 +31,11 @@ struct dr_batch {
     DevBuf<unsigned char> mie_pack;
     DevBuf<WorkQueue> work;
     DevBuf<unsigned long long> step;
+    // camera leaf lists (one header per pixel of every view, one entry pool)
+    DevBuf<uint4> cam_head, cam_pool;
+    DevBuf<unsigned int> cam_used;
+    DevBuf<uint32_t> pix_begins;
+    uint32_t n_pix = 0;
     std::vector<BatchView> host_views;
     std::vector<size_t> out_off;  // float4 offset of view v's sun tile; its sky tile follows
     size_t out_n = 0;             // float4 count of all outputs
@@ -57,8 +62,13 @@ int build_graph(dr_batch *b) {
     drop_graph(b);
     bool ext = b->any_sdf;  // surface leaves, or a view with the HG phase or a non-Hosek environment
     for (const BatchView &v : b->host_views) ext = ext || v.P.phase_mode == kPhaseHG || v.P.env_mode != kEnvHosek;
+    // camera leaf lists for the stack traversals (the cell walk counts grid
+    // cells and keeps its own traversal); without the storage the views traverse
+    const bool lists = b->tuning.traversal != 1u && b->cam_head.p && b->cam_pool.p && b->cam_used.p;
     uint64_t begin = 0;
+    uint32_t pix = 0;
     std::vector<uint64_t> begins(b->host_views.size());
+    std::vector<uint32_t> pix_begins(b->host_views.size());
     for (size_t v = 0; v < b->host_views.size(); ++v) {
         BatchView &V = b->host_views[v];
         TileArgs A;
@@ -66,6 +76,12 @@ int build_graph(dr_batch *b) {
         if (rc != DR_OK) return rc;
         // sky terms through the warps' queues (not with a whole-path finiteness check)
         A.defer_sky = (!ext && !V.P.finite_paths) ? 1u : 0u;
+        pix_begins[v] = pix;
+        if (lists) {
+            A.cam_head = b->cam_head.p + pix;
+            A.cam_pool = b->cam_pool.p;
+        }
+        pix += A.cols * A.rows;
         V.A = A;
         V.begin = begin;
         begins[v] = begin;
@@ -77,6 +93,18 @@ int build_graph(dr_batch *b) {
             "dr_batch: copy views");
     DR_CUDA(cudaMemcpy(b->begins.p, begins.data(), sizeof(uint64_t) * begins.size(), cudaMemcpyHostToDevice),
             "dr_batch: copy views");
+    DR_CUDA(cudaMemcpy(b->pix_begins.p, pix_begins.data(), sizeof(uint32_t) * pix_begins.size(),
+                       cudaMemcpyHostToDevice),
+            "dr_batch: copy views");
+    BatchLists bl;
+    if (lists) {
+        bl.lists.head = b->cam_head.p;
+        bl.lists.pool = b->cam_pool.p;
+        bl.lists.cap = (uint32_t)b->cam_pool.n;
+        bl.lists.used = b->cam_used.p;
+        bl.pix_begins = b->pix_begins.p;
+        bl.n_pix = pix;
+    }
     BatchArgs B;
     B.views = b->views.p;
     B.scenes = b->scenes.p;
@@ -88,7 +116,7 @@ int build_graph(dr_batch *b) {
     cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
     if (e == cudaSuccess)
         e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
-                                b->stack_levels, b->ctx->device, b->stream);
+                                b->stack_levels, b->ctx->device, b->stream, bl);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) {
@@ -112,6 +140,10 @@ void release(dr_batch *b) {
     b->mie_pack.release();
     b->work.release();
     b->step.release();
+    b->cam_head.release();
+    b->cam_pool.release();
+    b->cam_used.release();
+    b->pix_begins.release();
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
 }
@@ -214,6 +246,21 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
                "dr_batch_create: copy scenes");
     BATCH_CUDA(b->views.reserve(n_views), "dr_batch_create: alloc views");
     BATCH_CUDA(b->begins.reserve(n_views), "dr_batch_create: alloc views");
+    BATCH_CUDA(b->pix_begins.reserve(n_views), "dr_batch_create: alloc views");
+    {
+        // camera leaf lists: a header per pixel, a pool of up to 4 leaves per
+        // pixel (at most 2^26 entries); without them the views traverse
+        uint64_t n_pix = 0;
+        for (uint32_t v = 0; v < n_views; ++v) n_pix += (uint64_t)hv[v].A.cols * hv[v].A.rows;
+        const uint64_t n_pool = std::min<uint64_t>(4 * n_pix, 1ull << 26);
+        if (n_pix == 0 || n_pix >= (1ull << 31) || b->cam_head.reserve(n_pix) != cudaSuccess ||
+            b->cam_pool.reserve(n_pool) != cudaSuccess || b->cam_used.reserve(1) != cudaSuccess) {
+            b->cam_head.release();
+            b->cam_pool.release();
+            b->cam_used.release();
+            cudaGetLastError();  // not an error of the batch
+        }
+    }
     BATCH_CUDA(b->mie_pack.reserve(pack0.size()), "dr_batch_create: alloc tables");
     BATCH_CUDA(cudaMemcpy(b->mie_pack.p, pack0.data(), pack0.size(), cudaMemcpyHostToDevice),
                "dr_batch_create: copy tables");

@@ -810,49 +810,73 @@ __global__ void add_counters_kernel(DevCounters *dst, const DevCounters *src) {
     dst->gave_up += src->gave_up;
 }
 
-// Leaf lists of the launch's camera rays (one thread per pixel of the tile):
-// the stack traversal of the pixel's camera ray run to its end, as every
-// sample of the pixel would run it, recorded for the persistent kernel
-// (TileArgs::cam_head / cam_pool).  The leaves are counted first, then a
-// contiguous range of the pool is taken and filled by a second traversal; a
-// pixel whose range does not fit gets x = ~0 and its samples traverse.
+// Leaf list of one camera ray (pixel ix, iy of the tile A): the stack
+// traversal of the pixel's camera ray run to its end, as every sample of the
+// pixel would run it, recorded for the persistent kernel (TileArgs::cam_head /
+// cam_pool).  The leaves are counted first, then a contiguous range of the
+// pool is taken and filled by a second traversal; a pixel whose range does not
+// fit gets x = ~0 and its samples traverse.
+__device__ __forceinline__ uint4 camera_list(const DevScene &S, const DevParams &P, const TileArgs &A, uint32_t ix,
+                                             uint32_t iy, uint4 *pool, uint32_t cap, unsigned int *used) {
+    float ro[3], rd[3];
+    uint4 h = make_uint4(0u, 0u, 0u, 0u);
+    if (!camera_ray(P, A.x0 + ix, A.y0 + iy, ro, rd)) return h;
+    uint32_t nstack[kMaxDepth];
+    float tstack[kMaxDepth][6];
+    Trav T;
+    Count c;
+    c.zero();
+    trav_init(T, S, ro, rd, c);
+    h.z = c.node_visits;
+    uint32_t leaf, n = 0;
+    float tra, trb;
+    while (trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack) == kTravLeaf) ++n;
+    const unsigned int off = n ? atomicAdd(used, n) : 0u;
+    if (n && (off > cap || n > cap - off)) {
+        h.x = kNone;
+        return h;
+    }
+    h.x = off;
+    h.y = n;
+    trav_init(T, S, ro, rd, c);
+    c.zero();
+    for (uint32_t k = 0; k < n; ++k) {
+        trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);
+        pool[off + k] = make_uint4(leaf, __float_as_uint(tra), __float_as_uint(trb), c.node_visits);
+        c.zero();
+    }
+    trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);  // kTravDone
+    h.w = c.node_visits;
+    return h;
+}
+
+// The camera leaf lists of a single-tile launch (one thread per pixel).
 __global__ void __launch_bounds__(128) camera_list_kernel(DevScene S, DevParams P, TileArgs A, uint4 *head,
                                                           uint4 *pool, uint32_t cap, unsigned int *used) {
     const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= A.cols * A.rows) return;
     const uint32_t iy = pix / A.cols, ix = pix - iy * A.cols;
-    float ro[3], rd[3];
-    uint4 h = make_uint4(0u, 0u, 0u, 0u);
-    if (camera_ray(P, A.x0 + ix, A.y0 + iy, ro, rd)) {
-        uint32_t nstack[kMaxDepth];
-        float tstack[kMaxDepth][6];
-        Trav T;
-        Count c;
-        c.zero();
-        trav_init(T, S, ro, rd, c);
-        h.z = c.node_visits;
-        uint32_t leaf, n = 0;
-        float tra, trb;
-        while (trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack) == kTravLeaf) ++n;
-        const unsigned int off = n ? atomicAdd(used, n) : 0u;
-        if (n && (off > cap || n > cap - off)) {
-            h.x = kNone;
-        } else {
-            h.x = off;
-            h.y = n;
-            c.zero();
-            trav_init(T, S, ro, rd, c);
-            c.zero();
-            for (uint32_t k = 0; k < n; ++k) {
-                trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);
-                pool[off + k] = make_uint4(leaf, __float_as_uint(tra), __float_as_uint(trb), (uint32_t)c.node_visits);
-                c.zero();
-            }
-            trav_next_k(T, S, nstack, leaf, tra, trb, c, 0xffffffffu, tstack);  // kTravDone
-            h.w = c.node_visits;
-        }
+    head[pix] = camera_list(S, P, A, ix, iy, pool, cap, used);
+}
+
+// The camera leaf lists of every view of a batch: pixel p of the batch belongs
+// to the last view v with pix_begins[v] <= p; its header is head[p] (the view's
+// TileArgs::cam_head points at head + pix_begins[v]).
+__global__ void __launch_bounds__(128) batch_camera_list_kernel(BatchArgs B, const uint32_t *pix_begins,
+                                                                uint32_t n_pix, uint4 *head, uint4 *pool,
+                                                                uint32_t cap, unsigned int *used) {
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= n_pix) return;
+    uint32_t lo = 0, hi = B.n_views - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&pix_begins[mid]) <= pix) lo = mid;
+        else hi = mid - 1;
     }
-    head[pix] = h;
+    const BatchView &V = B.views[lo];
+    const uint32_t q = pix - __ldg(&pix_begins[lo]);
+    const uint32_t iy = q / V.A.cols, ix = q - iy * V.A.cols;
+    head[pix] = camera_list(B.scenes[V.scene], V.P, V.A, ix, iy, pool, cap, used);
 }
 
 // ---- parity probes ------------------------------------------------------------
@@ -1696,7 +1720,7 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
                                 WorkQueue *Q, unsigned long long *step, const Tuning &tune_in, bool ext,
-                                uint32_t stack_levels, int device, cudaStream_t st) {
+                                uint32_t stack_levels, int device, cudaStream_t st, const BatchLists &lists) {
     size_t smem = mie_smem(P0);
     Tuning tune = tune_in;
     const uint32_t shlevels = shared_stack_plan(tune, ext ? kFeatAll : 0u, stack_levels, smem);
@@ -1709,6 +1733,14 @@ cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const v
     batch |= shlevels << 24;
     e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
     if (e != cudaSuccess) return e;
+    if (B.n_paths && lists.lists.head && lists.n_pix) {  // the views' TileArgs point into these lists
+        e = cudaMemsetAsync(lists.lists.used, 0, sizeof(unsigned int), st);
+        if (e != cudaSuccess) return e;
+        batch_camera_list_kernel<<<(lists.n_pix + 127) / 128, 128, 0, st>>>(
+            B, lists.pix_begins, lists.n_pix, lists.lists.head, lists.lists.pool, lists.lists.cap, lists.lists.used);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     if (B.n_paths) {
         fn<<<blocks, kPersistentBlock, smem, st>>>(DevScene{}, DevParams{}, TileArgs{}, mie_pack, nullptr, nullptr, C,
                                                    Q, batch, B);

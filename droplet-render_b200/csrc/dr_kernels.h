@@ -30,9 +30,16 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
 // which fix the shared phase tables), then one increment of *step; Q->next is
 // cleared on st first.  The three launches are what a batch's graph captures.
 // stack_levels: the deepest traversal stack any of the batch's scenes needs (0: unknown)
+// lists: the views' camera leaf lists (the views' TileArgs::cam_head point at
+// lists.head + pix_begins[v]; head null when the views traverse), built first.
+struct BatchLists {
+    CamLists lists;
+    const uint32_t *pix_begins = nullptr;  // first pixel of each view among the batch's pixels
+    uint32_t n_pix = 0;
+};
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
                                 WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext,
-                                uint32_t stack_levels, int device, cudaStream_t st);
+                                uint32_t stack_levels, int device, cudaStream_t st, const BatchLists &lists = {});
 // Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,
