@@ -227,7 +227,7 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
         "small_views": small,
         "tuning": {"choice": list(best), "seconds": round(t_tune, 2), "probe": "centre <=128^2 crops, 4 spp",
                    "top": [[c, round(m, 3)] for c, m in table[:6]]},
-        "graph": "memset outputs -> persistent kernel over all views -> step counter", "build_s": round(t_build, 1),
+        "graph": "memset outputs -> camera leaf lists of every view -> persistent kernel over all views -> step counter", "build_s": round(t_build, 1),
         "l2": "flushed before each timed launch (256 MB write)",
     }
 
