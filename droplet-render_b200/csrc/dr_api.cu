@@ -220,12 +220,21 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     // allocate nothing (without it their camera segments traverse)
     const size_t frame = (size_t)p->w * p->h;
     if (c->cam_used.reserve(3) != cudaSuccess || c->cam_head.reserve(frame) != cudaSuccess ||
-        c->band_cam_head.reserve(frame) != cudaSuccess || c->cam_pool.reserve(dr_ctx::kCamPool) != cudaSuccess ||
-        c->band_cam_pool.reserve(2 * (size_t)dr_ctx::kCamPool) != cudaSuccess) {
+        c->band_cam_head.reserve(frame) != cudaSuccess || c->cam_pool.reserve(c->cam_cap) != cudaSuccess ||
+        c->band_cam_pool.reserve(2 * (size_t)c->cam_cap) != cudaSuccess) {
         c->cam_head.release();
         c->band_cam_head.release();
         cudaGetLastError();  // not an error of the parameters
     }
+    return DR_OK;
+}
+
+int dr_set_camera_lists(dr_ctx *c, uint32_t pool_entries) {
+    if (!c) return need(false, DR_ERR_INVALID, "dr_set_camera_lists: null context");
+    if (pool_entries != DR_NONE && pool_entries > (1u << 28))
+        return need(false, DR_ERR_INVALID, "dr_set_camera_lists: at most 2^28 entries per pool");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->cam_cap = pool_entries == DR_NONE ? 0u : pool_entries ? pool_entries : dr_ctx::kCamPool;
     return DR_OK;
 }
 
@@ -285,17 +294,18 @@ static int tile_args(const dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uin
 // the launch without lists (its camera segments traverse).
 static CamLists cam_lists(dr_ctx *c, uint32_t slot, size_t head_pixels, size_t head_off) {
     CamLists L;
+    if (c->cam_cap == 0) return L;
     DevBuf<uint4> &head = slot ? c->band_cam_head : c->cam_head;
     DevBuf<uint4> &pool = slot ? c->band_cam_pool : c->cam_pool;
-    const size_t pool_n = (slot ? 2u : 1u) * (size_t)dr_ctx::kCamPool;
+    const size_t pool_n = (slot ? 2u : 1u) * (size_t)c->cam_cap;
     if (c->cam_used.reserve(3) != cudaSuccess || head.reserve(head_pixels) != cudaSuccess ||
         pool.reserve(pool_n) != cudaSuccess) {
         cudaGetLastError();  // not an error of the render
         return L;
     }
     L.head = head.p + head_off;
-    L.pool = pool.p + (slot == 2 ? (size_t)dr_ctx::kCamPool : 0u);
-    L.cap = dr_ctx::kCamPool;
+    L.pool = pool.p + (slot == 2 ? (size_t)c->cam_cap : 0u);
+    L.cap = c->cam_cap;
     L.used = c->cam_used.p + slot;
     return L;
 }

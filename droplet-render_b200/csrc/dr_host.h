@@ -157,6 +157,7 @@ struct dr_ctx {
     // for the asynchronous render (slot 0) and each band stream of the blocking
     // render (slots 1, 2); allocated on first use
     static constexpr uint32_t kCamPool = 1u << 23;
+    uint32_t cam_cap = kCamPool;  // entries per pool (dr_set_camera_lists; 0: no lists)
     dr::DevBuf<uint4> cam_head, cam_pool, band_cam_head, band_cam_pool;
     dr::DevBuf<unsigned int> cam_used;
     float *pinned = nullptr;  // 2 * pinned_n float4: sun then sky

@@ -191,6 +191,7 @@ SIGNATURES = {
     "dr_synchronize": (C.c_int, [C.c_void_p]),
     "dr_check_complete": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dr_set_step_budget": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "dr_set_camera_lists": (C.c_int, [C.c_void_p, C.c_uint32]),
     "dr_set_bricks_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]),
     "dr_get_majorants": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dr_adjoint_tile_async": (

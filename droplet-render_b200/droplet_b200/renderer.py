@@ -252,6 +252,11 @@ class Renderer:
         """Tracking steps a path segment may take before it gives up (0: 2^24)."""
         N.check(N.lib().dr_set_step_budget(self._ctx, int(steps)))
 
+    def set_camera_lists(self, pool_entries: int = 0):
+        """Entries per camera leaf list pool (0: the default 2^23; N.DR_NONE: no
+        lists).  Results and counters do not depend on it."""
+        N.check(N.lib().dr_set_camera_lists(self._ctx, int(pool_entries)))
+
     def set_tuning(self, kernel: int = 0, blocks_per_sm: int = 0, event_batch: int = 0, traversal: int = 0,
                    tile: int = 0, visits: int = 0, steps: int = 0):
         t = N.DrTuning(int(kernel), int(blocks_per_sm), int(event_batch), int(traversal), int(tile), int(visits),

@@ -239,6 +239,15 @@ int dr_check_complete(dr_ctx *ctx, void *stream);
  * the segment ends); a small budget makes give-ups reproducible in tests. */
 int dr_set_step_budget(dr_ctx *ctx, uint32_t steps);
 
+/* Camera leaf lists of the persistent kernel: before a launch, each pixel's
+ * camera ray is traversed once and its samples read the leaf sequence instead
+ * of traversing (every sample of a pixel shares its camera ray).  Results and
+ * counters are the same with or without them.  pool_entries: entries of 16
+ * bytes per list pool (0 = the default 2^23; DR_NONE = no lists); the pixels
+ * whose lists do not fit traverse.  Applies to later renders of the context.
+ * No reference counterpart (the reference traverses per sample). */
+int dr_set_camera_lists(dr_ctx *ctx, uint32_t pool_entries);
+
 /* ---- launch shape (no reference counterpart: the reference schedules 2x2
  * pixel blocks with TBB, src/kernel.cpp:453) ------------------------------- */
 #define DR_KERNEL_PERSISTENT 0u  /* resident warps take paths from a queue (default) */
