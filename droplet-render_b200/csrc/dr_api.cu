@@ -219,8 +219,8 @@ int dr_set_params(dr_ctx *c, const dr_render_params *p) {
     // camera leaf list storage for tiles up to the whole frame, so that renders
     // allocate nothing (without it their camera segments traverse)
     const size_t frame = (size_t)p->w * p->h;
-    if (c->cam_used.reserve(3) != cudaSuccess || c->cam_head.reserve(frame) != cudaSuccess ||
-        c->band_cam_head.reserve(frame) != cudaSuccess || c->cam_pool.reserve(c->cam_cap) != cudaSuccess ||
+    if (c->cam_used.reserve(3) != cudaSuccess || c->cam_head.reserve(2 * frame) != cudaSuccess ||
+        c->band_cam_head.reserve(2 * frame) != cudaSuccess || c->cam_pool.reserve(c->cam_cap) != cudaSuccess ||
         c->band_cam_pool.reserve(2 * (size_t)c->cam_cap) != cudaSuccess) {
         c->cam_head.release();
         c->band_cam_head.release();
@@ -298,12 +298,12 @@ static CamLists cam_lists(dr_ctx *c, uint32_t slot, size_t head_pixels, size_t h
     DevBuf<uint4> &head = slot ? c->band_cam_head : c->cam_head;
     DevBuf<uint4> &pool = slot ? c->band_cam_pool : c->cam_pool;
     const size_t pool_n = (slot ? 2u : 1u) * (size_t)c->cam_cap;
-    if (c->cam_used.reserve(3) != cudaSuccess || head.reserve(head_pixels) != cudaSuccess ||
+    if (c->cam_used.reserve(3) != cudaSuccess || head.reserve(2 * head_pixels) != cudaSuccess ||
         pool.reserve(pool_n) != cudaSuccess) {
         cudaGetLastError();  // not an error of the render
         return L;
     }
-    L.head = head.p + head_off;
+    L.head = head.p + 2 * head_off;
     L.pool = pool.p + (slot == 2 ? (size_t)c->cam_cap : 0u);
     L.cap = c->cam_cap;
     L.used = c->cam_used.p + slot;

@@ -78,7 +78,7 @@ int build_graph(dr_batch *b) {
         A.defer_sky = (!ext && !V.P.finite_paths) ? 1u : 0u;
         pix_begins[v] = pix;
         if (lists) {
-            A.cam_head = b->cam_head.p + pix;
+            A.cam_head = b->cam_head.p + 2 * (size_t)pix;
             A.cam_pool = b->cam_pool.p;
         }
         pix += A.cols * A.rows;
@@ -248,12 +248,12 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
     BATCH_CUDA(b->begins.reserve(n_views), "dr_batch_create: alloc views");
     BATCH_CUDA(b->pix_begins.reserve(n_views), "dr_batch_create: alloc views");
     {
-        // camera leaf lists: a header per pixel, a pool of up to 4 leaves per
+        // camera leaf lists: two header words per pixel, a pool of up to 4 leaves per
         // pixel (at most 2^26 entries); without them the views traverse
         uint64_t n_pix = 0;
         for (uint32_t v = 0; v < n_views; ++v) n_pix += (uint64_t)hv[v].A.cols * hv[v].A.rows;
         const uint64_t n_pool = std::min<uint64_t>(4 * n_pix, 1ull << 26);
-        if (n_pix == 0 || n_pix >= (1ull << 31) || b->cam_head.reserve(n_pix) != cudaSuccess ||
+        if (n_pix == 0 || n_pix >= (1ull << 31) || b->cam_head.reserve(2 * n_pix) != cudaSuccess ||
             b->cam_pool.reserve(n_pool) != cudaSuccess || b->cam_used.reserve(1) != cudaSuccess) {
             b->cam_head.release();
             b->cam_pool.release();

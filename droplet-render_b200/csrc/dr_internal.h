@@ -131,11 +131,13 @@ struct TileArgs {
     uint32_t defer_sky;
     // Persistent kernel, stack traversals: the camera rays' leaf sequences,
     // built once per launch by camera_list_kernel (every sample of a pixel
-    // shares its camera ray).  cam_head[iy * cols + ix] = (first entry in
-    // cam_pool, leaves, node visits of the root test, node visits after the
-    // last leaf), or x = ~0 when the pixel's list did not fit (its samples
-    // traverse); cam_pool entries = (leaf, tra bits, trb bits, node visits
-    // since the previous leaf).  Null: every segment traverses.
+    // shares its camera ray).  Pixel q = iy * cols + ix: cam_head[2q] = (first
+    // entry in cam_pool, leaves, node visits of the root test, node visits
+    // after the last leaf), or x = ~0 when the pixel's list did not fit (its
+    // samples traverse); cam_head[2q + 1] = (the ray's direction bits, 1 if the
+    // pixel has a ray); cam_pool entries = (leaf, tra bits, trb bits, node
+    // visits since the previous leaf).  Null: rays are generated per sample and
+    // every segment traverses.
     const uint4 *cam_head;
     const uint4 *cam_pool;
 };

@@ -548,7 +548,25 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     }
     L.px = A.x0 + ix;
     L.py = A.y0 + iy;
-    if (!camera_ray(P, L.px, L.py, L.ro, L.rd)) return false;
+    // the pixel's header (leaf list and camera ray, every sample of the pixel
+    // shares them), or none: the ray is generated and the segment traverses
+    uint4 h = make_uint4(kNone, 0u, 0u, 0u);
+    if constexpr (!WALK) {
+        if (A.cam_head) {
+            const size_t hx = 2 * ((size_t)iy * A.cols + ix);
+            h = __ldg(&A.cam_head[hx]);
+            const uint4 ray = __ldg(&A.cam_head[hx + 1]);
+            if (!ray.w) return false;
+            for (int k = 0; k < 3; ++k) L.ro[k] = P.viewi[12 + k];  // camera_ray's origin
+            L.rd[0] = __uint_as_float(ray.x);
+            L.rd[1] = __uint_as_float(ray.y);
+            L.rd[2] = __uint_as_float(ray.z);
+        } else if (!camera_ray(P, L.px, L.py, L.ro, L.rd)) {
+            return false;
+        }
+    } else {
+        if (!camera_ray(P, L.px, L.py, L.ro, L.rd)) return false;
+    }
     ++paths;
     L.T[0] = L.T[1] = L.T[2] = 1.0f;
     L.sun = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -558,7 +576,6 @@ __device__ __forceinline__ bool start_path(PathLane<WALK> &L, uint64_t p, const 
     L.depth = (P.depth && P.depthcomp) ? __ldg(&P.depth[(size_t)L.py * P.w + L.px]) : 3.402823466e+38f;
     bool listed = false;
     if constexpr (!WALK) {
-        const uint4 h = A.cam_head ? __ldg(&A.cam_head[(size_t)iy * A.cols + ix]) : make_uint4(kNone, 0u, 0u, 0u);
         if (h.x != kNone) {
             // the pixel's camera leaf list: what trav_init and the traversal
             // would find, node visits included (h.z = 1: the root test passed)
@@ -815,12 +832,15 @@ __global__ void add_counters_kernel(DevCounters *dst, const DevCounters *src) {
 // pixel would run it, recorded for the persistent kernel (TileArgs::cam_head /
 // cam_pool).  The leaves are counted first, then a contiguous range of the
 // pool is taken and filled by a second traversal; a pixel whose range does not
-// fit gets x = ~0 and its samples traverse.
+// fit gets x = ~0 and its samples traverse.  `ray`: the ray's direction bits
+// and whether the pixel has a ray (camera_ray's result).
 __device__ __forceinline__ uint4 camera_list(const DevScene &S, const DevParams &P, const TileArgs &A, uint32_t ix,
-                                             uint32_t iy, uint4 *pool, uint32_t cap, unsigned int *used) {
+                                             uint32_t iy, uint4 *pool, uint32_t cap, unsigned int *used, uint4 &ray) {
     float ro[3], rd[3];
     uint4 h = make_uint4(0u, 0u, 0u, 0u);
-    if (!camera_ray(P, A.x0 + ix, A.y0 + iy, ro, rd)) return h;
+    const bool ok = camera_ray(P, A.x0 + ix, A.y0 + iy, ro, rd);
+    ray = make_uint4(__float_as_uint(rd[0]), __float_as_uint(rd[1]), __float_as_uint(rd[2]), ok ? 1u : 0u);
+    if (!ok) return h;
     uint32_t nstack[kMaxDepth];
     float tstack[kMaxDepth][6];
     Trav T;
@@ -856,12 +876,14 @@ __global__ void __launch_bounds__(128) camera_list_kernel(DevScene S, DevParams 
     const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= A.cols * A.rows) return;
     const uint32_t iy = pix / A.cols, ix = pix - iy * A.cols;
-    head[pix] = camera_list(S, P, A, ix, iy, pool, cap, used);
+    uint4 ray;
+    head[2 * (size_t)pix] = camera_list(S, P, A, ix, iy, pool, cap, used, ray);
+    head[2 * (size_t)pix + 1] = ray;
 }
 
 // The camera leaf lists of every view of a batch: pixel p of the batch belongs
-// to the last view v with pix_begins[v] <= p; its header is head[p] (the view's
-// TileArgs::cam_head points at head + pix_begins[v]).
+// to the last view v with pix_begins[v] <= p; its header is head[2p, 2p + 1]
+// (the view's TileArgs::cam_head points at head + 2 pix_begins[v]).
 __global__ void __launch_bounds__(128) batch_camera_list_kernel(BatchArgs B, const uint32_t *pix_begins,
                                                                 uint32_t n_pix, uint4 *head, uint4 *pool,
                                                                 uint32_t cap, unsigned int *used) {
@@ -876,7 +898,9 @@ __global__ void __launch_bounds__(128) batch_camera_list_kernel(BatchArgs B, con
     const BatchView &V = B.views[lo];
     const uint32_t q = pix - __ldg(&pix_begins[lo]);
     const uint32_t iy = q / V.A.cols, ix = q - iy * V.A.cols;
-    head[pix] = camera_list(B.scenes[V.scene], V.P, V.A, ix, iy, pool, cap, used);
+    uint4 ray;
+    head[2 * (size_t)pix] = camera_list(B.scenes[V.scene], V.P, V.A, ix, iy, pool, cap, used, ray);
+    head[2 * (size_t)pix + 1] = ray;
 }
 
 // ---- parity probes ------------------------------------------------------------

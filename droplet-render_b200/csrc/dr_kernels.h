@@ -12,7 +12,7 @@ cudaError_t launch_render_tile(const DevScene &S, const DevParams &P, const Tile
                                float4 *sun_out, float4 *sky_out, DevCounters *C, cudaStream_t st);
 cudaError_t launch_shadow_tile(const DevScene &S, const DevParams &P, const TileArgs &A, float4 *out, DevCounters *C,
                                cudaStream_t st);
-// Camera leaf list storage for one persistent launch: head[cols * rows],
+// Camera leaf list storage for one persistent launch: head[2 * cols * rows],
 // pool[cap] and its fill counter (head null: no lists).
 struct CamLists {
     uint4 *head = nullptr;
