@@ -153,22 +153,33 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
     b.set_tuning(*best)
     stream = torch.cuda.Stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    for _ in range(max(1, warmup)):
-        b.launch(stream.cuda_stream)
-    stream.synchronize()
-    r.reset_counters()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    with torch.cuda.stream(stream):
-        for k in range(steps):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
+
+    def time_launches():
+        for _ in range(max(1, warmup)):
             b.launch(stream.cuda_stream)
-            ev[k][1].record(stream)
-    stream.synchronize()
-    ms = [a.elapsed_time(e) for a, e in ev]
-    verts = r.counters()["vertices"] / steps
+        stream.synchronize()
+        r.reset_counters()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                b.launch(stream.cuda_stream)
+                ev[k][1].record(stream)
+        stream.synchronize()
+        return [a.elapsed_time(e) for a, e in ev], r.counters()["vertices"] / steps
+
+    # the library's default graph: views of at least 8 paths per lane of the
+    # grid in persistent kernels of their own, the rest in one batched kernel
+    split, own = b.get_split()
+    ms, verts = time_launches()
     n_paths, _ = b.info()
     batched = verts / (np.mean(ms) / 1e3)
+    # every view in the one batched kernel
+    b.set_split(0)
+    ms1, verts1 = time_launches()
+    single = verts1 / (np.mean(ms1) / 1e3)
+    b.set_split(split)
     # plain, one launch per view (same samples as the batch's first launch)
     r.set_tuning(*best)
     cur, plain_ms, plain_v = -1, 0.0, 0
@@ -221,13 +232,20 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
                     "(side U[128,1024], spp {16,64,256}, sun U[5,80] deg, 500 events), default_rng(2026)",
         "value": batched, "unit": "vertices/s", "ms_per_launch": float(np.mean(ms)), "launch_ms": ms,
         "vertices_per_launch": verts, "path_indices_per_launch": n_paths,
+        "split": {"min_paths": "auto: 8 paths per lane of the grid" if split == Batch.SPLIT_AUTO else split,
+                  "views_with_own_kernel": own, "of_views": len(views)},
+        "single_kernel": {"value": single, "unit": "vertices/s", "ms_per_launch": float(np.mean(ms1)),
+                          "launch_ms": ms1},
         "plain_per_view": {"value": plain, "ms": plain_ms, "launches": len(views)},
         "plain_addon_tiles_64": {"value": tiles, "seconds": t_tiles, "calls": n_tiles},
         "speedup_vs_plain_per_view": batched / plain, "speedup_vs_addon_tiles": batched / tiles,
+        "single_kernel_speedup_vs_plain_per_view": single / plain,
         "small_views": small,
         "tuning": {"choice": list(best), "seconds": round(t_tune, 2), "probe": "centre <=128^2 crops, 4 spp",
                    "top": [[c, round(m, 3)] for c, m in table[:6]]},
-        "graph": "memset outputs -> camera leaf lists of every view -> persistent kernel over all views -> step counter", "build_s": round(t_build, 1),
+        "graph": "memset outputs and queues -> camera leaf lists of every view -> {a plain persistent kernel per "
+                 "large view, one batched persistent kernel over the rest} as independent branches -> step counter",
+        "build_s": round(t_build, 1),
         "l2": "flushed before each timed launch (256 MB write)",
     }
 
@@ -1285,7 +1303,8 @@ def run_b200(args):
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = measure_batched(r, pdf, cdf, steps=2, warmup=1)
-        log(f"batched: {batched['value'] / 1e9:.3f} G vertices/s, plain per view "
+        log(f"batched: {batched['value'] / 1e9:.3f} G vertices/s ({batched['split']['views_with_own_kernel']} views "
+            f"in kernels of their own), one batched kernel {batched['single_kernel']['value'] / 1e9:.3f}, plain per view "
             f"{batched['plain_per_view']['value'] / 1e9:.3f}, addon tiles {batched['plain_addon_tiles_64']['value'] / 1e9:.3f}")
 
     if rank == 0:

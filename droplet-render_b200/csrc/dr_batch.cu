@@ -1,12 +1,18 @@
-// Batched rendering: many scenes and views in one persistent launch, replayed
-// from a CUDA graph (declared in include/droplet_b200.h, dr_batch_*).
+// Batched rendering: many scenes and views in one launch of a CUDA graph
+// (declared in include/droplet_b200.h, dr_batch_*).
 //
 // The reference renders one tile of one view per RenderKernel::Render call
 // (src/kernel.cpp:536-567).  A batch uploads every scene once, lays the paths
 // of all views out as one index space (view-major; inside a view, pixels in
 // the tuned order with consecutive samples), and captures
-//   memset(outputs) -> persistent kernel over all views -> step counter += 1
-// as a graph.  Launch k of a batch renders samples [k spp, (k+1) spp) of every
+//   memset(outputs, queues) -> camera leaf lists of every view
+//     -> persistent kernel over all views -> step counter += 1
+// as a graph.  With a split (dr_batch_set_split), each view of at least
+// min_paths paths gets a plain persistent kernel of its own instead (its
+// parameters in kernel arguments rather than per-lane records in global
+// memory); those kernels and the batched kernel over the remaining views are
+// independent branches between the lists and the step counter, on up to
+// kBranches capture streams, so a kernel's tail overlaps the next one's start.  Launch k of a batch renders samples [k spp, (k+1) spp) of every
 // view, the same streams dr_render_tile draws with sample_base = k spp.
 #include <algorithm>
 #include <cstring>
@@ -19,6 +25,11 @@
 
 using namespace dr;
 
+namespace {
+constexpr uint32_t kBranches = 4;         // capture streams of a split graph (kernels side by side)
+constexpr uint64_t kSplitAutoPerLane = 8;  // DR_BATCH_SPLIT_AUTO: paths per lane of a full grid
+}  // namespace
+
 struct dr_batch {
     dr_ctx *ctx = nullptr;
     cudaStream_t stream = nullptr;  // capture stream
@@ -29,8 +40,16 @@ struct dr_batch {
     DevBuf<uint64_t> begins;
     DevBuf<float4> out;
     DevBuf<unsigned char> mie_pack;
-    DevBuf<WorkQueue> work;
+    DevBuf<WorkQueue> work;  // [0]: the batched kernel; [1 + v]: view v's own kernel
     DevBuf<unsigned long long> step;
+    // split graphs: the views left to the batched kernel, their first path indices
+    DevBuf<BatchView> rest_views;
+    DevBuf<uint64_t> rest_begins;
+    std::vector<DevScene> host_scenes;
+    uint64_t split = DR_BATCH_SPLIT_AUTO;  // dr_batch_set_split
+    uint32_t own_kernels = 0;              // views with a kernel of their own in the current graph
+    cudaStream_t branch[kBranches] = {};
+    cudaEvent_t fork = nullptr, join[kBranches] = {};
     // camera leaf lists (one header per pixel of every view, one entry pool)
     DevBuf<uint4> cam_head, cam_pool;
     DevBuf<unsigned int> cam_used;
@@ -112,11 +131,72 @@ int build_graph(dr_batch *b) {
     B.n_views = (uint32_t)b->host_views.size();
     B.n_paths = b->n_paths;
     B.step = b->step.p;
+    // which views get a kernel of their own
+    uint64_t min_own = b->split;
+    if (min_own == DR_BATCH_SPLIT_AUTO) {
+        int sms = 0;
+        DR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ctx->device), "dr_batch: SM count");
+        const uint64_t bps = b->tuning.blocks_per_sm ? b->tuning.blocks_per_sm : 8u;
+        min_own = kSplitAutoPerLane * (uint64_t)sms * bps * 128u;
+    }
+    std::vector<uint32_t> own;
+    std::vector<BatchView> rest;
+    std::vector<uint64_t> rest_begins;
+    uint64_t rest_paths = 0;
+    for (uint32_t v = 0; v < (uint32_t)b->host_views.size(); ++v) {
+        const BatchView &V = b->host_views[v];
+        if (min_own && V.A.n_paths >= min_own) {
+            own.push_back(v);
+        } else {
+            rest.push_back(V);
+            rest.back().begin = rest_paths;
+            rest_begins.push_back(rest_paths);
+            rest_paths += V.A.n_paths;
+        }
+    }
+    BatchArgs R = B;  // the batched kernel's views
+    if (!own.empty()) {
+        if (!rest.empty()) {
+            DR_CUDA(cudaMemcpy(b->rest_views.p, rest.data(), sizeof(BatchView) * rest.size(), cudaMemcpyHostToDevice),
+                    "dr_batch: copy views");
+            DR_CUDA(cudaMemcpy(b->rest_begins.p, rest_begins.data(), sizeof(uint64_t) * rest.size(),
+                               cudaMemcpyHostToDevice),
+                    "dr_batch: copy views");
+        }
+        R.views = b->rest_views.p;
+        R.begins = b->rest_begins.p;
+        R.n_views = (uint32_t)rest.size();
+        R.n_paths = rest_paths;
+        for (uint32_t k = 0; k < kBranches && k < own.size(); ++k) {
+            if (!b->branch[k])
+                DR_CUDA(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking), "dr_batch: branch stream");
+            if (!b->join[k])
+                DR_CUDA(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming), "dr_batch: branch event");
+        }
+        if (!b->fork) DR_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "dr_batch: branch event");
+    }
+    const uint32_t nbr = (uint32_t)std::min<size_t>(kBranches, own.size());
     DR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "dr_batch: begin capture");
     cudaError_t e = cudaMemsetAsync(b->out.p, 0, sizeof(float4) * b->out_n, b->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->work.p, 0, sizeof(WorkQueue) * b->work.n, b->stream);
+    if (e == cudaSuccess) e = launch_batch_lists(B, bl, b->stream);
+    if (e == cudaSuccess && nbr) e = cudaEventRecord(b->fork, b->stream);
+    for (uint32_t k = 0; k < nbr && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(b->branch[k], b->fork, 0);
+    for (size_t k = 0; k < own.size() && e == cudaSuccess; ++k) {
+        const BatchView &V = b->host_views[own[k]];
+        e = launch_batch_view(b->host_scenes[V.scene], V.P, V.A, b->mie_pack.p, V.sun, V.sky, b->ctx->counters.p,
+                              b->work.p + 1 + own[k], b->step.p, b->tuning, b->ctx->device, b->branch[k % nbr]);
+    }
     if (e == cudaSuccess)
-        e = launch_render_batch(B, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->step.p, b->tuning, ext,
-                                b->stack_levels, b->ctx->device, b->stream, bl);
+        e = launch_batch_kernel(R, b->p0, b->mie_pack.p, b->ctx->counters.p, b->work.p, b->tuning, ext,
+                                b->stack_levels, b->ctx->device, b->stream);
+    // every branch joins the capture stream (also after an error, so that the capture can end)
+    for (uint32_t k = 0; k < nbr; ++k) {
+        const cudaError_t j = cudaEventRecord(b->join[k], b->branch[k]);
+        const cudaError_t w = j == cudaSuccess ? cudaStreamWaitEvent(b->stream, b->join[k], 0) : j;
+        if (e == cudaSuccess) e = w;
+    }
+    if (e == cudaSuccess) e = launch_batch_step(b->step.p, b->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) {
@@ -125,6 +205,7 @@ int build_graph(dr_batch *b) {
     }
     if (e2 != cudaSuccess) return cuda_fail(e2, "dr_batch: end capture");
     b->graph = g;
+    b->own_kernels = (uint32_t)own.size();
     DR_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "dr_batch: instantiate graph");
     return DR_OK;
 }
@@ -144,6 +225,16 @@ void release(dr_batch *b) {
     b->cam_pool.release();
     b->cam_used.release();
     b->pix_begins.release();
+    b->rest_views.release();
+    b->rest_begins.release();
+    for (uint32_t k = 0; k < kBranches; ++k) {
+        if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+        b->branch[k] = nullptr;
+        b->join[k] = nullptr;
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    b->fork = nullptr;
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
 }
@@ -264,12 +355,15 @@ int dr_batch_create(dr_ctx *c, const dr_scene_desc *scenes, uint32_t n_scenes, c
     BATCH_CUDA(b->mie_pack.reserve(pack0.size()), "dr_batch_create: alloc tables");
     BATCH_CUDA(cudaMemcpy(b->mie_pack.p, pack0.data(), pack0.size(), cudaMemcpyHostToDevice),
                "dr_batch_create: copy tables");
-    BATCH_CUDA(b->work.reserve(1), "dr_batch_create: alloc queue");
+    BATCH_CUDA(b->work.reserve(1 + (size_t)n_views), "dr_batch_create: alloc queue");
+    BATCH_CUDA(b->rest_views.reserve(n_views), "dr_batch_create: alloc views");
+    BATCH_CUDA(b->rest_begins.reserve(n_views), "dr_batch_create: alloc views");
     BATCH_CUDA(b->step.reserve(1), "dr_batch_create: alloc step");
     BATCH_CUDA(cudaMemset(b->step.p, 0, sizeof(unsigned long long)), "dr_batch_create: clear step");
 #undef BATCH_CUDA
     b->p0 = hv[0].P;
     b->host_views = std::move(hv);
+    b->host_scenes = ds;
     rc = build_graph(b.get());
     if (rc != DR_OK) return fail(rc);
     *out = b.release();
@@ -340,6 +434,21 @@ int dr_batch_read(dr_batch *b, uint32_t view, float *sun_out, float *sky_out) {
     DR_CUDA(cudaDeviceSynchronize(), "dr_batch_read: sync");
     DR_CUDA(cudaMemcpy(sun_out, V.sun, n * sizeof(float4), cudaMemcpyDeviceToHost), "dr_batch_read: copy");
     DR_CUDA(cudaMemcpy(sky_out, V.sky, n * sizeof(float4), cudaMemcpyDeviceToHost), "dr_batch_read: copy");
+    return DR_OK;
+}
+
+int dr_batch_set_split(dr_batch *b, uint64_t min_paths) {
+    if (!b) return need(false, DR_ERR_INVALID, "dr_batch_set_split: null batch");
+    DeviceGuard g(b->ctx->device);
+    DR_CUDA(cudaStreamSynchronize(b->stream), "dr_batch_set_split: sync");
+    b->split = min_paths;
+    return build_graph(b);
+}
+
+int dr_batch_get_split(dr_batch *b, uint64_t *min_paths, uint32_t *own_kernels) {
+    if (!b) return need(false, DR_ERR_INVALID, "dr_batch_get_split: null batch");
+    if (min_paths) *min_paths = b->split;
+    if (own_kernels) *own_kernels = b->own_kernels;
     return DR_OK;
 }
 

@@ -741,6 +741,9 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
         mb = mie_bytes(P);
         M = mie_view(P, smem);
         n_total = A.n_paths;
+        // a large view of a batch, as a kernel of its own in the batch's graph:
+        // launch k draws samples [k spp, (k+1) spp) like the batched kernel
+        if (B.step) shift = *B.step * A.spp;
     }
     const bool staged = stage_mie(mie_pack, mb, smem, &mbar);
     float *const shcol = reinterpret_cast<float *>(smem + ((mb + 15u) & ~15u)) + threadIdx.x;
@@ -781,7 +784,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
                         ok = start_path(L, p - V.begin, B.scenes[V.scene], V.P, V.A, shift * V.A.spp, cnt, paths,
                                         state, slow);
                     } else {
-                        ok = start_path(L, p, S, P, A, 0ull, cnt, paths, state, slow);
+                        ok = start_path(L, p, S, P, A, shift, cnt, paths, state, slow);
                     }
                     if (!ok) state = kFetch;
                 }
@@ -1742,37 +1745,72 @@ cudaError_t launch_render_persistent(const DevScene &S, const DevParams &P, cons
     return cudaGetLastError();
 }
 
-cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
-                                WorkQueue *Q, unsigned long long *step, const Tuning &tune_in, bool ext,
-                                uint32_t stack_levels, int device, cudaStream_t st, const BatchLists &lists) {
+cudaError_t launch_batch_lists(const BatchArgs &B, const BatchLists &lists, cudaStream_t st) {
+    if (!B.n_paths || !lists.lists.head || !lists.n_pix) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(lists.lists.used, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    batch_camera_list_kernel<<<(lists.n_pix + 127) / 128, 128, 0, st>>>(
+        B, lists.pix_begins, lists.n_pix, lists.lists.head, lists.lists.pool, lists.lists.cap, lists.lists.used);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_kernel(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
+                                WorkQueue *Q, const Tuning &tune_in, bool ext, uint32_t stack_levels, int device,
+                                cudaStream_t st) {
+    if (!B.n_paths) return cudaSuccess;
     size_t smem = mie_smem(P0);
     Tuning tune = tune_in;
     const uint32_t shlevels = shared_stack_plan(tune, ext ? kFeatAll : 0u, stack_levels, smem);
     if (!ext) smem = ((smem + 15) & ~(size_t)15) + (size_t)sky_queue_words<true>() * 4u * (kPersistentBlock / 32);
     PersistentFn fn;
     int blocks;
-    uint32_t batch;
-    cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatAll : 0u, fn, blocks, batch);
+    uint32_t knobs;
+    cudaError_t e = persistent_grid(tune, device, smem, true, ext ? kFeatAll : 0u, fn, blocks, knobs);
     if (e != cudaSuccess) return e;
-    batch |= shlevels << 24;
-    e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
+    knobs |= shlevels << 24;
+    fn<<<blocks, kPersistentBlock, smem, st>>>(DevScene{}, DevParams{}, TileArgs{}, mie_pack, nullptr, nullptr, C, Q,
+                                               knobs, B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_view(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                              float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
+                              const unsigned long long *step, const Tuning &tune_in, int device, cudaStream_t st) {
+    if (A.n_paths == 0) return cudaSuccess;
+    size_t smem = mie_smem(P);
+    const uint32_t feat = frame_features(S, P);
+    Tuning tune = tune_in;
+    const uint32_t shlevels = shared_stack_plan(tune, feat, S.stack_levels, smem);
+    TileArgs Ad = A;
+    Ad.defer_sky = (feat == 0 && !P.finite_paths) ? 1u : 0u;
+    if (Ad.defer_sky) smem = ((smem + 15) & ~(size_t)15) + (size_t)sky_queue_words<false>() * 4u * (kPersistentBlock / 32);
+    PersistentFn fn;
+    int blocks;
+    uint32_t knobs;
+    cudaError_t e = persistent_grid(tune, device, smem, false, feat, fn, blocks, knobs);
     if (e != cudaSuccess) return e;
-    if (B.n_paths && lists.lists.head && lists.n_pix) {  // the views' TileArgs point into these lists
-        e = cudaMemsetAsync(lists.lists.used, 0, sizeof(unsigned int), st);
-        if (e != cudaSuccess) return e;
-        batch_camera_list_kernel<<<(lists.n_pix + 127) / 128, 128, 0, st>>>(
-            B, lists.pix_begins, lists.n_pix, lists.lists.head, lists.lists.pool, lists.lists.cap, lists.lists.used);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    if (B.n_paths) {
-        fn<<<blocks, kPersistentBlock, smem, st>>>(DevScene{}, DevParams{}, TileArgs{}, mie_pack, nullptr, nullptr, C,
-                                                   Q, batch, B);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
+    knobs |= shlevels << 24;
+    BatchArgs B{};
+    B.step = step;
+    fn<<<blocks, kPersistentBlock, smem, st>>>(S, P, Ad, mie_pack, sun_out, sky_out, C, Q, knobs, B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_step(unsigned long long *step, cudaStream_t st) {
     batch_step_kernel<<<1, 1, 0, st>>>(step);
     return cudaGetLastError();
+}
+
+cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
+                                WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext,
+                                uint32_t stack_levels, int device, cudaStream_t st, const BatchLists &lists) {
+    cudaError_t e = cudaMemsetAsync(Q, 0, sizeof(WorkQueue), st);
+    if (e != cudaSuccess) return e;
+    e = launch_batch_lists(B, lists, st);  // the views' TileArgs point into these lists
+    if (e != cudaSuccess) return e;
+    e = launch_batch_kernel(B, P0, mie_pack, C, Q, tune, ext, stack_levels, device, st);
+    if (e != cudaSuccess) return e;
+    return launch_batch_step(step, st);
 }
 
 cudaError_t launch_add_counters(DevCounters *dst, const DevCounters *src, cudaStream_t st) {

@@ -40,6 +40,21 @@ struct BatchLists {
 cudaError_t launch_render_batch(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
                                 WorkQueue *Q, unsigned long long *step, const Tuning &tune, bool ext,
                                 uint32_t stack_levels, int device, cudaStream_t st, const BatchLists &lists = {});
+// The parts of launch_render_batch, for graphs that split a batch:
+// the camera leaf lists of every view of B (nothing when lists.head is null);
+cudaError_t launch_batch_lists(const BatchArgs &B, const BatchLists &lists, cudaStream_t st);
+// one batched persistent kernel over the views of B (Q->next must be 0);
+cudaError_t launch_batch_kernel(const BatchArgs &B, const DevParams &P0, const void *mie_pack, DevCounters *C,
+                                WorkQueue *Q, const Tuning &tune, bool ext, uint32_t stack_levels, int device,
+                                cudaStream_t st);
+// one view of a batch as a plain persistent kernel of its own: the view's
+// parameters and tile are kernel arguments (A.cam_head: its lists, already
+// built; A.sample_base + *step * spp is its first sample; Q->next must be 0);
+cudaError_t launch_batch_view(const DevScene &S, const DevParams &P, const TileArgs &A, const void *mie_pack,
+                              float4 *sun_out, float4 *sky_out, DevCounters *C, WorkQueue *Q,
+                              const unsigned long long *step, const Tuning &tune, int device, cudaStream_t st);
+// *step += 1 (the last node of a batch's graph).
+cudaError_t launch_batch_step(unsigned long long *step, cudaStream_t st);
 // Resident blocks per SM of the persistent kernel for the given dynamic shared memory.
 int persistent_max_blocks_per_sm(uint32_t variant, uint32_t traversal, size_t smem_bytes);
 cudaError_t launch_probe_leaf(const DevScene &S, const float *ro, const float *rd, uint32_t n, uint32_t maxn,

@@ -217,6 +217,8 @@ SIGNATURES = {
     "dr_batch_output": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "dr_batch_read": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "dr_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "dr_batch_set_split": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "dr_batch_get_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "dr_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
     "dr_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(DrTuning)]),
     "dr_get_counters": (C.c_int, [C.c_void_p, C.POINTER(DrCounters)]),

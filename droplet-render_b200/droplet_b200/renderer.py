@@ -382,9 +382,12 @@ class BatchView:
 
 
 class Batch:
-    """Many scenes and views rendered by one persistent launch replayed from a CUDA
-    graph (dr_batch_*).  Launch k renders samples [k spp, (k+1) spp) of each view,
-    the streams Renderer.render_tile draws with sample_base = k spp."""
+    """Many scenes and views rendered by one launch of a CUDA graph (dr_batch_*):
+    a persistent kernel over the views, large views optionally in kernels of
+    their own (set_split).  Launch k renders samples [k spp, (k+1) spp) of each
+    view, the streams Renderer.render_tile draws with sample_base = k spp."""
+
+    SPLIT_AUTO = (1 << 64) - 1  # DR_BATCH_SPLIT_AUTO
 
     def __init__(self, renderer: "Renderer", scenes: list, views: list):
         descs = (N.DrSceneDesc * len(scenes))()
@@ -455,3 +458,14 @@ class Batch:
         n, k = C.c_uint64(), C.c_uint64()
         N.check(N.lib().dr_batch_info(self._h, C.byref(n), C.byref(k)))
         return int(n.value), int(k.value)
+
+    def set_split(self, min_paths: int):
+        """Views of at least min_paths paths per launch get a kernel of their own
+        (0: one batched kernel for every view; SPLIT_AUTO: the library's rule)."""
+        N.check(N.lib().dr_batch_set_split(self._h, int(min_paths)))
+
+    def get_split(self):
+        """(min_paths setting, views with a kernel of their own in the graph)."""
+        m, k = C.c_uint64(), C.c_uint32()
+        N.check(N.lib().dr_batch_get_split(self._h, C.byref(m), C.byref(k)))
+        return int(m.value), int(k.value)

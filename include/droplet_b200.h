@@ -273,7 +273,8 @@ int dr_get_tuning(dr_ctx *ctx, dr_tuning *tuning);
 /* ---- batched rendering (no reference counterpart: the reference renders one
  * tile of one view per RenderKernel::Render call, src/kernel.cpp:536-567) ----
  * A batch holds several scenes and views and renders every view's spp new
- * samples in ONE persistent launch replayed from a CUDA graph.  Launch k of a
+ * samples in ONE launch of a CUDA graph: a persistent kernel over the views
+ * (large views may get kernels of their own, dr_batch_set_split).  Launch k of a
  * batch renders, for each view, the samples dr_render_tile would render with
  * sample_base = k * spp; outputs hold the sums of the last launch. */
 typedef struct dr_batch dr_batch;
@@ -301,6 +302,19 @@ int dr_batch_output(dr_batch *batch, uint32_t view, float **sun_dev, float **sky
 int dr_batch_read(dr_batch *batch, uint32_t view, float *sun_out, float *sky_out);
 /* Path indices per launch (tile padding included) and launches so far. */
 int dr_batch_info(dr_batch *batch, uint64_t *n_paths, uint64_t *launches);
+/* Views of at least min_paths path samples per launch (cols*rows*spp) get a
+ * persistent kernel of their own in the batch's graph, with their parameters
+ * as kernel arguments; those kernels and the one batched kernel over the other
+ * views are independent graph branches (up to 4 run side by side), so one
+ * kernel's tail overlaps the next one's start.  Results are unchanged (same
+ * paths and streams).  min_paths 0: every view in the one batched kernel;
+ * DR_BATCH_SPLIT_AUTO (the default): 8 paths per lane of a full grid
+ * (SMs x blocks per SM x 128).  Recaptures the graph. */
+#define DR_BATCH_SPLIT_AUTO UINT64_MAX
+int dr_batch_set_split(dr_batch *batch, uint64_t min_paths);
+/* The split setting and how many views have a kernel of their own in the
+ * current graph (either pointer may be NULL). */
+int dr_batch_get_split(dr_batch *batch, uint64_t *min_paths, uint32_t *own_kernels);
 
 /* ---- differentiable rendering (path-replay adjoint) -------------------------
  * No reference counterpart: the reference renders only (src/kernel.cpp).

@@ -65,12 +65,9 @@ def batch_setup():
     r.close()
 
 
-@pytest.mark.parametrize("tuning", [(0, 5, 24, 0, 0), (0, 8, 16, 1, 8), (0, 4, 8, 0, 16), (0, 8, 24, 2, 0),
-                                    (0, 6, 16, 2, 8)])
-def test_batch_views_equal_restatement(batch_setup, port, tuning):
-    r, b, specs, scenes = batch_setup
-    b.set_tuning(*tuning)
-    assert b.get_tuning()[1:5] == tuning[1:5]
+def check_launches(r, b, specs, scenes, port, tag):
+    """Two launches of b: every view equals the restatement's tile for
+    sample_base = k spp, the counters equal the sum over views."""
     S = [port.scene(oc.nodes, oc.bricks) for oc in scenes]
     for _ in range(2):
         _, k = b.info()
@@ -86,13 +83,42 @@ def test_batch_views_equal_restatement(batch_setup, port, tuning):
             psun, psky, pcnt = port.render_tile(S[s], P, x0, y0, tw, th, spp, seed=seed, sample_base=k * spp)
             for g, p in zip(got[v], (psun, psky)):
                 assert g.shape == p.shape
-                assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), (v, tuning)
+                assert np.allclose(g, p, rtol=2e-5, atol=1e-6 * np.abs(p).max() + 1e-30), (v, tag)
             for key in total:
                 total[key] += pcnt[key]
         for key, val in total.items():
-            assert cnt[key] == val, (key, cnt[key], val)
+            assert cnt[key] == val, (key, cnt[key], val, tag)
     n, launches = b.info()
     assert n > 0 and launches >= 2
+
+
+@pytest.mark.parametrize("tuning", [(0, 5, 24, 0, 0), (0, 8, 16, 1, 8), (0, 4, 8, 0, 16), (0, 8, 24, 2, 0),
+                                    (0, 6, 16, 2, 8)])
+def test_batch_views_equal_restatement(batch_setup, port, tuning):
+    r, b, specs, scenes = batch_setup
+    b.set_tuning(*tuning)
+    assert b.get_tuning()[1:5] == tuning[1:5]
+    assert b.get_split()[1] == 0  # these views are far below the automatic split size
+    check_launches(r, b, specs, scenes, port, tuning)
+
+
+# split graphs: views of at least `split` paths run in plain persistent kernels
+# of their own (independent graph branches, the launch counter read on the
+# device), the rest in the batched kernel; 60,000 paths leaves the last view
+# (60 x 58 pixels x 8 spp) to the batched kernel in both pixel orders
+@pytest.mark.parametrize("split,own", [(1, 4), (60_000, 3), (0, 0)])
+@pytest.mark.parametrize("tuning", [(0, 8, 24, 2, 0), (0, 5, 16, 1, 8), (0, 6, 8, 0, 16)])
+def test_batch_split_views_equal_restatement(batch_setup, port, tuning, split, own):
+    from droplet_b200.renderer import Batch
+
+    r, b, specs, scenes = batch_setup
+    b.set_tuning(*tuning)
+    b.set_split(split)
+    try:
+        assert b.get_split() == (split, own)
+        check_launches(r, b, specs, scenes, port, (tuning, split))
+    finally:
+        b.set_split(Batch.SPLIT_AUTO)
 
 
 def test_batch_rejects_mixed_phase_tables(batch_setup):
