@@ -123,6 +123,9 @@ def batched_workload(pdf, cdf):
     return fields, views, scenes, settings
 
 
+PROBE_SIDE, PROBE_SPP = 256, 8  # batch autotuner's probe: centre crops of every view
+
+
 def measure_batched(r, pdf, cdf, steps: int, warmup: int):
     """The batched workload (8 fields x 64 views, one persistent launch per step
     replayed from a CUDA graph) against the plain single-frame path on the same
@@ -139,13 +142,17 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
     saved = r.get_tuning()
     bviews = [BatchView(v["field"], settings[i], v["spp"], 100 + i) for i, v in enumerate(views)]
     b = Batch(r, scenes, bviews)
-    # the autotuner times a probe batch: every view, centre crop of at most 128^2, 4 spp
+    # the autotuner times a probe batch: every view, centre crop of at most
+    # 256^2, 8 spp (a probe of 128^2 crops at 4 spp launched so little work that
+    # its tails favoured an event batch 5% slower on the full batch)
     probe = []
     for i, v in enumerate(views):
-        c = min(v["side"], 128)
+        c = min(v["side"], PROBE_SIDE)
         o = (v["side"] - c) // 2
-        probe.append(BatchView(v["field"], settings[i], 4, 100 + i, (o, o, c, c)))
+        probe.append(BatchView(v["field"], settings[i], PROBE_SPP, 100 + i, (o, o, c, c)))
     pb = Batch(r, scenes, probe)
+    # the full batch runs most views in kernels of their own: so does the probe
+    pb.set_split(1)
     t = time.time()
     best, table = autotune.tune_batch(pb, "c2-probe", use_cache=False)
     t_tune = time.time() - t
@@ -241,7 +248,8 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
         "speedup_vs_plain_per_view": batched / plain, "speedup_vs_addon_tiles": batched / tiles,
         "single_kernel_speedup_vs_plain_per_view": single / plain,
         "small_views": small,
-        "tuning": {"choice": list(best), "seconds": round(t_tune, 2), "probe": "centre <=128^2 crops, 4 spp",
+        "tuning": {"choice": list(best), "seconds": round(t_tune, 2),
+                   "probe": f"centre <={PROBE_SIDE}^2 crops, {PROBE_SPP} spp",
                    "top": [[c, round(m, 3)] for c, m in table[:6]]},
         "graph": "memset outputs and queues -> camera leaf lists of every view -> {a plain persistent kernel per "
                  "large view, one batched persistent kernel over the rest} as independent branches -> step counter",
