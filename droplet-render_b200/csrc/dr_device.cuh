@@ -276,30 +276,52 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
 // the 3-bit child slots (the same floats).
 enum : uint32_t { kTravMore = 0, kTravLeaf = 1, kTravDone = 2 };
 
-// Where the traversal keeps its ancestors.  LocalStack: node ids and intervals
-// in the lane's own arrays (local memory), the next child to examine at each
-// level in 4-bit fields of T.tns; without `iv` a pop replays the interval from
-// the root.  SharedStack: level l of this lane at col[(7l + k) * STRIDE] (k =
-// 0..5 the interval t0.xyz, t1.xyz, k = 6 the node id with the next child in
-// bits 28-31, so node ids must stay below 2^28), one column per lane of the
-// block, so the lanes of a warp touch 32 consecutive words whatever their
-// levels (no bank conflicts); `levels` entries fit, and a descent that would
-// need more gives up like the reference's depth limit (the host sizes the
-// stack from the octree's depth, so that never happens).
+// Where the traversal keeps its ancestors.  push(T, l, cb) saves level l at a
+// descent into the child with slot bits cb (T still holds the parent: its node,
+// next child T.tn and interval); pop(T, l) restores level l's node and next
+// child and, when the stack keeps intervals, its interval (returns true).
+// LocalStack: node ids and intervals in the lane's own arrays (local memory),
+// the next child at each level in 4-bit fields of T.tns; without `iv` a pop
+// replays the interval from the root (returns false).
+// SharedStack: level l of this lane at col[(kShWords l + k) * STRIDE], one
+// column per lane of the block, so the lanes of a warp touch 32 consecutive
+// words whatever their levels (no bank conflicts).  k = 0..2: per axis, the
+// parent's bound the child does not share (t0 where the child lies in the upper
+// half, else t1); k = 3: the node id (below 2^25), the child's slot bits at 25-27
+// and the next child at 28-31.  A pop happens when the child's subtree is done,
+// with the child's interval still in T: the child shares the parent's t1 on
+// the axes where its bit is set and the parent's t0 elsewhere, so the saved
+// bound completes the parent's interval with the same floats.  `levels` entries
+// fit, and a descent that would need more gives up like the reference's depth
+// limit (the host sizes the stack from the octree's depth, so that never happens).
+constexpr int kShWords = 4;
+
 struct LocalStack {
     uint32_t *nodes;
     float (*iv)[6];
-    __device__ __forceinline__ void push_entry(Trav &T, int l) const {
+    __device__ __forceinline__ void push(Trav &T, int l, uint32_t) const {
         nodes[l] = T.node;
         T.tns = (T.tns & ~(15ull << (4 * l))) | ((uint64_t)T.tn << (4 * l));
+        if (iv) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                iv[l][k] = T.t0[k];
+                iv[l][3 + k] = T.t1[k];
+            }
+        }
     }
-    __device__ __forceinline__ void pop_entry(Trav &T, int l) const {
+    __device__ __forceinline__ bool pop(Trav &T, int l) const {
         T.node = nodes[l];
         T.tn = (uint32_t)(T.tns >> (4 * l)) & 15u;
+        if (!iv) return false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T.t0[k] = iv[l][k];
+            T.t1[k] = iv[l][3 + k];
+        }
+        return true;
     }
     __device__ __forceinline__ bool has_iv() const { return iv != nullptr; }
-    __device__ __forceinline__ float get(int l, int k) const { return iv[l][k]; }
-    __device__ __forceinline__ void put(int l, int k, float v) const { iv[l][k] = v; }
     __device__ __forceinline__ bool full(int l) const { return l + 1 >= kMaxDepth - 1; }
 };
 
@@ -307,17 +329,25 @@ template <int STRIDE>
 struct SharedStack {
     float *col;
     int levels;
-    __device__ __forceinline__ void push_entry(Trav &T, int l) const {
-        col[(7 * l + 6) * STRIDE] = __uint_as_float(T.node | (T.tn << 28));
+    __device__ __forceinline__ void push(Trav &T, int l, uint32_t cb) const {
+        col[(kShWords * l + 0) * STRIDE] = (cb & 1u) ? T.t0[0] : T.t1[0];
+        col[(kShWords * l + 1) * STRIDE] = (cb & 2u) ? T.t0[1] : T.t1[1];
+        col[(kShWords * l + 2) * STRIDE] = (cb & 4u) ? T.t0[2] : T.t1[2];
+        col[(kShWords * l + 3) * STRIDE] = __uint_as_float(T.node | (cb << 25) | (T.tn << 28));
     }
-    __device__ __forceinline__ void pop_entry(Trav &T, int l) const {
-        const uint32_t w = __float_as_uint(col[(7 * l + 6) * STRIDE]);
-        T.node = w & 0x0fffffffu;
+    __device__ __forceinline__ bool pop(Trav &T, int l) const {
+        const uint32_t w = __float_as_uint(col[(kShWords * l + 3) * STRIDE]);
+        T.node = w & 0x01ffffffu;
         T.tn = w >> 28;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float o = col[(kShWords * l + k) * STRIDE];
+            if ((w >> (25 + k)) & 1u) T.t0[k] = o;
+            else T.t1[k] = o;
+        }
+        return true;
     }
     __device__ __forceinline__ bool has_iv() const { return true; }
-    __device__ __forceinline__ float get(int l, int k) const { return col[(7 * l + k) * STRIDE]; }
-    __device__ __forceinline__ void put(int l, int k, float v) const { col[(7 * l + k) * STRIDE] = v; }
     // levels <= 13 (the host allows at most 7), so the reference's depth limit is implied
     __device__ __forceinline__ bool full(int l) const { return l >= levels; }
 };
@@ -335,15 +365,7 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             }
             const int l = T.l - 1;
             T.l = l;
-            stk.pop_entry(T, l);
-            if (stk.has_iv()) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    T.t0[k] = stk.get(l, k);
-                    T.t1[k] = stk.get(l, 3 + k);
-                }
-                continue;
-            }
+            if (stk.pop(T, l)) continue;
             float t0[3] = {T.t0r[0], T.t0r[1], T.t0r[2]}, t1[3] = {T.t1r[0], T.t1r[1], T.t1r[2]};
             for (int k = 0; k < l; ++k) {
                 const uint32_t s = (uint32_t)(T.slots >> (3 * k)) & 7u;
@@ -386,14 +408,7 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             ++cnt.gave_up;
             return kTravDone;
         }
-        stk.push_entry(T, l);
-        if (stk.has_iv()) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                stk.put(l, k, T.t0[k]);
-                stk.put(l, 3 + k, T.t1[k]);
-            }
-        }
+        stk.push(T, l, tn);
         if (!stk.has_iv()) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));  // replay path only
         T.l = l + 1;
         T.node = child;

@@ -163,8 +163,8 @@ int prepare_scene(const dr_scene_desc *s, HostScene &out) {
     }
     out.levels = levels;
     // a tree with every leaf at depth d pushes at most d - 1 ancestors; the
-    // shared-memory stack packs node ids into 28 bits
-    out.stack_levels = (levels >= 2 && s->n_nodes < (1u << 28)) ? levels - 1 : 0u;
+    // shared-memory stack packs node ids into 25 bits
+    out.stack_levels = (levels >= 2 && s->n_nodes < (1u << 25)) ? levels - 1 : 0u;
     out.n = n;
     out.mdim = mdim;
     out.n_nodes = s->n_nodes;

@@ -45,7 +45,7 @@ struct DevScene {
     uint32_t mdim;       // macro cells per axis
     // Entries the stack traversal can push on any ray: internal nodes below the
     // root on the deepest root-to-leaf path (0: unknown, e.g. leaves at mixed
-    // depths or a DAG, or 2^28 nodes or more; then only the local-memory stack
+    // depths or a DAG, or 2^25 nodes or more; then only the local-memory stack
     // is used).
     uint32_t stack_levels;
     // Occluder BVH (null: no occluders).  Node i = occ_nodes[4i .. 4i+3]: left

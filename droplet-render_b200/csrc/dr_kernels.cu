@@ -713,7 +713,7 @@ __device__ __forceinline__ uint32_t find_view(const BatchArgs &B, uint64_t p) {
 // a path and reads that view's records from global memory (L1-resident).
 // SHS (stack traversal only): the traversal stack of each lane lives in
 // dynamic shared memory after the phase tables, `knobs` bits 24-31 entries
-// deep (7 words per entry and lane), instead of local memory.
+// deep (kShWords words per entry and lane), instead of local memory.
 template <int MINB, bool WALK, bool BATCH, uint32_t FEAT, bool SHS = false>
 __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kernel(DevScene S, DevParams P, TileArgs A,
                                                                             const void *mie_pack, float4 *sun_out,
@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(kPersistentBlock, MINB) render_persistent_kern
     const unsigned FULL = 0xffffffffu;
     // this warp's sky queue, after the phase tables and the shared traversal stack
     float *const skyq = reinterpret_cast<float *>(smem + ((mb + 15u) & ~15u) +
-                                                  (size_t)shlevels * 7u * 4u * kPersistentBlock) +
+                                                  (size_t)shlevels * kShWords * 4u * kPersistentBlock) +
                         (threadIdx.x >> 5) * sky_queue_words<BATCH>();
     uint32_t nsky = 0;
     for (;;) {
@@ -1692,7 +1692,7 @@ static cudaError_t persistent_grid(const Tuning &tune, int device, size_t smem, 
 }
 
 // Largest octree depth whose traversal stack goes to shared memory: 7 entries
-// x 28 B x 128 lanes = 25 KB per block besides the phase tables.
+// x 16 B x 128 lanes = 14 KB per block besides the phase tables.
 constexpr uint32_t kShStackMax = 7;
 
 // DR_TRAVERSAL_STACK_SHARED: only for the plain instantiation and octrees of
@@ -1700,7 +1700,7 @@ constexpr uint32_t kShStackMax = 7;
 // otherwise the local-memory stack.  Returns the stack entries (0: local).
 static uint32_t shared_stack_plan(Tuning &tune, uint32_t feat, uint32_t stack_levels, size_t &smem) {
     if (tune.traversal != 2u) return 0;
-    const size_t with = ((smem + 15) & ~(size_t)15) + (size_t)stack_levels * 7 * 4 * kPersistentBlock;
+    const size_t with = ((smem + 15) & ~(size_t)15) + (size_t)stack_levels * kShWords * 4 * kPersistentBlock;
     if (feat == 0 && stack_levels >= 1 && stack_levels <= kShStackMax && with <= 48 * 1024) {
         smem = with;
         return stack_levels;

@@ -266,7 +266,7 @@ typedef struct {
 #define DR_TRAVERSAL_WALK 1u   /* cell walk over the leaf grid, same leaf order and intervals */
 #define DR_TRAVERSAL_STACK_SHARED 2u  /* the octree descent with its stack in shared memory (frames and batches
                                          without optional features whose octrees keep every leaf at one depth
-                                         <= 8 and have fewer than 2^28 nodes; otherwise DR_TRAVERSAL_STACK) */
+                                         <= 8 and have fewer than 2^25 nodes; otherwise DR_TRAVERSAL_STACK) */
 int dr_set_tuning(dr_ctx *ctx, const dr_tuning *tuning);
 int dr_get_tuning(dr_ctx *ctx, dr_tuning *tuning);
 
