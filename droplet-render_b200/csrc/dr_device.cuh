@@ -195,23 +195,18 @@ struct Count {
 // The decisions are the same; in slot order the remap is one XOR with the
 // mirror mask.
 __device__ __forceinline__ uint32_t first_node(const float t0[3], const float tm[3]) {
-    uint32_t a = 0;
-    if (t0[0] > t0[1]) {
-        if (t0[0] > t0[2]) {
-            if (tm[1] < t0[0]) a |= 2;
-            if (tm[2] < t0[0]) a |= 4;
-            return a;
-        }
-    } else {
-        if (t0[1] > t0[2]) {
-            if (tm[0] < t0[1]) a |= 1;
-            if (tm[2] < t0[1]) a |= 4;
-            return a;
-        }
-    }
-    if (tm[0] < t0[2]) a |= 1;
-    if (tm[1] < t0[2]) a |= 2;
-    return a;
+    // the entry axis: x when t0.x exceeds both others, y when t0.x <= t0.y and
+    // t0.y > t0.z, else z (the reference's branches, NaN compares false); the
+    // first child has the bit of every other axis whose midplane lies before
+    // the entry.  Written with selects: the entry axis's own bit is never set
+    // (tm >= t0 on that axis, or NaN), and it is cleared all the same.
+    const bool xy = t0[0] > t0[1];
+    const bool ax = xy && (t0[0] > t0[2]);
+    const bool ay = !xy && (t0[1] > t0[2]);
+    const float te = ax ? t0[0] : (ay ? t0[1] : t0[2]);
+    const uint32_t own = ax ? 1u : (ay ? 2u : 4u);
+    const uint32_t a = (tm[0] < te ? 1u : 0u) | (tm[1] < te ? 2u : 0u) | (tm[2] < te ? 4u : 0u);
+    return a & ~own;
 }
 
 __device__ __forceinline__ uint32_t child_entry(const DevScene &S, uint32_t node, uint32_t slot) {
