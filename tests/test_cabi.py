@@ -40,6 +40,10 @@ def test_version_and_errors():
     assert rc == N.DR_ERR_INVALID
     assert b"null" in L.dr_last_error()
     assert L.dr_destroy(None) == N.DR_OK
+    # batch calls refuse a null batch before touching the device
+    assert L.dr_batch_set_split(None, 0) == N.DR_ERR_INVALID
+    assert L.dr_batch_get_split(None, None, None) == N.DR_ERR_INVALID
+    assert b"null batch" in L.dr_last_error()
 
 
 def test_no_device_is_an_error_not_a_fallback():
