@@ -954,7 +954,7 @@ def measure_large(r, pdf, cdf, cfgs, rads, steps: int = 2, warmup: int = 1, spp:
     r.upload(oc)
     big = settings(3840, 2160)
     r.set_params(big)
-    best, _ = autotune.tune(r, (960, 540, 1920, 1080), 4, key="c4", use_cache=False)
+    best, _ = autotune.tune(r, (960, 540, 1920, 1080), 16, key="c4", use_cache=False)
     stream = torch.cuda.Stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     sun = torch.empty((1080, 1920, 4), device="cuda")

@@ -482,9 +482,11 @@ int dr_render_tile(dr_ctx *c, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th
         const cudaError_t e = cudaEventSynchronize(c->copy_done[k]);
         if (e != cudaSuccess && err == cudaSuccess) err = e;
         if (err != cudaSuccess) break;
-        std::memcpy(sun_out + 4 * spans[k].first, c->pinned + 4 * spans[k].first, spans[k].second * sizeof(float4));
-        std::memcpy(sky_out + 4 * spans[k].first, c->pinned + 4 * (c->pinned_n + spans[k].first),
-                    spans[k].second * sizeof(float4));
+        const CopyPool::Range r[2] = {
+            {sun_out + 4 * spans[k].first, c->pinned + 4 * spans[k].first, spans[k].second * sizeof(float4)},
+            {sky_out + 4 * spans[k].first, c->pinned + 4 * (c->pinned_n + spans[k].first),
+             spans[k].second * sizeof(float4)}};
+        c->copies.copy(r, 2);
     }
     // keep the context stream ordered after the bands and the copies
     if (err == cudaSuccess) err = cudaStreamSynchronize(c->copy_stream);

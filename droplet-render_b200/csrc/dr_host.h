@@ -2,9 +2,12 @@
 // error reporting, device buffers, and the validation + conversion of scenes
 // and render settings into their device layouts.
 #pragma once
+#include <condition_variable>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 #include <cuda_runtime.h>
 #include "../../include/droplet_b200.h"
@@ -115,6 +118,110 @@ int build_occluder_bvh(const dr_surface *s, uint32_t n, uint32_t mode, OccBvh &o
 }  // namespace dr
 
 // The context behind the C ABI's opaque dr_ctx handle.
+namespace dr {
+// Host threads that share the copies from pinned staging into the caller's
+// buffers (dr_render_tile).  The costly bands of a frame (the cloud's rows)
+// tend to finish last and close together, so one thread copying each 8 MB band
+// after it lands (about 1 ms each) put several milliseconds after the last
+// kernel; split over the pool's threads and the calling thread, each copy
+// takes a fraction of that.  Threads start on the first large copy and stop
+// when the pool is destroyed.
+class CopyPool {
+  public:
+    struct Range {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    CopyPool() = default;
+    CopyPool(const CopyPool &) = delete;
+    CopyPool &operator=(const CopyPool &) = delete;
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            quit_ = true;
+        }
+        work_.notify_all();
+        for (std::thread &t : threads_) t.join();
+    }
+    // Copies every range; returns when all bytes are in place.
+    void copy(const Range *r, size_t n) {
+        size_t total = 0;
+        for (size_t i = 0; i < n; ++i) total += r[i].bytes;
+        start();
+        if (threads_.empty() || total < kMinSplit) {
+            for (size_t i = 0; i < n; ++i) std::memcpy(r[i].dst, r[i].src, r[i].bytes);
+            return;
+        }
+        const size_t parts = threads_.size() + 1;
+        const size_t chunk = ((total / parts) + 4095) & ~(size_t)4095;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            jobs_.clear();
+            next_ = 0;
+            for (size_t i = 0; i < n; ++i)
+                for (size_t o = 0; o < r[i].bytes; o += chunk)
+                    jobs_.push_back({static_cast<char *>(r[i].dst) + o, static_cast<const char *>(r[i].src) + o,
+                                     r[i].bytes - o < chunk ? r[i].bytes - o : chunk});
+            pending_ = jobs_.size();
+        }
+        work_.notify_all();
+        for (;;) {  // the calling thread copies too
+            Job j;
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                if (next_ >= jobs_.size()) break;
+                j = jobs_[next_++];
+            }
+            run(j);
+        }
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+  private:
+    static constexpr size_t kMinSplit = 1u << 20;
+    struct Job {
+        char *dst;
+        const char *src;
+        size_t n;
+    };
+    void run(const Job &j) {
+        std::memcpy(j.dst, j.src, j.n);
+        std::lock_guard<std::mutex> lk(m_);
+        if (--pending_ == 0) done_.notify_all();
+    }
+    void start() {
+        if (started_) return;
+        started_ = true;
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = hw > 1 ? (hw < 8 ? hw : 8) - 1 : 0;
+        try {
+            for (unsigned i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
+        } catch (...) {  // fewer threads (or none): the calling thread copies the rest
+        }
+    }
+    void loop() {
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                work_.wait(lk, [&] { return quit_ || next_ < jobs_.size(); });
+                if (quit_) return;
+                j = jobs_[next_++];
+            }
+            run(j);
+        }
+    }
+    std::mutex m_;
+    std::condition_variable work_, done_;
+    std::vector<std::thread> threads_;
+    std::vector<Job> jobs_;
+    size_t next_ = 0, pending_ = 0;
+    bool quit_ = false, started_ = false;
+};
+}  // namespace dr
+
 struct dr_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -162,4 +269,5 @@ struct dr_ctx {
     dr::DevBuf<unsigned int> cam_used;
     float *pinned = nullptr;  // 2 * pinned_n float4: sun then sky
     size_t pinned_n = 0;
+    dr::CopyPool copies;      // host threads for the staging -> caller copies
 };
