@@ -180,7 +180,7 @@ class CopyPool {
     }
 
   private:
-    static constexpr size_t kMinSplit = 1u << 20;
+    static constexpr size_t kMinSplit = 4u << 20;
     struct Job {
         char *dst;
         const char *src;
