@@ -449,7 +449,8 @@ def profiled_l2():
     try:
         with open(p) as f:
             for line in f:
-                for key in ("l2_throughput_pct", "lts_hit_rate"):
+                for key in ("l2_throughput_pct", "lts_hit_rate", "alu_pipe_pct", "issue_active_pct",
+                            "lanes_per_instruction"):
                     if line.startswith(key + ":"):
                         out[key] = float(line.split(":")[1])
     except Exception:
@@ -1272,6 +1273,15 @@ def run_b200(args):
                           "lts_hit_rate": l2.get("lts_hit_rate"),
                           "source": "ncu L2 throughput (% of peak) and lts__t_sector_hit_rate.pct on a 512^2 crop "
                                     "launch (profiles/render_persistent_kernel_c1.md)"}
+        # the roof that binds: instruction issue on the ALU pipe (compares,
+        # selects and integer work of the octree traversal), same capture
+        if "alu_pipe_pct" in l2:
+            roofline["issue"] = {"alu_pipe_frac": l2["alu_pipe_pct"] / 100.0,
+                                 "issue_active_frac": l2.get("issue_active_pct", float("nan")) / 100.0,
+                                 "lanes_per_instruction": l2.get("lanes_per_instruction"),
+                                 "source": "ncu sm__inst_executed_pipe_alu, smsp__issue_active and "
+                                           "smsp__thread_inst_executed_per_inst_executed on the same 512^2 crop "
+                                           "launch (profiles/render_persistent_kernel_c1.md)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
