@@ -363,6 +363,34 @@ def test_banded_host_render_equals_restatement(port):
                 assert cnt[k] == pcnt[k], (tuning, k)
 
 
+def test_blocking_render_with_copy_threads_equals_device_render():
+    """A tile whose row bands pass the 4 MB floor of the host copy threads
+    (2048 x 512 pixels: 8 bands of 4.2 MB) comes back through the threaded
+    copies equal to the same render into device buffers (the same paths; the
+    per-pixel sums may differ in the order of their float additions)."""
+    import torch
+
+    from droplet_b200.renderer import Renderer
+    from droplet_b200.scene import Octree
+
+    nodes, bricks, mlevel = golden_octree()
+    cfg = c0_cfg(2048, 512)
+    with Renderer(0) as r:
+        r.upload(Octree(nodes, bricks, mlevel))
+        r.set_params(settings_from_cfg(cfg))
+        r.set_tuning(0, 8, 24, 2, 0, 3, 1)
+        for k in range(2):  # the second call reuses the started threads
+            sun, sky = r.render_tile(0, 0, 2048, 512, 2, seed=5, sample_base=2 * k)
+            dsun = torch.full((512, 2048, 4), -1.0, device="cuda")
+            dsky = torch.full_like(dsun, -1.0)
+            torch.cuda.synchronize()
+            r.render_tile_async(0, 0, 2048, 512, 2, 5, 2 * k, dsun.data_ptr(), dsky.data_ptr())
+            r.synchronize()
+            for g, d in ((sun, dsun.cpu().numpy()), (sky, dsky.cpu().numpy())):
+                assert np.isfinite(g).all() and g[..., 3].sum() > 0
+                assert np.allclose(g, d, rtol=2e-5, atol=1e-6 * np.abs(d).max() + 1e-30), k
+
+
 def test_large_sparse_scene_recipe_paths_equal_restatement(port):
     """The large sparse scene's recipe (24 puffs in a slab, sigma_t 100, 128
     events) at 256^3: GPU paths equal the restatement's."""
