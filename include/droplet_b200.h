@@ -198,7 +198,9 @@ int dr_sky_cook(const double *const dataset_rgb[3], const double *const dataset_
  * Path (pixel p = py*w + px, sample s) draws from stream (seed, p, sample_base + s).
  * Blocking; host buffers.  Returns DR_ERR_GAVE_UP, with the tiles written,
  * when some of the call's paths were cut short by an iteration budget (the
- * reference has no budget: it renders every path to its end). */
+ * reference has no budget: it renders every path to its end).  Large tiles
+ * are copied into the caller's buffers by up to 7 host threads of the context,
+ * started on the first such copy and joined by dr_destroy. */
 int dr_render_tile(dr_ctx *ctx, uint32_t x0, uint32_t y0, uint32_t tw, uint32_t th, uint32_t spp, uint64_t seed,
                    uint64_t sample_base, float *sun_out, float *sky_out);
 /* Same on device buffers, enqueued on stream (NULL = context stream); returns
