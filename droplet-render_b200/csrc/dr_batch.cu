@@ -374,7 +374,9 @@ int dr_batch_destroy(dr_batch *b) {
     if (!b) return DR_OK;
     {
         DeviceGuard g(b->ctx->device);
-        if (b->stream) cudaStreamSynchronize(b->stream);
+        // launches may run on any caller stream: wait for the device before
+        // the graph and its buffers go
+        cudaDeviceSynchronize();
         release(b);
     }
     delete b;
@@ -386,7 +388,8 @@ int dr_batch_set_tuning(dr_batch *b, const dr_tuning *t) {
     if (t->kernel != DR_KERNEL_PERSISTENT)
         return need(false, DR_ERR_INVALID, "dr_batch_set_tuning: a batch runs the persistent kernel");
     DeviceGuard g(b->ctx->device);
-    DR_CUDA(cudaStreamSynchronize(b->stream), "dr_batch_set_tuning: sync");
+    // a launch on any caller stream may still read the views: wait for the device
+    DR_CUDA(cudaDeviceSynchronize(), "dr_batch_set_tuning: sync");
     b->tuning.kernel = DR_KERNEL_PERSISTENT;
     b->tuning.blocks_per_sm = t->blocks_per_sm;
     b->tuning.event_batch = t->event_batch;
@@ -440,7 +443,7 @@ int dr_batch_read(dr_batch *b, uint32_t view, float *sun_out, float *sky_out) {
 int dr_batch_set_split(dr_batch *b, uint64_t min_paths) {
     if (!b) return need(false, DR_ERR_INVALID, "dr_batch_set_split: null batch");
     DeviceGuard g(b->ctx->device);
-    DR_CUDA(cudaStreamSynchronize(b->stream), "dr_batch_set_split: sync");
+    DR_CUDA(cudaDeviceSynchronize(), "dr_batch_set_split: sync");
     b->split = min_paths;
     return build_graph(b);
 }

@@ -293,7 +293,8 @@ typedef struct {
 int dr_batch_create(dr_ctx *ctx, const dr_scene_desc *scenes, uint32_t n_scenes, const dr_batch_view *views,
                     uint32_t n_views, dr_batch **out);
 int dr_batch_destroy(dr_batch *batch);
-/* Re-lays the views out and recaptures the graph for another launch shape. */
+/* Re-lays the views out and recaptures the graph for another launch shape
+ * (waits for the device first: launches may run on any stream). */
 int dr_batch_set_tuning(dr_batch *batch, const dr_tuning *tuning);
 int dr_batch_get_tuning(dr_batch *batch, dr_tuning *tuning);
 /* Enqueues one graph launch on stream (NULL = the context stream). */
@@ -311,7 +312,7 @@ int dr_batch_info(dr_batch *batch, uint64_t *n_paths, uint64_t *launches);
  * kernel's tail overlaps the next one's start.  Results are unchanged (same
  * paths and streams).  min_paths 0: every view in the one batched kernel;
  * DR_BATCH_SPLIT_AUTO (the default): 8 paths per lane of a full grid
- * (SMs x blocks per SM x 128).  Recaptures the graph. */
+ * (SMs x blocks per SM x 128).  Waits for the device, then recaptures the graph. */
 #define DR_BATCH_SPLIT_AUTO UINT64_MAX
 int dr_batch_set_split(dr_batch *batch, uint64_t min_paths);
 /* The split setting and how many views have a kernel of their own in the
