@@ -221,6 +221,7 @@ struct Trav {
     uint32_t a, node, tn;
     int l;
     bool active;
+    bool fresh;  // the origin lies in the root box: the first call descends straight to it
 };
 
 __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const float ro[3], const float rd[3],
@@ -257,6 +258,12 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, const floa
         }
         T.tn = first_node(T.t0, tm);
     }
+    // A segment that starts inside the root box (max t0 <= 0; finite planes,
+    // i.e. no zero direction component) can start its traversal at the node
+    // holding its origin: see trav_next_s.
+    T.fresh = T.active && std_max(std_max(T.t0r[0], T.t0r[1]), T.t0r[2]) <= 0.0f && isfinite(T.t0r[0]) &&
+              isfinite(T.t0r[1]) && isfinite(T.t0r[2]) && isfinite(T.t1r[0]) && isfinite(T.t1r[1]) &&
+              isfinite(T.t1r[2]);
 }
 
 // Up to `budget` loop iterations towards the next leaf, each one child
@@ -351,6 +358,43 @@ template <class ST>
 __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, const ST &stk, uint32_t &leaf,
                                                 float &tra, float &trb, Count &cnt, uint32_t budget) {
     if (!T.active) return kTravDone;
+    if (T.fresh) {
+        // Straight descent to the child holding t = 0 at each level.  In the
+        // examination order below (children in ray order from first_node),
+        // every child before that one exits behind the origin (some c1 < 0)
+        // and is skipped uncounted, so the state reached here -- stack
+        // entries, next children, intervals, node visits -- is the state the
+        // loop reaches when it arrives at that child.  The descent stops at a
+        // leaf, an empty child or a full stack and leaves that child for the
+        // loop to examine.
+        T.fresh = false;
+        for (;;) {
+            float tm[3], c0[3], c1[3];
+            for (int k = 0; k < 3; ++k) tm[k] = 0.5f * (T.t0[k] + T.t1[k]);
+            const uint32_t tn = (tm[0] < 0.0f ? 1u : 0u) | (tm[1] < 0.0f ? 2u : 0u) | (tm[2] < 0.0f ? 4u : 0u);
+            const bool bx = tn & 1, by = tn & 2, bz = tn & 4;
+            c0[0] = bx ? tm[0] : T.t0[0]; c1[0] = bx ? T.t1[0] : tm[0];
+            c0[1] = by ? tm[1] : T.t0[1]; c1[1] = by ? T.t1[1] : tm[1];
+            c0[2] = bz ? tm[2] : T.t0[2]; c1[2] = bz ? T.t1[2] : tm[2];
+            const uint32_t child = child_entry(S, T.node, tn ^ T.a);
+            const int l = T.l;
+            if (child == 0u || (child & kLeafBit) || stk.full(l)) {
+                T.tn = tn;
+                break;
+            }
+            ++cnt.node_visits;
+            const uint32_t eb = (c1[0] < c1[1]) ? ((c1[0] < c1[2]) ? 1u : 4u) : ((c1[1] < c1[2]) ? 2u : 4u);
+            T.tn = (tn & eb) ? 8u : (tn | eb);
+            stk.push(T, l, tn);
+            if (!stk.has_iv()) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));
+            T.l = l + 1;
+            T.node = child;
+            for (int k = 0; k < 3; ++k) {
+                T.t0[k] = c0[k];
+                T.t1[k] = c1[k];
+            }
+        }
+    }
     for (uint32_t it = 0;; ++it) {
         if (it == budget) return kTravMore;
         while (T.tn >= 8) {  // T.l falls by one per pop: at most kMaxDepth pops
