@@ -366,7 +366,8 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
         // entries, next children, intervals, node visits -- is the state the
         // loop reaches when it arrives at that child.  The descent stops at a
         // leaf, an empty child or a full stack and leaves that child for the
-        // loop to examine.
+        // loop to examine.  A leaf or an empty child reached this way is
+        // examined here (both are not behind the origin).
         T.fresh = false;
         for (;;) {
             float tm[3], c0[3], c1[3];
@@ -378,13 +379,24 @@ __device__ __forceinline__ uint32_t trav_next_s(Trav &T, const DevScene &S, cons
             c0[2] = bz ? tm[2] : T.t0[2]; c1[2] = bz ? T.t1[2] : tm[2];
             const uint32_t child = child_entry(S, T.node, tn ^ T.a);
             const int l = T.l;
-            if (child == 0u || (child & kLeafBit) || stk.full(l)) {
+            if (stk.full(l) && child != 0u && !(child & kLeafBit)) {
                 T.tn = tn;
                 break;
             }
-            ++cnt.node_visits;
+            // this child is what the loop below would examine next, and it is
+            // not behind the origin (every c1 >= 0): its examination is done
+            // here -- the next child, then an empty child is passed, a leaf
+            // returned and an internal node entered, as in the loop
             const uint32_t eb = (c1[0] < c1[1]) ? ((c1[0] < c1[2]) ? 1u : 4u) : ((c1[1] < c1[2]) ? 2u : 4u);
             T.tn = (tn & eb) ? 8u : (tn | eb);
+            if (child == 0u) break;
+            ++cnt.node_visits;
+            if (child & kLeafBit) {
+                leaf = child & ~kLeafBit;
+                tra = std_max(std_max(c0[0], c0[1]), c0[2]);
+                trb = std_min(std_min(c1[0], c1[1]), c1[2]);
+                return kTravLeaf;
+            }
             stk.push(T, l, tn);
             if (!stk.has_iv()) T.slots = (T.slots & ~(7ull << (3 * l))) | ((uint64_t)tn << (3 * l));
             T.l = l + 1;
