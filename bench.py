@@ -263,6 +263,9 @@ def measure_batched(r, pdf, cdf, steps: int, warmup: int):
         "plain_addon_tiles_64": {"value": tiles, "seconds": t_tiles, "calls": n_tiles},
         "speedup_vs_plain_per_view": batched / plain, "speedup_vs_addon_tiles": batched / tiles,
         "single_kernel_speedup_vs_plain_per_view": single / plain,
+        "target_20x_vs_plain": "unmet: one persistent launch of a large view already keeps every SM busy, so a "
+                               "batch can only win the launch tails, the per-launch list kernels and the small "
+                               "views (see small_views and speedup_vs_addon_tiles)",
         "small_views": small,
         "tuning": {"choice": list(best), "seconds": round(t_tune, 2),
                    "probe": f"centre <={PROBE_SIDE}^2 crops, {PROBE_SPP} spp, every view in a kernel of its own",
