@@ -130,6 +130,27 @@ def search(target, timer, per_path: bool = True):
     return best, table
 
 
+def final_stage(target, candidates, timer):
+    """Times each distinct candidate shape on the real workload (target.set_tuning,
+    then timer()), leaves the fastest set and returns (best, [(shape, ms), ...]).
+    A search on a reduced probe (tune_batch) can favour shapes that lose on the
+    full workload: its winner and, for example, the frame's tuned shape are
+    the usual finalists."""
+    shapes, times = [], []
+    for c in candidates:
+        c = tuple(c)
+        if c in shapes:
+            continue
+        shapes.append(c)
+        target.set_tuning(*c)
+        times.append(timer())
+    if not shapes:
+        raise ValueError("final_stage: no candidate")
+    i = min(range(len(shapes)), key=lambda k: times[k])
+    target.set_tuning(*shapes[i])
+    return shapes[i], list(zip(shapes, times))
+
+
 def _cached(key, target, use_cache):
     import torch
 

@@ -42,3 +42,19 @@ def test_search_confirms_the_leaders():
     assert target.calls[(0, 8, 24, 0, 0, 2, 1)] == 1
     # the three leaders were timed three more times each
     assert target.calls[(0, 8, 24, 0, 0, 4, 4)] == 4 and target.calls[(0, 8, 24, 0, 0, 4, 2)] == 4
+
+
+def test_final_stage_keeps_the_fastest_on_the_full_workload():
+    target = FakeTarget()
+    cost = {(0, 5, 16, 2, 0, 4, 2): 468.0, (0, 8, 24, 2, 0, 3, 1): 448.0}
+
+    def timer():
+        target.calls[target.tuning] = target.calls.get(target.tuning, 0) + 1
+        return cost[target.tuning]
+
+    # the probe's winner first, then the frame's shape; duplicates are timed once
+    best, times = autotune.final_stage(
+        target, [(0, 5, 16, 2, 0, 4, 2), [0, 8, 24, 2, 0, 3, 1], (0, 5, 16, 2, 0, 4, 2)], timer)
+    assert best == (0, 8, 24, 2, 0, 3, 1) and target.tuning == best
+    assert times == [((0, 5, 16, 2, 0, 4, 2), 468.0), ((0, 8, 24, 2, 0, 3, 1), 448.0)]
+    assert all(n == 1 for n in target.calls.values())
